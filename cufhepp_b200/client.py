@@ -1,0 +1,158 @@
+"""Client side of the gate API: seeded keys, encryption, decryption.
+
+In the reference this role is TFHEpp's (``TFHEpp::SecretKey``,
+``TFHEpp::EvalKey``, ``tlweSymEncrypt``/``tlweSymDecrypt``; see
+test/test_gate_gpu.cc:50-58).  The arithmetic lives in
+``csrc/client/tfhe_client.c``; this module wraps it with numpy arrays in the
+TFHEpp layouts the engine consumes (``include/cufhe_b200.h``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import params as P
+from .build import LIB, build_client
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        path = LIB / "libcufhe_client.so"
+        if not path.exists():
+            build_client()
+        lib = C.CDLL(str(path))
+        u64, u32, i32, dbl, vp, i = C.c_uint64, C.c_uint32, C.c_int32, C.c_double, C.c_void_p, C.c_int
+        sigs = {
+            "tfhe_keygen_binary": [u64, u64, u32, vp],
+            "tfhe_tlwe32_encrypt_bits": [u64, u64, vp, u32, vp, u64, u32, dbl, vp],
+            "tfhe_tlwe32_phase_batch": [vp, u32, vp, u64, vp],
+            "tfhe_tlwe32_decrypt_bits": [vp, u32, vp, u64, vp],
+            "tfhe_trlwe32_encrypt": [u64, u64, vp, u32, vp, dbl, vp],
+            "tfhe_trlwe32_phase": [vp, u32, vp, vp],
+            "tfhe_trgsw32_encrypt": [u64, u64, vp, u32, u32, u32, i32, dbl, vp],
+            "tfhe_bk32_gen": [u64, vp, u32, vp, u32, u32, u32, dbl, i, vp],
+            "tfhe_ksk32_gen": [u64, vp, u32, vp, u32, u32, u32, dbl, vp],
+        }
+        for name, argt in sigs.items():
+            fn = getattr(lib, name)
+            fn.argtypes = argt
+            fn.restype = None
+        lib.tfhe_tlwe32_phase.restype = u32
+        _lib = lib
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class SecretKey:
+    """lvl0 (n = 636) and lvl1 (N = 1024) binary keys."""
+    lvl0: np.ndarray  # int32 [636]
+    lvl1: np.ndarray  # int32 [1024]
+    seed: int
+
+    @classmethod
+    def generate(cls, seed: int) -> "SecretKey":
+        lib = _load()
+        k0 = np.empty(P.LVL0_N, np.int32)
+        k1 = np.empty(P.LVL1_N, np.int32)
+        lib.tfhe_keygen_binary(seed, 0, P.LVL0_N, _p(k0))
+        lib.tfhe_keygen_binary(seed, 1, P.LVL1_N, _p(k1))
+        return cls(k0, k1, seed)
+
+
+@dataclass
+class EvalKey:
+    """Bootstrapping key (TRGSW[n0] or, with KeyBundle, TRGSW[n0/2][3]) and
+    lvl1->lvl0 key-switching key, in TFHEpp layouts (uint32 words)."""
+    bk: np.ndarray
+    ksk: np.ndarray
+    keybundle: bool
+
+    @classmethod
+    def generate(cls, sk: SecretKey, keybundle: bool = True, seed: int | None = None) -> "EvalKey":
+        lib = _load()
+        seed = sk.seed + 0x5EED if seed is None else seed
+        bk = np.empty(P.BKKB_WORDS if keybundle else P.BK_WORDS, np.uint32)
+        lib.tfhe_bk32_gen(seed, _p(sk.lvl0), P.LVL0_N, _p(sk.lvl1), P.LVL1_N, P.LVL1_L,
+                          P.LVL1_BGBIT, P.LVL1_ALPHA, int(keybundle), _p(bk))
+        ksk = np.empty(P.KSK_WORDS, np.uint32)
+        lib.tfhe_ksk32_gen(seed + 1, _p(sk.lvl1), P.LVL1_N, _p(sk.lvl0), P.LVL0_N,
+                           P.LVL10_BASEBIT, P.LVL10_T, P.LVL0_ALPHA, _p(ksk))
+        return cls(bk, ksk, keybundle)
+
+
+def _level_n(level: int) -> tuple[int, np.ndarray]:
+    return (P.LVL1_N, None) if level == 1 else (P.LVL0_N, None)
+
+
+def encrypt_bits(sk: SecretKey, bits: np.ndarray, level: int, seed: int,
+                 stream0: int = 0, alpha: float | None = None) -> np.ndarray:
+    """TLWE encryptions of bits (+mu / -mu) at lvl0 or lvl1: [count][n+1]."""
+    lib = _load()
+    bits = np.ascontiguousarray(bits, dtype=np.uint8)
+    n = P.LVL1_N if level == 1 else P.LVL0_N
+    key = sk.lvl1 if level == 1 else sk.lvl0
+    if alpha is None:
+        alpha = P.LVL1_ALPHA if level == 1 else P.LVL0_ALPHA
+    out = np.empty((bits.size, n + 1), np.uint32)
+    lib.tfhe_tlwe32_encrypt_bits(seed, stream0, _p(key), n, _p(bits), bits.size, P.MU32,
+                                 alpha, _p(out))
+    return out
+
+
+def phase(sk: SecretKey, ct: np.ndarray, level: int) -> np.ndarray:
+    lib = _load()
+    ct = np.ascontiguousarray(ct, dtype=np.uint32)
+    n = P.LVL1_N if level == 1 else P.LVL0_N
+    key = sk.lvl1 if level == 1 else sk.lvl0
+    cnt = ct.size // (n + 1)
+    out = np.empty(cnt, np.uint32)
+    lib.tfhe_tlwe32_phase_batch(_p(key), n, _p(ct), cnt, _p(out))
+    return out
+
+
+def decrypt_bits(sk: SecretKey, ct: np.ndarray, level: int) -> np.ndarray:
+    lib = _load()
+    ct = np.ascontiguousarray(ct, dtype=np.uint32)
+    n = P.LVL1_N if level == 1 else P.LVL0_N
+    key = sk.lvl1 if level == 1 else sk.lvl0
+    cnt = ct.size // (n + 1)
+    out = np.empty(cnt, np.uint8)
+    lib.tfhe_tlwe32_decrypt_bits(_p(key), n, _p(ct), cnt, _p(out))
+    return out
+
+
+def trlwe_phase(sk: SecretKey, c: np.ndarray) -> np.ndarray:
+    lib = _load()
+    c = np.ascontiguousarray(c, dtype=np.uint32)
+    out = np.empty(P.LVL1_N, np.uint32)
+    lib.tfhe_trlwe32_phase(_p(sk.lvl1), P.LVL1_N, _p(c), _p(out))
+    return out
+
+
+def trgsw_encrypt(sk: SecretKey, m: int, seed: int, stream: int = 0,
+                  alpha: float = P.LVL1_ALPHA) -> np.ndarray:
+    lib = _load()
+    out = np.empty(P.TRGSW1_WORDS, np.uint32)
+    lib.tfhe_trgsw32_encrypt(seed, stream, _p(sk.lvl1), P.LVL1_N, P.LVL1_L, P.LVL1_BGBIT, m,
+                             alpha, _p(out))
+    return out
+
+
+def trlwe_encrypt(sk: SecretKey, msg: np.ndarray | None, seed: int, stream: int = 0,
+                  alpha: float = P.LVL1_ALPHA) -> np.ndarray:
+    lib = _load()
+    out = np.empty(P.TRLWE1_WORDS, np.uint32)
+    m = None if msg is None else np.ascontiguousarray(msg, dtype=np.uint32)
+    lib.tfhe_trlwe32_encrypt(seed, stream, _p(sk.lvl1), P.LVL1_N,
+                             None if m is None else _p(m), alpha, _p(out))
+    return out
