@@ -76,7 +76,7 @@ def build_engine(force: bool = False, extra: list[str] | None = None) -> Path:
         o = objdir / (s.stem + ".o")
         _run(common + ["-c", str(s), "-o", str(o)])
         objs.append(str(o))
-    _run([NVCC, *GENCODE, "-shared", "-o", str(out), *objs, "-lcudart"])
+    _run([NVCC, *GENCODE, "-shared", "-cudart", "static", "-o", str(out), *objs])
     return out
 
 

@@ -1,0 +1,320 @@
+// FP64 FFNT blind rotation (the drop-in precision form) with fused
+// SampleExtract.
+//
+// Semantics: __BlindRotate__ / __BlindRotateKeyBundle__ with Accumulate /
+// AccumulateKeyBundle (include/gatebootstrapping_gpu.cuh:69-221, :801-884,
+// :895-1033, :1335-1380) and __SampleExtractIndex__<P,0>
+// (src/bootstrap_gpu.cu:1201-1221):
+//   bar = 2N - (b >> 21)  (no rounding), abar_i = (a_i + 2^20) >> 21,
+//   acc = X^bar * (0, vec(mu)),
+//   non-KB step i : acc += round(IFFNT(sum_r FFNT(dec_r(X^abar acc - acc)) BK_i[r]))
+//   KB pair p     : acc  = round(IFFNT(sum_r FFNT(dec_r(acc)) KB_p[r])),
+//                   KB = H + bk0 (X^{a0+a1}-1) + bk1 (X^{a0}-1) + bk2 (X^{a1}-1).
+//
+// B200 layout.  One CTA carries G lanes (gates) through every step in
+// lockstep, so each Fourier-domain key row read from L2 serves G gates
+// (the reference reads the whole key per gate).  4 warps per lane:
+//   phase 1  warp (g, r): digits of row r of lane g, fold + twist, forward
+//            512-point FFT (one warp per transform, fft64.cuh) -> spec[g][r]
+//   phase 2  thread f (frequency bin): key multiply-accumulate for all G lanes;
+//            key words are read once per CTA with 128-bit loads; the KeyBundle
+//            factors X^a - 1 are evaluated from a 2N-entry root table
+//            (psi^{(1+4f) a} - 1) instead of the reference's 16 MB xai table
+//   phase 3  warp (g, j): inverse FFT, untwist, round, write acc[g][j]
+// Epilogue: SampleExtract straight from shared memory to the lane output.
+#include "engine.h"
+#include "fft64.cuh"
+
+namespace cufhe {
+
+namespace {
+
+constexpr int kAbarStride = 640;
+constexpr uint32_t kDecOffset = (128u << 24) + (128u << 16) + (1u << 15);  // offsetgen + round
+
+template <int G>
+constexpr size_t br_smem_bytes()
+{
+    return sizeof(double2) * G * 4 * kSlotStride + sizeof(uint32_t) * G * kTrlwe +
+           sizeof(uint16_t) * G * kAbarStride;
+}
+
+// signed digit d (0 = most significant) of an offset Torus32 value
+__device__ __forceinline__ double digit_of(uint32_t t, int d)
+{
+    return (double)((int32_t)((t >> (24 - 8 * d)) & 255u) - 128);
+}
+
+template <bool KB, int G>
+__global__ void __launch_bounds__(G * 128) k_br_fp64(const uint32_t* __restrict__ lane_in, int lanes,
+                                                     uint32_t mu, const double2* __restrict__ bkf,
+                                                     const double2* __restrict__ psi,
+                                                     const double2* __restrict__ tw512, int steps,
+                                                     uint32_t* __restrict__ acc_out,
+                                                     uint32_t* __restrict__ lane_out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2* spec = reinterpret_cast<double2*>(smem);
+    uint32_t* acc = reinterpret_cast<uint32_t*>(spec + G * 4 * kSlotStride);
+    uint16_t* abar = reinterpret_cast<uint16_t*>(acc + G * kTrlwe);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int lane_base = blockIdx.x * G;
+
+    // ---- prologue: modulus switch and test vector (RotatedTestVector)
+#pragma unroll 1
+    for (int g = 0; g < G; g++) {
+        const int l = lane_base + g;
+        const bool ok = l < lanes;
+        const uint32_t* x = lane_in + (size_t)(ok ? l : 0) * kTlwe0;
+        for (int i = tid; i < kN0; i += blockDim.x)
+            abar[g * kAbarStride + i] = ok ? (uint16_t)((x[i] + (1u << 20)) >> 21) : 0;
+        const uint32_t bar = ok ? 2u * kN - (x[kN0] >> 21) : 2u * kN;
+        for (int i = tid; i < kN; i += blockDim.x) {
+            acc[g * kTrlwe + i] = 0;
+            uint32_t v;
+            if (bar == 2u * kN)
+                v = mu;
+            else
+                v = (((uint32_t)i < (bar & (kN - 1))) ^ (bar >> 10)) ? 0u - mu : mu;
+            acc[g * kTrlwe + kN + i] = v;
+        }
+    }
+    __syncthreads();
+
+    const int total = KB ? kN0 / 2 : kN0;
+    const int nsteps = (steps < 0 || steps > total) ? total : steps;
+    constexpr size_t kTrgswF = 4 * 2 * kHalfN;  // double2 per Fourier TRGSW
+
+#pragma unroll 1
+    for (int p = 0; p < nsteps; p++) {
+        // ---- phase 1: decompose + fold + twist + forward FFT, warp (g, r)
+        {
+            const int g = warp >> 2, r = warp & 3, j = r >> 1, d = r & 1;
+            const uint32_t* a = acc + g * kTrlwe + j * kN;
+            double2 v[16];
+            const uint32_t ab = KB ? 0u : abar[g * kAbarStride + p];
+            const uint32_t abm = ab & (kN - 1), abn = ab >> 10;
+#pragma unroll
+            for (int n2 = 0; n2 < 16; n2++) {
+                const int n = lane + 32 * n2;
+                uint32_t lo = a[n], hi = a[n + kHalfN];
+                if (!KB) {
+                    // X^abar acc - acc (include/gatebootstrapping_gpu.cuh:114-138)
+                    uint32_t rl = a[(n - ab) & (kN - 1)];
+                    uint32_t rh = a[(n + kHalfN - ab) & (kN - 1)];
+                    rl = (((uint32_t)n < abm) ^ abn) ? 0u - rl : rl;
+                    rh = (((uint32_t)(n + kHalfN) < abm) ^ abn) ? 0u - rh : rh;
+                    lo = rl - lo;
+                    hi = rh - hi;
+                }
+                const double2 z = make_double2(digit_of(lo + kDecOffset, d),
+                                               digit_of(hi + kDecOffset, d));
+                v[n2] = cmul(z, __ldg(&psi[n]));
+            }
+            double2* slot = spec + (g * 4 + r) * kSlotStride;
+            fft512_warp<1>(v, slot, tw512, lane);
+#pragma unroll
+            for (int m = 0; m < 16; m++) slot[(lane & 15) + 16 * m + 256 * (lane >> 4)] = v[m];
+        }
+        __syncthreads();
+
+        // ---- phase 2: key multiply-accumulate, thread f = frequency bin
+        if (KB) {
+            const double2* bk = bkf + (size_t)p * 3 * kTrgswF;
+            for (int f = tid; f < kHalfN; f += blockDim.x) {
+                const uint32_t ef = 1u + 4u * (uint32_t)f;
+                double2 out0[G];
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    double2 b[3][4];
+#pragma unroll
+                    for (int e = 0; e < 3; e++)
+#pragma unroll
+                        for (int r = 0; r < 4; r++)
+                            b[e][r] = __ldg(&bk[((e * 4 + r) * 2 + j) * kHalfN + f]);
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        double2 D[4];
+#pragma unroll
+                        for (int r = 0; r < 4; r++) D[r] = spec[(g * 4 + r) * kSlotStride + f];
+                        const uint32_t a0 = abar[g * kAbarStride + 2 * p];
+                        const uint32_t a1 = abar[g * kAbarStride + 2 * p + 1];
+                        double2 x0 = __ldg(&psi[(ef * a0) & 2047u]);
+                        double2 x1 = __ldg(&psi[(ef * a1) & 2047u]);
+                        double2 x01 = __ldg(&psi[(ef * (a0 + a1)) & 2047u]);
+                        x0.x -= 1.0;
+                        x1.x -= 1.0;
+                        x01.x -= 1.0;
+                        double2 s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0;
+#pragma unroll
+                        for (int r = 0; r < 4; r++) {
+                            s0 = cfma(s0, D[r], b[0][r]);
+                            s1 = cfma(s1, D[r], b[1][r]);
+                            s2 = cfma(s2, D[r], b[2][r]);
+                        }
+                        // FFNT(H 2^-32) = 2^-8 (d = 0), 2^-16 (d = 1) on poly j
+                        double2 o = make_double2(fma(D[2 * j].x, 0x1p-8, D[2 * j + 1].x * 0x1p-16),
+                                                 fma(D[2 * j].y, 0x1p-8, D[2 * j + 1].y * 0x1p-16));
+                        o = cfma(o, x01, s0);
+                        o = cfma(o, x0, s1);
+                        o = cfma(o, x1, s2);
+                        if (j == 0) {
+                            out0[g] = o;
+                        } else {
+                            spec[(g * 4 + 0) * kSlotStride + f] = out0[g];
+                            spec[(g * 4 + 1) * kSlotStride + f] = o;
+                        }
+                    }
+                }
+            }
+        } else {
+            const double2* bk = bkf + (size_t)p * kTrgswF;
+            for (int f = tid; f < kHalfN; f += blockDim.x) {
+                double2 out0[G];
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    double2 b[4];
+#pragma unroll
+                    for (int r = 0; r < 4; r++) b[r] = __ldg(&bk[(r * 2 + j) * kHalfN + f]);
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        double2 o = make_double2(0.0, 0.0);
+#pragma unroll
+                        for (int r = 0; r < 4; r++)
+                            o = cfma(o, spec[(g * 4 + r) * kSlotStride + f], b[r]);
+                        if (j == 0) {
+                            out0[g] = o;
+                        } else {
+                            spec[(g * 4 + 0) * kSlotStride + f] = out0[g];
+                            spec[(g * 4 + 1) * kSlotStride + f] = o;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- phase 3: inverse FFT + untwist + round, warp (g, j)
+        if (warp < 2 * G) {
+            const int g = warp >> 1, j = warp & 1;
+            double2* slot = spec + (g * 4 + j) * kSlotStride;
+            double2 v[16];
+#pragma unroll
+            for (int n2 = 0; n2 < 16; n2++) v[n2] = slot[lane + 32 * n2];
+            __syncwarp();
+            fft512_warp<-1>(v, slot, tw512, lane);
+            uint32_t* a = acc + g * kTrlwe + j * kN;
+#pragma unroll
+            for (int m = 0; m < 16; m++) {
+                const int n = (lane & 15) + 16 * m + 256 * (lane >> 4);
+                // untwist = conj(psi^n) / 512; then x 2^32  =>  x 2^23
+                const double2 u = cmulc(v[m], __ldg(&psi[n]));
+                const uint32_t lo = (uint32_t)__double2ll_rn(u.x * 0x1p23);
+                const uint32_t hi = (uint32_t)__double2ll_rn(u.y * 0x1p23);
+                if (KB) {
+                    a[n] = lo;
+                    a[n + kHalfN] = hi;
+                } else {
+                    a[n] += lo;
+                    a[n + kHalfN] += hi;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- epilogue: accumulator and/or SampleExtract (index 0)
+    for (int g = 0; g < G; g++) {
+        const int l = lane_base + g;
+        if (l >= lanes) break;
+        const uint32_t* a = acc + g * kTrlwe;
+        if (acc_out)
+            for (int i = tid; i < kTrlwe; i += blockDim.x) acc_out[(size_t)l * kTrlwe + i] = a[i];
+        if (lane_out) {
+            uint32_t* o = lane_out + (size_t)l * kTlwe1;
+            for (int i = tid; i <= kN; i += blockDim.x)
+                o[i] = i == kN ? a[kN] : (i == 0 ? a[0] : 0u - a[kN - i]);
+        }
+    }
+}
+
+// BK polynomial -> Fourier domain: read as signed int32, scale 2^-32, fold,
+// twist, forward FFT (src/bootstrap_gpu.cu:59-112).  One warp per polynomial.
+__global__ void __launch_bounds__(128) k_bk_to_fft(const uint32_t* __restrict__ bk, int npolys,
+                                                   const double2* __restrict__ psi,
+                                                   const double2* __restrict__ tw512,
+                                                   double2* __restrict__ out)
+{
+    __shared__ __align__(16) double2 tiles[4][kSlotStride];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int poly = blockIdx.x * 4 + warp;
+    if (poly >= npolys) return;
+    const uint32_t* src = bk + (size_t)poly * kN;
+    double2 v[16];
+#pragma unroll
+    for (int n2 = 0; n2 < 16; n2++) {
+        const int n = lane + 32 * n2;
+        const double2 z = make_double2((double)(int32_t)src[n] * 0x1p-32,
+                                       (double)(int32_t)src[n + kHalfN] * 0x1p-32);
+        v[n2] = cmul(z, __ldg(&psi[n]));
+    }
+    fft512_warp<1>(v, tiles[warp], tw512, lane);
+    double2* dst = out + (size_t)poly * kHalfN;
+#pragma unroll
+    for (int m = 0; m < 16; m++) dst[(lane & 15) + 16 * m + 256 * (lane >> 4)] = v[m];
+}
+
+template <bool KB, int G>
+cudaError_t launch_g(const uint32_t* lane_in, int lanes, uint32_t mu, const double2* bkf,
+                     const Fp64Tables& t, int steps, uint32_t* acc_out, uint32_t* lane_out,
+                     cudaStream_t st)
+{
+    constexpr size_t smem = br_smem_bytes<G>();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr[64] = {};
+    if (!attr[dev & 63]) {
+        cudaError_t e = cudaFuncSetAttribute(k_br_fp64<KB, G>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr[dev & 63] = true;
+    }
+    const int blocks = (lanes + G - 1) / G;
+    k_br_fp64<KB, G><<<blocks, G * 128, smem, st>>>(lane_in, lanes, mu, bkf, t.psi, t.tw512, steps,
+                                                    acc_out, lane_out);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+constexpr int kBrGates = 4;
+
+cudaError_t launch_br_fp64(bool kb, const uint32_t* lane_in, int lanes, uint32_t mu,
+                           const double2* bkf, const Fp64Tables& t, int steps, uint32_t* acc_out,
+                           uint32_t* lane_out, cudaStream_t st)
+{
+    if (lanes <= 0) return cudaSuccess;
+    return kb ? launch_g<true, kBrGates>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st)
+              : launch_g<false, kBrGates>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st);
+}
+
+cudaError_t launch_bk_to_fft(const uint32_t* bk, int npolys, const Fp64Tables& t, double2* out,
+                             cudaStream_t st)
+{
+    k_bk_to_fft<<<(npolys + 3) / 4, 128, 0, st>>>(bk, npolys, t.psi, t.tw512, out);
+    return cudaGetLastError();
+}
+
+cudaError_t upload_fft_constants(void)
+{
+    double2 w[16];
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < 16; k++) {
+        const long double a = 2 * pi * k / 32;
+        w[k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    return cudaMemcpyToSymbol(c_w32, w, sizeof(w));
+}
+
+}  // namespace cufhe

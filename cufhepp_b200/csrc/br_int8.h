@@ -1,0 +1,29 @@
+// Exact INT8 tensor-core blind rotation (tcgen05, sm_100a): key and
+// workspace types shared with the engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cufhe {
+
+struct Int8Key {
+    bool ready = false;
+    uint8_t* limbs = nullptr;  // per CMUX step: Toeplitz source rows of the key limbs
+    size_t bytes = 0;
+};
+
+struct Int8Workspace {
+    size_t cap = 0;       // lanes
+    uint32_t* acc = nullptr;
+    int8_t* digits = nullptr;
+    uint16_t* abar = nullptr;
+};
+
+cudaError_t int8_key_build(Int8Key& k, const uint32_t* bk_dev, cudaStream_t st);
+void int8_key_free(Int8Key& k);
+void int8_workspace_free(Int8Workspace& w);
+cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* lane_in, int lanes,
+                           uint32_t mu, int steps, uint32_t* acc_out, uint32_t* lane_out,
+                           cudaStream_t st, int* launches);
+
+}  // namespace cufhe

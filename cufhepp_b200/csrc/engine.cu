@@ -1,0 +1,620 @@
+// C-ABI of the gate engine (include/cufhe_b200.h): global key state per GPU,
+// streams with their own workspaces, and the batched gate pipeline.
+//
+// Reference counterparts: Initialize/CleanUp (src/cufhe_gates_gpu.cu:34-73),
+// key uploads (src/keyswitch_gpu.cu:7-22, src/bootstrap_gpu.cu:212-332), FFT
+// tables (src/ntt_small_modulus.cu:207-244, :369-443), Stream / StreamQuery /
+// Synchronize (include/cufhe_gpu.cuh:70-76, :162-199), gate entry points
+// (src/cufhe_gates_gpu.cu:198-824).
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <atomic>
+#include <vector>
+
+#include "cufhe_b200.h"
+#include "engine.h"
+#include "br_int8.h"
+
+namespace cufhe {
+
+namespace {
+
+constexpr int kMaxDev = 16;
+
+struct DeviceState {
+    bool ready = false;
+    int kb = 0;
+    uint32_t* ksk = nullptr;
+    double2* bkf = nullptr;  // FP64 Fourier-domain bootstrapping key
+    double2* psi = nullptr;
+    double2* tw512 = nullptr;
+    Int8Key i8;              // INT8 exact-path key (non-KeyBundle only)
+};
+
+struct Workspace {
+    size_t lane_cap = 0, gate_cap = 0, io_cap = 0, stage_cap = 0;
+    uint32_t* lane_in = nullptr;
+    uint32_t* lane_out = nullptr;
+    int8_t* ops = nullptr;
+    int32_t* lane_gate = nullptr;
+    int8_t* lane_sub = nullptr;
+    int32_t* gate_lane0 = nullptr;
+    uint32_t* io = nullptr;  // device staging for batch_host: in0,in1,in2,out
+    unsigned char* stage = nullptr;  // pinned host staging for plan uploads
+    cudaEvent_t stage_ev = nullptr;
+    Int8Workspace i8;
+};
+
+}  // namespace
+}  // namespace cufhe
+
+struct cufhe_stream_s {
+    cudaStream_t st = nullptr;
+    int device = 0;
+    cufhe::Workspace ws;
+};
+
+namespace cufhe {
+namespace {
+
+int g_gpu_num = 1;
+int g_stream_count = 0;
+int g_precision = CUFHE_FP64_FFNT;
+DeviceState g_dev[kMaxDev];
+cufhe_stream_s g_default[kMaxDev];
+char g_err[512] = "";
+std::atomic<uint64_t> g_launches{0};
+
+int fail(int code, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(CUFHE_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                             \
+    } while (0)
+
+#define CKL(call)              \
+    do {                       \
+        CK(call);              \
+        g_launches.fetch_add(1); \
+    } while (0)
+
+void free_ws(Workspace& w)
+{
+    cudaFree(w.lane_in);
+    cudaFree(w.lane_out);
+    cudaFree(w.ops);
+    cudaFree(w.lane_gate);
+    cudaFree(w.lane_sub);
+    cudaFree(w.gate_lane0);
+    cudaFree(w.io);
+    if (w.stage) cudaFreeHost(w.stage);
+    if (w.stage_ev) cudaEventDestroy(w.stage_ev);
+    int8_workspace_free(w.i8);
+    w = Workspace();
+}
+
+// grow workspace buffers; waits for the stream first so no kernel still uses
+// the old ones
+int ensure_ws(cufhe_stream_s* s, size_t gates, size_t lanes)
+{
+    Workspace& w = s->ws;
+    if (lanes > w.lane_cap) {
+        CK(cudaStreamSynchronize(s->st));
+        cudaFree(w.lane_in);
+        cudaFree(w.lane_out);
+        cudaFree(w.lane_gate);
+        cudaFree(w.lane_sub);
+        w.lane_in = w.lane_out = nullptr;
+        size_t cap = lanes < 256 ? 256 : lanes;
+        CK(cudaMalloc(&w.lane_in, cap * kTlwe0 * sizeof(uint32_t)));
+        CK(cudaMalloc(&w.lane_out, cap * kTlwe1 * sizeof(uint32_t)));
+        CK(cudaMalloc(&w.lane_gate, cap * sizeof(int32_t)));
+        CK(cudaMalloc(&w.lane_sub, cap));
+        w.lane_cap = cap;
+    }
+    if (gates > w.gate_cap) {
+        CK(cudaStreamSynchronize(s->st));
+        cudaFree(w.ops);
+        cudaFree(w.gate_lane0);
+        size_t cap = gates < 256 ? 256 : gates;
+        CK(cudaMalloc(&w.ops, cap));
+        CK(cudaMalloc(&w.gate_lane0, cap * sizeof(int32_t)));
+        w.gate_cap = cap;
+    }
+    return CUFHE_OK;
+}
+
+cufhe_stream_s* resolve(cufhe_stream_t st)
+{
+    if (st) return st;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxDev) dev = 0;
+    g_default[dev].device = dev;
+    return &g_default[dev];
+}
+
+void host_tables(std::vector<double2>& psi, std::vector<double2>& tw)
+{
+    const long double pi = 3.141592653589793238462643383279502884L;
+    psi.resize(2 * kN);
+    for (int t = 0; t < 2 * kN; t++) {
+        const long double a = pi * t / kN;  // psi = e^{i pi / N}
+        psi[t] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    tw.resize(16 * 32);
+    for (int k2 = 0; k2 < 16; k2++)
+        for (int n1 = 0; n1 < 32; n1++) {
+            const long double a = 2 * pi * (long double)(n1 * k2) / 512;
+            tw[k2 * 32 + n1] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+}
+
+void release_device(int d)
+{
+    DeviceState& D = g_dev[d];
+    cudaSetDevice(d);
+    cudaFree(D.ksk);
+    cudaFree(D.bkf);
+    cudaFree(D.psi);
+    cudaFree(D.tw512);
+    int8_key_free(D.i8);
+    D = DeviceState();
+    free_ws(g_default[d].ws);
+}
+
+int init_device(int d, const cufhe_keyview* ek)
+{
+    DeviceState& D = g_dev[d];
+    CK(cudaSetDevice(d));
+    CK(upload_fft_constants());
+    std::vector<double2> psi, tw;
+    host_tables(psi, tw);
+    CK(cudaMalloc(&D.psi, psi.size() * sizeof(double2)));
+    CK(cudaMalloc(&D.tw512, tw.size() * sizeof(double2)));
+    CK(cudaMemcpy(D.psi, psi.data(), psi.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(D.tw512, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+
+    CK(cudaMalloc(&D.ksk, ek->ksk_words * sizeof(uint32_t)));
+    CK(cudaMemcpy(D.ksk, ek->ksk, ek->ksk_words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+
+    uint32_t* raw = nullptr;
+    CK(cudaMalloc(&raw, ek->bk_words * sizeof(uint32_t)));
+    CK(cudaMemcpy(raw, ek->bk, ek->bk_words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    const int npolys = (int)(ek->bk_words / kN);
+    CK(cudaMalloc(&D.bkf, (size_t)npolys * 512 * sizeof(double2)));
+    const Fp64Tables t = {D.psi, D.tw512};
+    CKL(launch_bk_to_fft(raw, npolys, t, D.bkf, 0));
+    if (!ek->keybundle) {
+        cudaError_t e = int8_key_build(D.i8, raw, 0);
+        if (e != cudaSuccess) {
+            cudaFree(raw);
+            return fail(CUFHE_ERR_CUDA, "INT8 key conversion: %s", cudaGetErrorString(e));
+        }
+    }
+    CK(cudaDeviceSynchronize());
+    cudaFree(raw);
+    D.kb = ek->keybundle;
+    D.ready = true;
+    return CUFHE_OK;
+}
+
+// Host-side lane plan of a batch (uploaded through pinned staging).
+int build_plan(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count, Plan& plan)
+{
+    plan = Plan();
+    plan.count = (int)count;
+    plan.uniform_op = uniform;
+    if (!gates) {
+        if (uniform < 0 || uniform >= kNumGates) return fail(CUFHE_ERR_ARG, "bad gate id %d", uniform);
+        plan.lanes = (int)(count * lanes_of_gate(uniform));
+        return ensure_ws(s, count, plan.lanes);
+    }
+    size_t lanes = 0;
+    for (size_t b = 0; b < count; b++) {
+        if (gates[b] < 0 || gates[b] >= kNumGates)
+            return fail(CUFHE_ERR_ARG, "bad gate id %d at %zu", gates[b], b);
+        lanes += lanes_of_gate(gates[b]);
+    }
+    int rc = ensure_ws(s, count, lanes);
+    if (rc) return rc;
+    Workspace& w = s->ws;
+    const size_t bytes = count * (1 + 4) + lanes * (4 + 1);
+    if (bytes > w.stage_cap) {
+        if (w.stage) {
+            CK(cudaEventSynchronize(w.stage_ev));
+            cudaFreeHost(w.stage);
+            w.stage = nullptr;
+        }
+        CK(cudaMallocHost(&w.stage, bytes));
+        if (!w.stage_ev) CK(cudaEventCreateWithFlags(&w.stage_ev, cudaEventDisableTiming));
+        w.stage_cap = bytes;
+    } else if (w.stage_ev) {
+        CK(cudaEventSynchronize(w.stage_ev));  // previous upload finished reading
+    }
+    int8_t* ops = (int8_t*)w.stage;
+    int32_t* g0 = (int32_t*)(w.stage + count);
+    int32_t* lg = (int32_t*)(w.stage + count * 5);
+    int8_t* ls = (int8_t*)(w.stage + count * 5 + lanes * 4);
+    size_t l = 0;
+    for (size_t b = 0; b < count; b++) {
+        const int n = lanes_of_gate(gates[b]);
+        ops[b] = (int8_t)gates[b];
+        g0[b] = n ? (int32_t)l : -1;
+        for (int k = 0; k < n; k++, l++) {
+            lg[l] = (int32_t)b;
+            ls[l] = (int8_t)k;
+        }
+    }
+    CK(cudaMemcpyAsync(w.ops, ops, count, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(w.gate_lane0, g0, count * 4, cudaMemcpyHostToDevice, s->st));
+    if (lanes) {
+        CK(cudaMemcpyAsync(w.lane_gate, lg, lanes * 4, cudaMemcpyHostToDevice, s->st));
+        CK(cudaMemcpyAsync(w.lane_sub, ls, lanes, cudaMemcpyHostToDevice, s->st));
+    }
+    CK(cudaEventRecord(w.stage_ev, s->st));
+    plan.lanes = (int)lanes;
+    plan.ops = w.ops;
+    plan.lane_gate = w.lane_gate;
+    plan.lane_sub = w.lane_sub;
+    plan.gate_lane0 = w.gate_lane0;
+    return CUFHE_OK;
+}
+
+// blind rotation of plan.lanes lanes with the selected precision form
+int run_br(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint32_t mu, int steps,
+           uint32_t* acc_out, uint32_t* lane_out)
+{
+    DeviceState& D = g_dev[s->device];
+    if (g_precision == CUFHE_INT8_EXACT) {
+        if (D.kb || !D.i8.ready)
+            return fail(CUFHE_ERR_STATE, "INT8_EXACT needs a bootstrapping key without KeyBundle");
+        int launches = 0;
+        cudaError_t e = launch_br_int8(D.i8, s->ws.i8, lane_in, lanes, mu, steps, acc_out,
+                                       lane_out, s->st, &launches);
+        g_launches.fetch_add(launches);
+        if (e != cudaSuccess) return fail(CUFHE_ERR_CUDA, "INT8 blind rotation: %s", cudaGetErrorString(e));
+        return CUFHE_OK;
+    }
+    const Fp64Tables t = {D.psi, D.tw512};
+    CKL(launch_br_fp64(D.kb != 0, lane_in, lanes, mu, D.bkf, t, steps, acc_out, lane_out, s->st));
+    return CUFHE_OK;
+}
+
+int run_batch(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count, int level,
+              uint32_t* out, const uint32_t* in0, const uint32_t* in1, const uint32_t* in2)
+{
+    if (!g_dev[s->device].ready) return fail(CUFHE_ERR_STATE, "cufhe_initialize() not called");
+    if (level != CUFHE_LVL0 && level != CUFHE_LVL1) return fail(CUFHE_ERR_ARG, "bad level %d", level);
+    if (count == 0) return CUFHE_OK;
+    if (count > (1u << 24)) return fail(CUFHE_ERR_ARG, "batch of %zu gates too large", count);
+    if (!out || !in0) return fail(CUFHE_ERR_ARG, "null ciphertext pointer");
+    bool need1 = false, need2 = false;
+    if (gates) {
+        for (size_t b = 0; b < count; b++) {
+            need1 |= lanes_of_gate(gates[b]) > 0;
+            need2 |= gates[b] == kMux || gates[b] == kNMux;
+        }
+    } else {
+        need1 = lanes_of_gate(uniform) > 0;
+        need2 = uniform == kMux || uniform == kNMux;
+    }
+    if ((need1 && !in1) || (need2 && !in2)) return fail(CUFHE_ERR_ARG, "missing input operand");
+    CK(cudaSetDevice(s->device));
+    Plan plan;
+    int rc = build_plan(s, gates, uniform, count, plan);
+    if (rc) return rc;
+    DeviceState& D = g_dev[s->device];
+    Workspace& w = s->ws;
+    if (plan.lanes) {
+        if (level == CUFHE_LVL1)
+            CKL(launch_iks(0, plan, in0, in1, in2, nullptr, D.ksk, w.lane_in, s->st));
+        else
+            CKL(launch_preadd_lvl0(plan, in0, in1, in2, w.lane_in, s->st));
+        rc = run_br(s, w.lane_in, plan.lanes, kMu, -1, nullptr, w.lane_out);
+        if (rc) return rc;
+        if (level == CUFHE_LVL1)
+            CKL(launch_finalize_lvl1(plan, w.lane_out, out, s->st));
+        else
+            CKL(launch_iks(1, plan, nullptr, nullptr, nullptr, w.lane_out, D.ksk, out, s->st));
+    }
+    const bool any_nc = gates ? true : (uniform == kNot || uniform == kCopy);
+    if (any_nc) {
+        bool has = !gates;
+        for (size_t b = 0; gates && b < count && !has; b++)
+            has = gates[b] == kNot || gates[b] == kCopy;
+        if (has) CKL(launch_not_copy(plan, level == CUFHE_LVL1 ? kTlwe1 : kTlwe0, in0, out, s->st));
+    }
+    return CUFHE_OK;
+}
+
+}  // namespace
+}  // namespace cufhe
+
+using namespace cufhe;
+
+extern "C" {
+
+int cufhe_set_gpu_num(int n)
+{
+    int avail = 0;
+    if (cudaGetDeviceCount(&avail) != cudaSuccess) avail = 0;
+    if (n < 1 || n > kMaxDev) return fail(CUFHE_ERR_ARG, "gpu num %d out of range", n);
+    if (avail && n > avail) return fail(CUFHE_ERR_ARG, "only %d GPUs visible", avail);
+    g_gpu_num = n;
+    return CUFHE_OK;
+}
+
+int cufhe_get_gpu_num(void) { return g_gpu_num; }
+
+int cufhe_initialize(const cufhe_keyview* ek)
+{
+    if (!ek || !ek->bk || !ek->ksk) return fail(CUFHE_ERR_ARG, "null key view");
+    const uint64_t want_bk = ek->keybundle ? CUFHE_BKKB1_WORDS : CUFHE_BK1_WORDS;
+    if (ek->bk_words != want_bk)
+        return fail(CUFHE_ERR_ARG, "bootstrapping key has %zu words, expected %llu", ek->bk_words,
+                    (unsigned long long)want_bk);
+    if (ek->ksk_words != CUFHE_KSK10_WORDS)
+        return fail(CUFHE_ERR_ARG, "key-switching key has %zu words, expected %llu",
+                    ek->ksk_words, (unsigned long long)CUFHE_KSK10_WORDS);
+    int avail = 0;
+    if (cudaGetDeviceCount(&avail) != cudaSuccess || avail == 0)
+        return fail(CUFHE_ERR_CUDA, "no CUDA device visible");
+    if (g_gpu_num > avail) return fail(CUFHE_ERR_ARG, "gpu num %d > %d visible", g_gpu_num, avail);
+    for (int d = 0; d < g_gpu_num; d++) {
+        if (g_dev[d].ready) release_device(d);
+        int rc = init_device(d, ek);
+        if (rc) {
+            release_device(d);
+            return rc;
+        }
+    }
+    cudaSetDevice(0);
+    return CUFHE_OK;
+}
+
+int cufhe_cleanup(void)
+{
+    for (int d = 0; d < kMaxDev; d++)
+        if (g_dev[d].ready) release_device(d);
+    cudaSetDevice(0);
+    return CUFHE_OK;
+}
+
+int cufhe_synchronize(void)
+{
+    for (int d = 0; d < g_gpu_num; d++) {
+        CK(cudaSetDevice(d));
+        CK(cudaDeviceSynchronize());
+    }
+    return CUFHE_OK;
+}
+
+int cufhe_set_precision(int form)
+{
+    if (form != CUFHE_FP64_FFNT && form != CUFHE_INT8_EXACT)
+        return fail(CUFHE_ERR_ARG, "unknown precision form %d", form);
+    g_precision = form;
+    return CUFHE_OK;
+}
+
+int cufhe_get_precision(void) { return g_precision; }
+
+int cufhe_stream_create(cufhe_stream_t* st, int device)
+{
+    if (!st) return fail(CUFHE_ERR_ARG, "null stream handle");
+    if (device < 0) device = g_stream_count % g_gpu_num;
+    if (device >= g_gpu_num) return fail(CUFHE_ERR_ARG, "device %d >= gpu num", device);
+    g_stream_count++;
+    cufhe_stream_s* s = new cufhe_stream_s();
+    s->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete s;
+        return fail(CUFHE_ERR_CUDA, "stream create: %s", cudaGetErrorString(e));
+    }
+    *st = s;
+    return CUFHE_OK;
+}
+
+int cufhe_stream_destroy(cufhe_stream_t st)
+{
+    if (!st) return CUFHE_OK;
+    cudaSetDevice(st->device);
+    cudaStreamSynchronize(st->st);
+    free_ws(st->ws);
+    cudaStreamDestroy(st->st);
+    delete st;
+    return CUFHE_OK;
+}
+
+int cufhe_stream_query(cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    cudaSetDevice(s->device);
+    cudaError_t e = cudaStreamQuery(s->st);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) return 0;
+    return fail(CUFHE_ERR_CUDA, "stream query: %s", cudaGetErrorString(e));
+}
+
+int cufhe_stream_device(cufhe_stream_t st) { return resolve(st)->device; }
+
+int cufhe_stream_synchronize(cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->st));
+    return CUFHE_OK;
+}
+
+int cufhe_ctxt_alloc(void** dptr, size_t bytes, int device)
+{
+    if (!dptr) return fail(CUFHE_ERR_ARG, "null pointer");
+    CK(cudaSetDevice(device < 0 ? 0 : device));
+    if (cudaMalloc(dptr, bytes) != cudaSuccess) return fail(CUFHE_ERR_NOMEM, "cudaMalloc(%zu) failed", bytes);
+    return CUFHE_OK;
+}
+
+int cufhe_ctxt_free(void* dptr, int device)
+{
+    CK(cudaSetDevice(device < 0 ? 0 : device));
+    CK(cudaFree(dptr));
+    return CUFHE_OK;
+}
+
+int cufhe_host_register(void* host, size_t bytes)
+{
+    CK(cudaHostRegister(host, bytes, cudaHostRegisterDefault));
+    return CUFHE_OK;
+}
+
+int cufhe_host_unregister(void* host)
+{
+    CK(cudaHostUnregister(host));
+    return CUFHE_OK;
+}
+
+int cufhe_memcpy_h2d(void* dst, const void* src, size_t bytes, cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    CK(cudaSetDevice(s->device));
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->st));
+    return CUFHE_OK;
+}
+
+int cufhe_memcpy_d2h(void* dst, const void* src, size_t bytes, cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    CK(cudaSetDevice(s->device));
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->st));
+    return CUFHE_OK;
+}
+
+int cufhe_gate(int gate, int level, uint32_t* out, const uint32_t* in0, const uint32_t* in1,
+               const uint32_t* in2, cufhe_stream_t st)
+{
+    if (gate < 0 || gate >= kNumGates) return fail(CUFHE_ERR_ARG, "bad gate id %d", gate);
+    return run_batch(resolve(st), nullptr, gate, 1, level, out, in0, in1, in2);
+}
+
+int cufhe_gate_copy(int gate, int level, uint32_t* out_host, uint32_t* out_dev,
+                    const uint32_t* in0_host, uint32_t* in0_dev, const uint32_t* in1_host,
+                    uint32_t* in1_dev, const uint32_t* in2_host, uint32_t* in2_dev,
+                    cufhe_stream_t st)
+{
+    if (gate < 0 || gate >= kNumGates) return fail(CUFHE_ERR_ARG, "bad gate id %d", gate);
+    cufhe_stream_s* s = resolve(st);
+    const size_t bytes = (level == CUFHE_LVL1 ? kTlwe1 : kTlwe0) * sizeof(uint32_t);
+    CK(cudaSetDevice(s->device));
+    const int nin = gate == kNot || gate == kCopy ? 1 : (gate == kMux || gate == kNMux ? 3 : 2);
+    const uint32_t* hs[3] = {in0_host, in1_host, in2_host};
+    uint32_t* ds[3] = {in0_dev, in1_dev, in2_dev};
+    for (int i = 0; i < nin; i++) {
+        if (!hs[i] || !ds[i]) return fail(CUFHE_ERR_ARG, "missing operand %d", i);
+        CK(cudaMemcpyAsync(ds[i], hs[i], bytes, cudaMemcpyHostToDevice, s->st));
+    }
+    int rc = run_batch(s, nullptr, gate, 1, level, out_dev, in0_dev, in1_dev, in2_dev);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(out_host, out_dev, bytes, cudaMemcpyDeviceToHost, s->st));
+    return CUFHE_OK;
+}
+
+int cufhe_gate_batch(const int32_t* gates_host, int uniform_gate, size_t count, int level,
+                     uint32_t* out, const uint32_t* in0, const uint32_t* in1, const uint32_t* in2,
+                     cufhe_stream_t st)
+{
+    return run_batch(resolve(st), gates_host, uniform_gate, count, level, out, in0, in1, in2);
+}
+
+int cufhe_gate_batch_host(const int32_t* gates_host, int uniform_gate, size_t count, int level,
+                          uint32_t* out_host, const uint32_t* in0_host, const uint32_t* in1_host,
+                          const uint32_t* in2_host, cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    if (count == 0) return CUFHE_OK;
+    const size_t words = level == CUFHE_LVL1 ? kTlwe1 : kTlwe0;
+    const size_t bytes = count * words * sizeof(uint32_t);
+    CK(cudaSetDevice(s->device));
+    Workspace& w = s->ws;
+    if (4 * count * words > w.io_cap) {
+        CK(cudaStreamSynchronize(s->st));
+        cudaFree(w.io);
+        w.io = nullptr;
+        if (cudaMalloc(&w.io, 4 * bytes) != cudaSuccess)
+            return fail(CUFHE_ERR_NOMEM, "io buffer of %zu bytes", 4 * bytes);
+        w.io_cap = 4 * count * words;
+    }
+    uint32_t* d0 = w.io;
+    uint32_t* d1 = w.io + count * words;
+    uint32_t* d2 = w.io + 2 * count * words;
+    uint32_t* dout = w.io + 3 * count * words;
+    CK(cudaMemcpyAsync(d0, in0_host, bytes, cudaMemcpyHostToDevice, s->st));
+    if (in1_host) CK(cudaMemcpyAsync(d1, in1_host, bytes, cudaMemcpyHostToDevice, s->st));
+    if (in2_host) CK(cudaMemcpyAsync(d2, in2_host, bytes, cudaMemcpyHostToDevice, s->st));
+    int rc = run_batch(s, gates_host, uniform_gate, count, level, dout, d0, in1_host ? d1 : nullptr,
+                       in2_host ? d2 : nullptr);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(out_host, dout, bytes, cudaMemcpyDeviceToHost, s->st));
+    return CUFHE_OK;
+}
+
+int cufhe_blind_rotate(const uint32_t* tlwe0, size_t count, uint32_t mu, int steps,
+                       uint32_t* acc_out, uint32_t* tlwe_out, cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    if (!g_dev[s->device].ready) return fail(CUFHE_ERR_STATE, "cufhe_initialize() not called");
+    if (!tlwe0 || (!acc_out && !tlwe_out)) return fail(CUFHE_ERR_ARG, "null pointer");
+    if (count == 0) return CUFHE_OK;
+    if (count > (1u << 24)) return fail(CUFHE_ERR_ARG, "too many inputs");
+    CK(cudaSetDevice(s->device));
+    return run_br(s, tlwe0, (int)count, mu, steps, acc_out, tlwe_out);
+}
+
+int cufhe_identity_keyswitch(const uint32_t* tlwe1, size_t count, uint32_t* tlwe0_out,
+                             cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    if (!g_dev[s->device].ready) return fail(CUFHE_ERR_STATE, "cufhe_initialize() not called");
+    if (!tlwe1 || !tlwe0_out) return fail(CUFHE_ERR_ARG, "null pointer");
+    if (count == 0) return CUFHE_OK;
+    if (count > (1u << 24)) return fail(CUFHE_ERR_ARG, "too many inputs");
+    CK(cudaSetDevice(s->device));
+    Plan plan = Plan();
+    plan.count = plan.lanes = (int)count;
+    // mode 1 reads the inputs as lane outputs; a binary gate id gives one lane
+    // per input and the identity combination (1, 0, 0)
+    plan.uniform_op = kAnd;
+    CKL(launch_iks(1, plan, nullptr, nullptr, nullptr, tlwe1, g_dev[s->device].ksk, tlwe0_out,
+                   s->st));
+    return CUFHE_OK;
+}
+
+const char* cufhe_last_error(void) { return g_err; }
+
+uint64_t cufhe_kernel_launches(void) { return g_launches.load(); }
+
+int cufhe_device_ok(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return 0;
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, 0) != cudaSuccess) return 0;
+    return p.major == 10 ? 1 : 0;
+}
+
+}  // extern "C"

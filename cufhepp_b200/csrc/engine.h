@@ -1,0 +1,166 @@
+// Internal declarations shared by the engine's CUDA sources.
+//
+// Execution model.  A call of the gate API carries a batch of B gates.  Each
+// gate expands into "lanes", one per blind rotation it needs: a binary gate
+// has one lane, Mux/NMux have two (src/bootstrap_gpu.cu:1557-1672), Not/Copy
+// none (:2200-2222).  Every kernel processes lanes or gates in bulk:
+//
+//   IKS->BR order (Ctxt<lvl1>):  k_iks (gate inputs -> lane lvl0 TLWEs)
+//                                k_br_*  (lane lvl0 -> lane lvl1 TLWE, SE fused)
+//                                k_finalize_lvl1 (lanes -> gate outputs)
+//   BR->IKS order (Ctxt<lvl0>):  k_preadd_lvl0 (gate inputs -> lane lvl0)
+//                                k_br_*
+//                                k_iks (lanes combined -> gate outputs)
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "params.h"
+
+namespace cufhe {
+
+constexpr int kN0 = CUFHE_LVL0_N;          // 636
+constexpr int kN = CUFHE_LVL1_N;           // 1024
+constexpr int kTlwe0 = CUFHE_TLWE0_WORDS;  // 637
+constexpr int kTlwe1 = CUFHE_TLWE1_WORDS;  // 1025
+constexpr int kTrlwe = CUFHE_TRLWE1_WORDS; // 2048
+constexpr uint32_t kMu = CUFHE_MU32;
+
+enum GateId {
+    kNand = 0, kOr, kOrYN, kOrNY, kAnd, kAndYN, kAndNY, kNor, kXor, kXnor,
+    kNot, kCopy, kMux, kNMux, kNumGates
+};
+
+// Pre-add coefficients of the binary gates, in the input level's torus
+// (src/bootstrap_gpu.cu:1905-1914, :1937-1946).
+struct GateCoef {
+    int32_t ca, cb;
+    uint32_t off;
+};
+
+__host__ __device__ inline GateCoef gate_coef(int g)
+{
+    const uint32_t mu = kMu;
+    switch (g) {
+    case kNand: return {-1, -1, mu};
+    case kNor: return {-1, -1, 0u - mu};
+    case kXnor: return {-2, -2, 0u - 2 * mu};
+    case kAnd: return {1, 1, 0u - mu};
+    case kOr: return {1, 1, mu};
+    case kXor: return {2, 2, 2 * mu};
+    case kAndNY: return {-1, 1, 0u - mu};
+    case kAndYN: return {1, -1, 0u - mu};
+    case kOrNY: return {-1, 1, mu};
+    case kOrYN: return {1, -1, mu};
+    default: return {1, 0, 0};
+    }
+}
+
+__host__ __device__ inline int lanes_of_gate(int g)
+{
+    return (g == kMux || g == kNMux) ? 2 : (g == kNot || g == kCopy) ? 0 : 1;
+}
+
+// Lane plan of a batch.  With ops == nullptr every gate is `uniform_op` and
+// lanes map arithmetically; otherwise lane_gate[l] is the gate of lane l,
+// lane_sub[l] its index within the gate (0/1), gate_lane0[b] the first lane
+// of gate b (-1 for Not/Copy).
+struct Plan {
+    int count;       // gates
+    int lanes;       // lanes
+    int uniform_op;  // used when ops == nullptr
+    const int8_t* ops;
+    const int32_t* lane_gate;
+    const int8_t* lane_sub;
+    const int32_t* gate_lane0;
+};
+
+__device__ inline int plan_op(const Plan& p, int b) { return p.ops ? p.ops[b] : p.uniform_op; }
+
+__device__ inline void plan_lane(const Plan& p, int l, int& b, int& sub)
+{
+    if (p.ops) {
+        b = p.lane_gate[l];
+        sub = p.lane_sub[l];
+    } else if (lanes_of_gate(p.uniform_op) == 2) {
+        b = l >> 1;
+        sub = l & 1;
+    } else {
+        b = l;
+        sub = 0;
+    }
+}
+
+__device__ inline int plan_lane0(const Plan& p, int b)
+{
+    if (p.ops) return p.gate_lane0[b];
+    const int n = lanes_of_gate(p.uniform_op);
+    return n ? b * n : -1;
+}
+
+// Pre-add of lane (b, sub): x = ca * A + cb * B (+ off on b)
+//   binary gate : A = in0[b], B = in1[b], table coefficients
+//   mux lane 0  : A = inc = in0[b], B = in1[b], (1, 1, -mu)
+//   mux lane 1  : A = inc = in0[b], B = in0_mux = in2[b], (-1, 1, -mu)
+struct LanePreadd {
+    const uint32_t* a;
+    const uint32_t* b;
+    int32_t ca, cb;
+    uint32_t off;
+};
+
+__device__ inline LanePreadd lane_preadd(int op, int sub, const uint32_t* in0,
+                                         const uint32_t* in1, const uint32_t* in2)
+{
+    if (op == kMux || op == kNMux) {
+        if (sub == 0) return {in0, in1, 1, 1, 0u - kMu};
+        return {in0, in2, -1, 1, 0u - kMu};
+    }
+    const GateCoef c = gate_coef(op);
+    return {in0, in1, c.ca, c.cb, c.off};
+}
+
+// Combination of a gate's lane outputs (lvl1 TLWEs) into the gate's lvl1
+// result: binary -> lane0; Mux -> lane0 + lane1 + mu; NMux -> -(..) - mu.
+__device__ inline LanePreadd gate_combine(int op, const uint32_t* lane0, const uint32_t* lane1)
+{
+    if (op == kMux) return {lane0, lane1, 1, 1, kMu};
+    if (op == kNMux) return {lane0, lane1, -1, -1, 0u - kMu};
+    return {lane0, nullptr, 1, 0, 0};
+}
+
+// ------------------------------------------------------------ launchers ----
+// Each returns cudaSuccess or the launch error.
+
+// IKS of lanes (mode 0: IKS->BR, gate inputs at lvl1 -> lane_in) or of gates
+// (mode 1: BR->IKS, combined lane outputs -> out at lvl0).
+cudaError_t launch_iks(int mode, const Plan& plan, const uint32_t* in0, const uint32_t* in1,
+                       const uint32_t* in2, const uint32_t* lane_out, const uint32_t* ksk,
+                       uint32_t* dst, cudaStream_t st);
+
+cudaError_t launch_preadd_lvl0(const Plan& plan, const uint32_t* in0, const uint32_t* in1,
+                               const uint32_t* in2, uint32_t* lane_in, cudaStream_t st);
+
+cudaError_t launch_finalize_lvl1(const Plan& plan, const uint32_t* lane_out, uint32_t* out,
+                                 cudaStream_t st);
+
+cudaError_t launch_not_copy(const Plan& plan, int words, const uint32_t* in0, uint32_t* out,
+                            cudaStream_t st);
+
+// FP64 FFNT blind rotation + SampleExtract of `lanes` lvl0 TLWEs.
+// acc_out (optional) receives the TRLWE accumulators; lane_out (optional) the
+// extracted lvl1 TLWEs.  steps < 0: all steps.
+struct Fp64Tables {
+    const double2* psi;    // psi^t, t < 2048, psi = e^{i pi / 1024}
+    const double2* tw512;  // [16][32] e^{2 pi i n1 k2 / 512}
+};
+cudaError_t launch_br_fp64(bool kb, const uint32_t* lane_in, int lanes, uint32_t mu,
+                           const double2* bkf, const Fp64Tables& t, int steps,
+                           uint32_t* acc_out, uint32_t* lane_out, cudaStream_t st);
+
+cudaError_t launch_bk_to_fft(const uint32_t* bk, int npolys, const Fp64Tables& t, double2* out,
+                             cudaStream_t st);
+cudaError_t upload_fft_constants(void);
+
+}  // namespace cufhe

@@ -1,0 +1,155 @@
+// FP64 negacyclic FFNT for N = 1024 (512-point complex transform), one warp
+// per polynomial.
+//
+// Same transform as the reference's GPU-FFT backend (fold, twist, N/2-point
+// FFT with roots e^{+2 pi i k/(N/2)}, inverse with conjugate roots, untwist
+// with 1/(N/2) folded in: src/ntt_small_modulus.cu:207-244,
+// include/ntt_small_modulus.cuh:977-1182), restructured for a warp:
+//
+//   512 = 16 x 32.  Lane n1 holds x[n1 + 32 n2], n2 = 0..15, in registers.
+//   1. 16-point DFT over n2 in registers (radix 4 x 4).
+//   2. twiddle w512^(n1 k2) (table, coalesced per lane).
+//   3. transpose through a padded 16 x 33 shared-memory tile (conflict-free).
+//   4. lane (k2 + 16 h) holds the n1 = h + 2m half of sequence k2; 16-point
+//      DFT over m in registers.
+//   5. one radix-2 stage across lanes l and l ^ 16 (warp shuffle).
+//   Output: lane (k2 + 16 h), register m holds bin k2 + 16 m + 256 h.
+//
+// The reference runs one 512-point FFT per CTA with 256 threads and
+// __syncthreads between stages; here a warp owns a whole transform and only
+// synchronises with __syncwarp, so 16+ transforms proceed independently per
+// SM.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cufhe {
+
+constexpr int kHalfN = 512;
+constexpr int kSlotStride = 528;  // double2 per transform slot (16 x 33 tile)
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// a * conj(b)
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b)
+{
+    return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ double2 cfma(double2 acc, double2 a, double2 b)
+{
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+    return acc;
+}
+// multiply by S*i, S = +1 (forward) or -1 (inverse)
+template <int S>
+__device__ __forceinline__ double2 mul_si(double2 a)
+{
+    return S > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+// In-place 4-point DFT with root S*i.
+template <int S>
+__device__ __forceinline__ void dft4(double2& u0, double2& u1, double2& u2, double2& u3)
+{
+    const double2 t0 = cadd(u0, u2), t1 = csub(u0, u2);
+    const double2 t2 = cadd(u1, u3), t3 = mul_si<S>(csub(u1, u3));
+    u0 = cadd(t0, t2);
+    u2 = csub(t0, t2);
+    u1 = cadd(t1, t3);
+    u3 = csub(t1, t3);
+}
+
+// In-place 16-point DFT, natural order in and out:
+//   X[k] = sum_n x[n] e^{S 2 pi i n k / 16}
+// radix 4 x 4: n = 4a + b, k = c + 4d.
+template <int S>
+__device__ __forceinline__ void dft16(double2 (&v)[16])
+{
+    constexpr double C1 = 0.92387953251128675613; // cos(pi/8)
+    constexpr double S1 = 0.38268343236508977173; // sin(pi/8)
+    constexpr double R2 = 0.70710678118654752440; // cos(pi/4)
+#pragma unroll
+    for (int b = 0; b < 4; b++) dft4<S>(v[b], v[4 + b], v[8 + b], v[12 + b]);
+    // now v[4c + b] = y[b][c]; twiddle by w^(b c), w = e^{S 2 pi i/16}
+    // (b, c) = (1,1): w, (1,2): w^2, (1,3): w^3, (2,1): w^2, (2,2): w^4 = S i,
+    // (2,3): w^6, (3,1): w^3, (3,2): w^6, (3,3): w^9
+    const double2 w1 = make_double2(C1, S * S1);
+    const double2 w3 = make_double2(S1, S * C1);
+    const double2 w9 = make_double2(-C1, -S * S1);
+    auto mw2 = [](double2 a) {  // * (R2, S R2)
+        return make_double2(R2 * (a.x - S * a.y), R2 * (a.y + S * a.x));
+    };
+    auto mw6 = [](double2 a) {  // * (-R2, S R2)
+        return make_double2(-R2 * (a.x + S * a.y), R2 * (S * a.x - a.y));
+    };
+    v[4 * 1 + 1] = cmul(v[4 * 1 + 1], w1);
+    v[4 * 2 + 1] = mw2(v[4 * 2 + 1]);
+    v[4 * 3 + 1] = cmul(v[4 * 3 + 1], w3);
+    v[4 * 1 + 2] = mw2(v[4 * 1 + 2]);
+    v[4 * 2 + 2] = mul_si<S>(v[4 * 2 + 2]);
+    v[4 * 3 + 2] = mw6(v[4 * 3 + 2]);
+    v[4 * 1 + 3] = cmul(v[4 * 1 + 3], w3);
+    v[4 * 2 + 3] = mw6(v[4 * 2 + 3]);
+    v[4 * 3 + 3] = cmul(v[4 * 3 + 3], w9);
+    // 4-point DFT over b for each c: X[c + 4d]
+    double2 o[16];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        double2 u0 = v[4 * c + 0], u1 = v[4 * c + 1], u2 = v[4 * c + 2], u3 = v[4 * c + 3];
+        dft4<S>(u0, u1, u2, u3);
+        o[c + 0] = u0;
+        o[c + 4] = u1;
+        o[c + 8] = u2;
+        o[c + 12] = u3;
+    }
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = o[k];
+}
+
+// Twiddles of the 32-point stage: e^{2 pi i k / 32}, k = 0..15
+static __constant__ double2 c_w32[16];
+
+// Warp-level 512-point DFT with root e^{S 2 pi i / 512}.
+//   in : v[n2] = x[lane + 32 n2]
+//   out: v[m]  = X[(lane & 15) + 16 m + 256 (lane >> 4)]
+// tile: this warp's shared slot (>= 528 double2), free on entry; tw512:
+// global table tw512[k2 * 32 + n1] = e^{2 pi i n1 k2 / 512}.
+template <int S>
+__device__ __forceinline__ void fft512_warp(double2 (&v)[16], double2* tile,
+                                            const double2* __restrict__ tw512, int lane)
+{
+    dft16<S>(v);
+#pragma unroll
+    for (int k2 = 1; k2 < 16; k2++) {
+        const double2 w = __ldg(&tw512[k2 * 32 + lane]);
+        v[k2] = S > 0 ? cmul(v[k2], w) : cmulc(v[k2], w);
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < 16; k2++) tile[k2 * 33 + lane] = v[k2];
+    __syncwarp();
+    const int k2 = lane & 15, h = lane >> 4;
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = tile[k2 * 33 + h + 2 * m];
+    __syncwarp();
+    dft16<S>(v);
+    // radix-2 across lanes l, l^16: Z[k2 + 16 m + 256 b] = E0[m] +- w32^m E1[m]
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        double2 w = c_w32[m];
+        if (S < 0) w.y = -w.y;
+        double2 t = h ? cmul(v[m], w) : v[m];
+        double2 o;
+        o.x = __shfl_xor_sync(0xffffffffu, t.x, 16);
+        o.y = __shfl_xor_sync(0xffffffffu, t.y, 16);
+        v[m] = h ? csub(o, t) : cadd(t, o);
+    }
+}
+
+}  // namespace cufhe

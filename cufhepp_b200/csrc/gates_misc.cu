@@ -1,0 +1,91 @@
+// Elementwise parts of the gate front-end:
+//   k_preadd_lvl0   lvl0 pre-add of the BR->IKS order, which the reference
+//                   folds into the modulus switch (__BlindRotatePreAdd__,
+//                   include/gatebootstrapping_gpu.cuh:1382-1429, :1432-1521)
+//   k_finalize_lvl1 lane outputs -> gate outputs of the IKS->BR order
+//                   (Mux: + mu, NMux: negate - mu; src/bootstrap_gpu.cu:1557-1672)
+//   k_not_copy      Not / Copy (src/bootstrap_gpu.cu:2200-2222)
+#include "engine.h"
+
+namespace cufhe {
+
+namespace {
+
+__global__ void k_preadd_lvl0(Plan plan, const uint32_t* __restrict__ in0,
+                              const uint32_t* __restrict__ in1, const uint32_t* __restrict__ in2,
+                              uint32_t* __restrict__ lane_in)
+{
+    const int l = blockIdx.x;
+    if (l >= plan.lanes) return;
+    int b, sub;
+    plan_lane(plan, l, b, sub);
+    const size_t o = (size_t)b * kTlwe0;
+    const LanePreadd p = lane_preadd(plan_op(plan, b), sub, in0 + o, in1 ? in1 + o : nullptr,
+                                     in2 ? in2 + o : nullptr);
+    uint32_t* dst = lane_in + (size_t)l * kTlwe0;
+    for (int i = threadIdx.x; i < kTlwe0; i += blockDim.x) {
+        uint32_t x = (uint32_t)p.ca * p.a[i];
+        if (p.cb) x += (uint32_t)p.cb * p.b[i];
+        if (i == kN0) x += p.off;
+        dst[i] = x;
+    }
+}
+
+__global__ void k_finalize_lvl1(Plan plan, const uint32_t* __restrict__ lane_out,
+                                uint32_t* __restrict__ out)
+{
+    const int b = blockIdx.x;
+    if (b >= plan.count) return;
+    const int op = plan_op(plan, b);
+    const int l0 = plan_lane0(plan, b);
+    if (l0 < 0) return;
+    const LanePreadd p = gate_combine(op, lane_out + (size_t)l0 * kTlwe1,
+                                      lane_out + (size_t)(l0 + 1) * kTlwe1);
+    uint32_t* dst = out + (size_t)b * kTlwe1;
+    for (int i = threadIdx.x; i < kTlwe1; i += blockDim.x) {
+        uint32_t x = (uint32_t)p.ca * p.a[i];
+        if (p.cb) x += (uint32_t)p.cb * p.b[i];
+        if (i == kN) x += p.off;
+        dst[i] = x;
+    }
+}
+
+__global__ void k_not_copy(Plan plan, int words, const uint32_t* __restrict__ in0,
+                           uint32_t* __restrict__ out)
+{
+    const int b = blockIdx.x;
+    if (b >= plan.count) return;
+    const int op = plan_op(plan, b);
+    if (op != kNot && op != kCopy) return;
+    const uint32_t* s = in0 + (size_t)b * words;
+    uint32_t* d = out + (size_t)b * words;
+    for (int i = threadIdx.x; i < words; i += blockDim.x) d[i] = op == kNot ? 0u - s[i] : s[i];
+}
+
+}  // namespace
+
+cudaError_t launch_preadd_lvl0(const Plan& plan, const uint32_t* in0, const uint32_t* in1,
+                               const uint32_t* in2, uint32_t* lane_in, cudaStream_t st)
+{
+    if (plan.lanes <= 0) return cudaSuccess;
+    k_preadd_lvl0<<<plan.lanes, 128, 0, st>>>(plan, in0, in1, in2, lane_in);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_lvl1(const Plan& plan, const uint32_t* lane_out, uint32_t* out,
+                                 cudaStream_t st)
+{
+    if (plan.count <= 0) return cudaSuccess;
+    k_finalize_lvl1<<<plan.count, 256, 0, st>>>(plan, lane_out, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_not_copy(const Plan& plan, int words, const uint32_t* in0, uint32_t* out,
+                            cudaStream_t st)
+{
+    if (plan.count <= 0) return cudaSuccess;
+    k_not_copy<<<plan.count, 256, 0, st>>>(plan, words, in0, out);
+    return cudaGetLastError();
+}
+
+}  // namespace cufhe

@@ -1,0 +1,228 @@
+"""ctypes binding of the engine's C-ABI (``include/cufhe_b200.h``).
+
+Loads the in-tree ``lib/libcufhe_b200.so`` and raises if it is missing or
+fails to load: there is no CPU fallback for any engine operation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import params as P
+from .build import LIB
+
+OK = 0
+ERR = {-1: "CUFHE_ERR_ARG", -2: "CUFHE_ERR_STATE", -3: "CUFHE_ERR_CUDA", -4: "CUFHE_ERR_NOMEM",
+       -5: "CUFHE_ERR_UNSUPPORTED"}
+
+LVL0, LVL1 = 0, 1
+
+# every symbol include/cufhe_b200.h declares: (argtypes, restype)
+_vp, _sz, _i, _u32, _u64 = C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_uint64
+SIGNATURES = {
+    "cufhe_set_gpu_num": ([_i], _i),
+    "cufhe_get_gpu_num": ([], _i),
+    "cufhe_initialize": ([_vp], _i),
+    "cufhe_cleanup": ([], _i),
+    "cufhe_synchronize": ([], _i),
+    "cufhe_set_precision": ([_i], _i),
+    "cufhe_get_precision": ([], _i),
+    "cufhe_stream_create": ([_vp, _i], _i),
+    "cufhe_stream_destroy": ([_vp], _i),
+    "cufhe_stream_query": ([_vp], _i),
+    "cufhe_stream_device": ([_vp], _i),
+    "cufhe_stream_synchronize": ([_vp], _i),
+    "cufhe_ctxt_alloc": ([_vp, _sz, _i], _i),
+    "cufhe_ctxt_free": ([_vp, _i], _i),
+    "cufhe_host_register": ([_vp, _sz], _i),
+    "cufhe_host_unregister": ([_vp], _i),
+    "cufhe_memcpy_h2d": ([_vp, _vp, _sz, _vp], _i),
+    "cufhe_memcpy_d2h": ([_vp, _vp, _sz, _vp], _i),
+    "cufhe_gate": ([_i, _i, _vp, _vp, _vp, _vp, _vp], _i),
+    "cufhe_gate_copy": ([_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _i),
+    "cufhe_gate_batch": ([_vp, _i, _sz, _i, _vp, _vp, _vp, _vp, _vp], _i),
+    "cufhe_gate_batch_host": ([_vp, _i, _sz, _i, _vp, _vp, _vp, _vp, _vp], _i),
+    "cufhe_blind_rotate": ([_vp, _sz, _u32, _i, _vp, _vp, _vp], _i),
+    "cufhe_identity_keyswitch": ([_vp, _sz, _vp, _vp], _i),
+    "cufhe_last_error": ([], C.c_char_p),
+    "cufhe_kernel_launches": ([], _u64),
+    "cufhe_device_ok": ([], _i),
+}
+
+
+class KeyView(C.Structure):
+    _fields_ = [("bk", _vp), ("bk_words", _sz), ("ksk", _vp), ("ksk_words", _sz),
+                ("keybundle", _i)]
+
+
+class CufheError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib_path() -> Path:
+    return LIB / "libcufhe_b200.so"
+
+
+def load():
+    """Load the engine library (never falls back to anything else)."""
+    global _lib
+    if _lib is None:
+        path = lib_path()
+        if not path.exists():
+            raise CufheError(f"engine library {path} is not built; run "
+                             "`python -m cufhepp_b200.build` (nvcc, sm_100a)")
+        L = C.CDLL(str(path))
+        for name, (args, res) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != OK:
+        msg = load().cufhe_last_error().decode()
+        raise CufheError(f"{what}: {ERR.get(rc, rc)}: {msg}")
+
+
+def _p(a):
+    if a is None:
+        return None
+    if isinstance(a, DeviceBuffer):
+        return C.c_void_p(a.ptr)
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class DeviceBuffer:
+    """A device allocation made through cufhe_ctxt_alloc."""
+
+    def __init__(self, nbytes: int, device: int = 0):
+        p = C.c_void_p()
+        check(load().cufhe_ctxt_alloc(C.byref(p), max(int(nbytes), 4), device), "ctxt_alloc")
+        self.ptr = p.value
+        self.nbytes = int(nbytes)
+        self.device = device
+
+    def offset(self, nbytes: int) -> "DeviceView":
+        return DeviceView(self.ptr + nbytes)
+
+    def upload(self, a: np.ndarray, stream=None) -> None:
+        a = np.ascontiguousarray(a)
+        assert a.nbytes <= self.nbytes
+        check(load().cufhe_memcpy_h2d(C.c_void_p(self.ptr), _p(a), a.nbytes, stream), "h2d")
+
+    def download(self, a: np.ndarray, stream=None) -> np.ndarray:
+        assert a.flags["C_CONTIGUOUS"] and a.nbytes <= self.nbytes
+        check(load().cufhe_memcpy_d2h(_p(a), C.c_void_p(self.ptr), a.nbytes, stream), "d2h")
+        return a
+
+    def free(self):
+        if self.ptr:
+            load().cufhe_ctxt_free(C.c_void_p(self.ptr), self.device)
+            self.ptr = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class DeviceView:
+    def __init__(self, ptr: int):
+        self.ptr = ptr
+
+
+def to_device(a: np.ndarray, device: int = 0) -> DeviceBuffer:
+    a = np.ascontiguousarray(a)
+    d = DeviceBuffer(a.nbytes, device)
+    d.upload(a)
+    check(load().cufhe_synchronize(), "sync")
+    return d
+
+
+def from_device(d: DeviceBuffer, shape, dtype=np.uint32) -> np.ndarray:
+    out = np.empty(shape, dtype)
+    d.download(out)
+    check(load().cufhe_synchronize(), "sync")
+    return out
+
+
+def dptr(x):
+    if x is None:
+        return None
+    if isinstance(x, (DeviceBuffer, DeviceView)):
+        return C.c_void_p(x.ptr)
+    if isinstance(x, int):
+        return C.c_void_p(x)
+    # torch tensors and anything exposing data_ptr()
+    return C.c_void_p(x.data_ptr())
+
+
+def initialize(ek, gpus: int | None = None) -> None:
+    L = load()
+    if gpus is not None:
+        check(L.cufhe_set_gpu_num(gpus), "set_gpu_num")
+    bk = np.ascontiguousarray(ek.bk, np.uint32)
+    ksk = np.ascontiguousarray(ek.ksk, np.uint32)
+    kv = KeyView(bk.ctypes.data, bk.size, ksk.ctypes.data, ksk.size, int(ek.keybundle))
+    check(L.cufhe_initialize(C.byref(kv)), "initialize")
+
+
+def cleanup() -> None:
+    check(load().cufhe_cleanup(), "cleanup")
+
+
+def synchronize() -> None:
+    check(load().cufhe_synchronize(), "synchronize")
+
+
+def set_precision(form: int) -> None:
+    check(load().cufhe_set_precision(form), "set_precision")
+
+
+def gate_batch(gates, count: int, level: int, out, in0, in1=None, in2=None, stream=None,
+               uniform: int = 0) -> None:
+    g = None
+    if gates is not None:
+        g = np.ascontiguousarray(gates, np.int32)
+        assert g.size == count
+    check(load().cufhe_gate_batch(_p(g), uniform, count, level, dptr(out), dptr(in0), dptr(in1),
+                                  dptr(in2), stream), "gate_batch")
+
+
+def gate_batch_host(gates, level: int, in0: np.ndarray, in1=None, in2=None, stream=None,
+                    uniform: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+    words = P.TLWE1_WORDS if level == LVL1 else P.TLWE0_WORDS
+    in0 = np.ascontiguousarray(in0, np.uint32).reshape(-1, words)
+    count = in0.shape[0]
+    if out is None:
+        out = np.empty((count, words), np.uint32)
+    g = None if gates is None else np.ascontiguousarray(gates, np.int32)
+    i1 = None if in1 is None else np.ascontiguousarray(in1, np.uint32)
+    i2 = None if in2 is None else np.ascontiguousarray(in2, np.uint32)
+    check(load().cufhe_gate_batch_host(_p(g), uniform, count, level, _p(out), _p(in0), _p(i1),
+                                       _p(i2), stream), "gate_batch_host")
+    return out
+
+
+def blind_rotate(tlwe0, count: int, mu: int, steps: int, acc_out=None, tlwe_out=None,
+                 stream=None) -> None:
+    check(load().cufhe_blind_rotate(dptr(tlwe0), count, mu, steps, dptr(acc_out),
+                                    dptr(tlwe_out), stream), "blind_rotate")
+
+
+def identity_keyswitch(tlwe1, count: int, out, stream=None) -> None:
+    check(load().cufhe_identity_keyswitch(dptr(tlwe1), count, dptr(out), stream),
+          "identity_keyswitch")
+
+
+def kernel_launches() -> int:
+    return int(load().cufhe_kernel_launches())

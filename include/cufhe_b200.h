@@ -1,0 +1,180 @@
+/*
+ * cufhe_b200.h -- C-ABI of the B200 TFHE gate-bootstrapping engine.
+ *
+ * Drop-in boundary for cuFHEpp's gate API (include/cufhe_gpu.cuh:42-358 and
+ * src/cufhe_gates_gpu.cu:34-824).  The reference exposes C++ templates over
+ * TFHEpp types; this header exposes the same operations as plain C functions
+ * over pointers and sizes.  include/cufhe_gpu.hpp rebuilds the reference's
+ * C++ names (cufhe::Initialize, cufhe::Nand<P>, cufhe::Stream, ...) on top.
+ *
+ * Conventions
+ *  - Every function returns CUFHE_OK (0) or a negative CUFHE_ERR_* code; the
+ *    reference prints and exit(-1)s instead (include/error_gpu.cuh:30-66).
+ *    cufhe_last_error() describes the most recent failure.
+ *  - Ciphertexts use TFHEpp layouts: TLWE<lvl0> = uint32_t[637],
+ *    TLWE<lvl1> = uint32_t[1025], b last.
+ *  - Gate calls are asynchronous on the given stream; results are valid after
+ *    cufhe_synchronize() or once cufhe_stream_query() returns 1, as in the
+ *    reference (include/cufhe_gpu.cuh:70-76, src/cufhe_gates_gpu.cu:104-114).
+ *  - Not thread-safe, like the reference (global key state).
+ */
+#ifndef CUFHE_B200_H
+#define CUFHE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+#define CUFHE_OK 0
+#define CUFHE_ERR_ARG (-1)         /* bad argument (size, pointer, id) */
+#define CUFHE_ERR_STATE (-2)       /* not initialized / wrong key form */
+#define CUFHE_ERR_CUDA (-3)        /* CUDA runtime error */
+#define CUFHE_ERR_NOMEM (-4)       /* device or host allocation failed */
+#define CUFHE_ERR_UNSUPPORTED (-5) /* feature not available in this build */
+
+/* ---- gate ids (the 14 gates of include/cufhe_gpu.cuh:230-358) -------- */
+#define CUFHE_NAND 0
+#define CUFHE_OR 1
+#define CUFHE_ORYN 2
+#define CUFHE_ORNY 3
+#define CUFHE_AND 4
+#define CUFHE_ANDYN 5
+#define CUFHE_ANDNY 6
+#define CUFHE_NOR 7
+#define CUFHE_XOR 8
+#define CUFHE_XNOR 9
+#define CUFHE_NOT 10
+#define CUFHE_COPY 11
+#define CUFHE_MUX 12  /* out = in0 ? in1 : in2   (Mux(out, inc, in1, in0)) */
+#define CUFHE_NMUX 13 /* out = !(in0 ? in1 : in2) */
+
+/* ---- ciphertext level of a gate call -------------------------------- */
+/* CUFHE_LVL0: Ctxt<lvl0param> I/O, blind rotation then key switching
+ *             (src/cufhe_gates_gpu.cu:198-511)
+ * CUFHE_LVL1: Ctxt<lvl1param> I/O, key switching then blind rotation
+ *             (src/cufhe_gates_gpu.cu:513-824) */
+#define CUFHE_LVL0 0
+#define CUFHE_LVL1 1
+
+/* ---- external-product precision form -------------------------------- */
+#define CUFHE_FP64_FFNT 0  /* the reference's FP64 negacyclic FFNT */
+#define CUFHE_INT8_EXACT 1 /* exact INT8 tensor-core Toeplitz products */
+
+/* Evaluation key in TFHEpp layouts (stands in for TFHEpp::EvalKey):
+ *   bk : keybundle == 0 -> TRGSW<lvl1>[636]     (20,840,448 words)
+ *        keybundle == 1 -> TRGSW<lvl1>[318][3]  (31,260,672 words),
+ *        elements (s0 s1, s0 (1-s1), (1-s0) s1) of each key pair
+ *   ksk: TLWE<lvl0>[1024][7][2]                 (9,132,032 words)  */
+typedef struct cufhe_keyview {
+    const uint32_t* bk;
+    size_t bk_words;
+    const uint32_t* ksk;
+    size_t ksk_words;
+    int keybundle;
+} cufhe_keyview;
+
+typedef struct cufhe_stream_s* cufhe_stream_t; /* NULL = legacy default stream */
+
+/* ---- setup / teardown ----------------------------------------------- */
+/* SetGPUNum(int) -- include/cufhe_gpu.cuh:52, src/cufhe_gates_gpu.cu:38 */
+int cufhe_set_gpu_num(int n);
+int cufhe_get_gpu_num(void);
+
+/* Initialize(const TFHEpp::EvalKey&) -- src/cufhe_gates_gpu.cu:42-61:
+ * uploads the keys to every GPU and converts the bootstrapping key to the
+ * forms both precision paths use. */
+int cufhe_initialize(const cufhe_keyview* ek);
+
+/* CleanUp() -- src/cufhe_gates_gpu.cu:63-73 */
+int cufhe_cleanup(void);
+
+/* Synchronize() -- include/cufhe_gpu.cuh:70-76 */
+int cufhe_synchronize(void);
+
+/* Chooses the external-product form used by subsequent gate calls (the
+ * reference fixes it at compile time: CMakeLists.txt:49-62).  INT8_EXACT
+ * needs a bootstrapping key without KeyBundle. */
+int cufhe_set_precision(int form);
+int cufhe_get_precision(void);
+
+/* ---- streams (class Stream, include/cufhe_gpu.cuh:162-199) ----------- */
+/* device < 0 picks GPUs round robin, like Stream() */
+int cufhe_stream_create(cufhe_stream_t* st, int device);
+int cufhe_stream_destroy(cufhe_stream_t st);
+/* StreamQuery(Stream) -- src/cufhe_gates_gpu.cu:104-114: 1 idle, 0 busy */
+int cufhe_stream_query(cufhe_stream_t st);
+int cufhe_stream_device(cufhe_stream_t st);
+int cufhe_stream_synchronize(cufhe_stream_t st);
+
+/* ---- ciphertext buffers (Ctxt's per-GPU device buffer and pinned host
+ *      copy: include/cufhe_gpu.cuh:78-121, 203-217) -------------------- */
+int cufhe_ctxt_alloc(void** dptr, size_t bytes, int device);
+int cufhe_ctxt_free(void* dptr, int device);
+int cufhe_host_register(void* host, size_t bytes);
+int cufhe_host_unregister(void* host);
+int cufhe_memcpy_h2d(void* dst_dev, const void* src_host, size_t bytes, cufhe_stream_t st);
+int cufhe_memcpy_d2h(void* dst_host, const void* src_dev, size_t bytes, cufhe_stream_t st);
+
+/* ---- gates ------------------------------------------------------------ */
+/* One gate on device-resident ciphertexts: the reference's g* variants
+ * (gNand ... gNMux, gNot, gCopy; src/cufhe_gates_gpu.cu:212-221 and
+ * include/cufhe_gpu.cuh:243-249).  in1 is unused by Not/Copy, in2 is used by
+ * Mux/NMux only. */
+int cufhe_gate(int gate, int level, uint32_t* out, const uint32_t* in0, const uint32_t* in1,
+               const uint32_t* in2, cufhe_stream_t st);
+
+/* One gate with host ciphertexts: the copying variants (Nand ... NMux, Not,
+ * Copy; src/cufhe_gates_gpu.cu:198-210): inputs are copied host -> device,
+ * the gate runs, the output is copied back, all asynchronously on st.
+ * *_dev are the device buffers of the same ciphertexts. */
+int cufhe_gate_copy(int gate, int level, uint32_t* out_host, uint32_t* out_dev,
+                    const uint32_t* in0_host, uint32_t* in0_dev, const uint32_t* in1_host,
+                    uint32_t* in1_dev, const uint32_t* in2_host, uint32_t* in2_dev,
+                    cufhe_stream_t st);
+
+/* Batched gates (no counterpart in the reference, which launches one kernel
+ * per gate): count gates, gate ids in host memory (NULL: every gate is
+ * uniform_gate); in0/in1/in2/out are device arrays of count ciphertexts of
+ * the given level. */
+int cufhe_gate_batch(const int32_t* gates_host, int uniform_gate, size_t count, int level,
+                     uint32_t* out, const uint32_t* in0, const uint32_t* in1,
+                     const uint32_t* in2, cufhe_stream_t st);
+
+/* Same with host arrays: copies the inputs in, runs, copies the outputs
+ * back (asynchronous on st; host arrays should be pinned for overlap). */
+int cufhe_gate_batch_host(const int32_t* gates_host, int uniform_gate, size_t count, int level,
+                          uint32_t* out_host, const uint32_t* in0_host, const uint32_t* in1_host,
+                          const uint32_t* in2_host, cufhe_stream_t st);
+
+/* ---- lower-level path pieces (used by the parity tests) --------------- */
+/* Blind rotation of count lvl0 TLWEs (device [count][637]) with test
+ * polynomial mu, first `steps` CMUX steps (KeyBundle pairs) when steps >= 0;
+ * writes the TRLWE accumulators [count][2][1024] (acc_out, may be NULL) and
+ * the SampleExtract results [count][1025] (tlwe_out, may be NULL).
+ * __BlindRotate__ / __SampleExtractIndex__, include/gatebootstrapping_gpu.cuh
+ * :801-884, :1335-1380, src/bootstrap_gpu.cu:1201-1221. */
+int cufhe_blind_rotate(const uint32_t* tlwe0, size_t count, uint32_t mu, int steps,
+                       uint32_t* acc_out, uint32_t* tlwe_out, cufhe_stream_t st);
+
+/* Identity key switching lvl1 -> lvl0 of count TLWEs (device arrays):
+ * KeySwitchFromTLWE, include/keyswitch_gpu.cuh:128-187; SEIandKS,
+ * src/keyswitch_gpu.cu:52-68. */
+int cufhe_identity_keyswitch(const uint32_t* tlwe1, size_t count, uint32_t* tlwe0_out,
+                             cufhe_stream_t st);
+
+/* ---- diagnostics ----------------------------------------------------- */
+const char* cufhe_last_error(void);
+/* kernels launched by this process so far (all devices) */
+uint64_t cufhe_kernel_launches(void);
+/* 1 when the library was built for sm_100a and a device is visible */
+int cufhe_device_ok(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUFHE_B200_H */
