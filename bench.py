@@ -1,0 +1,435 @@
+#!/usr/bin/env python
+"""Throughput of lvl1 TFHE gate bootstrapping on B200 (one JSON line).
+
+A step is one batch of 4096 independent lvl1 gates drawn uniformly from
+{NAND, AND, OR, XOR, XNOR, MUX} on random bits, with Ctxt<lvl1> inputs (key
+switching, then blind rotation, then SampleExtract), through the engine's
+C-ABI.  A MUX needs two blind rotations, so the unit is bootstraps/s
+(binary gate = 1, MUX = 2).
+
+  value  device-resident inputs, CUDA events around each step (L2 flushed
+         between steps by a 256 MiB write), max over ranks
+  e2e    the same through cufhe_gate_batch_host with pinned host buffers:
+         H2D of the inputs and D2H of the outputs inside the timed region
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W]
+                       [--path fp64|int8|both] [--impl ours|reference]
+Under torchrun each rank runs its own batch on its own GPU (weak scaling, no
+data-path collective: gates are independent).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "lvl1 NAND bootstraps/sec on 1 B200: INT8-exact vs FP64-FFNT; p50 gate latency"
+UNIT = "bootstraps/s"
+GATE_SET = [0, 4, 1, 8, 9, 12]  # NAND, AND, OR, XOR, XNOR, MUX
+A100_PUBLISHED = 1.0 / 0.12e-3   # reference README: 0.12 ms/gate, lvl1 NAND FP64 + KeyBundle
+# algorithmic work per bootstrap (lvl1): FP64 FFNT flops, INT8 tensor ops
+FLOP_FP64 = {True: 287_744 * 318, False: 189_440 * 636}
+OPS_INT8 = {False: 2 * 636 * 4096 * 8192}
+WORKLOAD = ("lvl1 mixed-gate batch: 4096 independent gates uniform over "
+            "NAND/AND/OR/XOR/XNOR/MUX, Ctxt<lvl1> I/O (IKS->BR->SampleExtract), "
+            "n0=636 N=1024 l=2 Bgbit=8 IKS basebit=2 t=7, Torus32")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--path", choices=["fp64", "int8", "both"], default="fp64")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_workload(rng, batch):
+    gates = rng.choice(GATE_SET, size=batch).astype(np.int32)
+    a, b, c = (rng.integers(0, 2, batch).astype(np.uint8) for _ in range(3))
+    return gates, a, b, c
+
+
+def bootstraps(gates):
+    return int(gates.size + np.count_nonzero(gates == 12))
+
+
+# ---------------------------------------------------------------- clocks ---
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r)
+                          if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "samples": len(rows), "reasons": reasons}
+
+
+# ----------------------------------------------------------- reference arm ---
+def cpu_gate_rate(seconds, seed, sample_gates=None):
+    """Oracle port of the reference's CPU gate (FP64 FFNT restatement,
+    KeyBundle), OpenMP over gates on all host cores; bounded sample."""
+    from cufhepp_b200 import client
+    from oracle import oracle as O
+    sk = client.SecretKey.generate(seed)
+    ek = client.EvalKey.generate(sk, keybundle=True)
+    fft = O.FFT()
+    bkf = O.bk_to_fft(fft, ek.bk)
+    cores = os.cpu_count() or 1
+    n = sample_gates or max(8, cores) * 2
+    rng = np.random.default_rng(seed)
+    gates, a, b, c = make_workload(rng, n)
+    cts = [client.encrypt_bits(sk, x, 1, seed=seed + i) for i, x in enumerate((a, b, c))]
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        O.gate_batch(gates, 1, *cts, bkf, ek.ksk, True, O.FP64, fft)
+        done += bootstraps(gates)
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return done / el, cores, f"{n}-gate batches of the same mix, repeated for {el:.1f} s"
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    n = max(8, cores) * 2
+    from cufhepp_b200 import client
+    from oracle import oracle as O
+    sk = client.SecretKey.generate(args.seed)
+    ek = client.EvalKey.generate(sk, keybundle=True)
+    fft = O.FFT()
+    bkf = O.bk_to_fft(fft, ek.bk)
+    rng = np.random.default_rng(args.seed)
+    gates, a, b, c = make_workload(rng, n)
+    cts = [client.encrypt_bits(sk, x, 1, seed=args.seed + i) for i, x in enumerate((a, b, c))]
+    for _ in range(args.warmup):
+        O.gate_batch(gates, 1, *cts, bkf, ek.ksk, True, O.FP64, fft)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        O.gate_batch(gates, 1, *cts, bkf, ek.ksk, True, O.FP64, fft)
+        times.append(time.perf_counter() - t)
+    value = bootstraps(gates) * args.steps / sum(times)
+    sample = (f"{n}-gate sample of the workload's gate mix per step (FP64 FFNT, KeyBundle), "
+              f"OpenMP over gates on {cores} host threads")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded keys, random bits", "impl": "reference",
+        "config": {"workload": WORKLOAD, "gates_per_step": n, "keybundle": True,
+                   "path": "cpu: oracle port of the reference algorithm (reference not buildable: "
+                           "TFHEpp submodule absent)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------- our arm ---
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch recorded from an ncu capture in profiles/."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        m = re.search(rf"dram_bytes_per_launch\[{kernel}\]\s*=\s*([0-9.eE+]+)", f.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, flush):
+    gates, a, b, c = workload
+    kb = ek.keybundle
+    engine.initialize(ek)
+    engine.set_precision(P.FP64_FFNT if path == "fp64" else P.INT8_EXACT)
+    level = 1
+    words = P.TLWE1_WORDS
+    B = gates.size
+    cts = [client.encrypt_bits(sk, x, level, seed=args.seed + 100 * rank + i)
+           for i, x in enumerate((a, b, c))]
+    dev_in = [engine.to_device(x) for x in cts]
+    dev_out = engine.DeviceBuffer(B * words * 4)
+
+    def step():
+        engine.gate_batch(gates, B, level, dev_out, *dev_in)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    out = engine.from_device(dev_out, (B, words))
+    exp = np.array([P.TRUTH[g](int(x), int(y), int(z)) for g, x, y, z in zip(gates, a, b, c)])
+    fails = int(np.count_nonzero(client.decrypt_bits(sk, out, level) != exp))
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    engine.profile_reset()
+    engine.profile_enable(True)
+    l0 = engine.kernel_launches()
+    clk = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clk.start()
+    for k in range(args.steps):
+        ev[k][0].record()
+        step()
+        ev[k][1].record()
+        flush.zero_()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    launches = engine.kernel_launches() - l0
+    engine.profile_enable(False)
+    kern = {}
+    for cls, name in enumerate(engine.K_NAMES):
+        ms, n = engine.profile_read(cls)
+        if n:
+            kern[name] = (ms, n)
+    if ws > 1:
+        torch.distributed.barrier()
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    total = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        torch.distributed.all_reduce(total, op=torch.distributed.ReduceOp.MAX)
+    nb = bootstraps(gates)
+    value = nb * ws * args.steps / (total.item() * 1e-3)
+
+    # e2e through the C-ABI with pinned host buffers
+    host_in = [np.ascontiguousarray(x) for x in cts]
+    host_out = np.empty((B, words), np.uint32)
+    for h in host_in + [host_out]:
+        engine.check(engine.load().cufhe_host_register(engine._p(h), h.nbytes), "host_register")
+    for _ in range(2):
+        engine.gate_batch_host(gates, level, *host_in, out=host_out)
+    torch.cuda.synchronize()
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for k in range(args.steps):
+        ev2[k][0].record()
+        engine.gate_batch_host(gates, level, *host_in, out=host_out)
+        ev2[k][1].record()
+        flush.zero_()
+    torch.cuda.synchronize()
+    e2e_ms = torch.tensor([sum(e0.elapsed_time(e1) for e0, e1 in ev2)], dtype=torch.float64,
+                          device="cuda")
+    if ws > 1:
+        torch.distributed.all_reduce(e2e_ms, op=torch.distributed.ReduceOp.MAX)
+    fails += int(np.count_nonzero(client.decrypt_bits(sk, host_out, level) != exp))
+    for h in host_in + [host_out]:
+        engine.load().cufhe_host_unregister(engine._p(h))
+
+    # single-gate latency on an idle GPU (one NAND through cufhe_gate)
+    lat = []
+    L = engine.load()
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        engine.check(L.cufhe_gate(0, level, engine.dptr(dev_out), engine.dptr(dev_in[0]),
+                                  engine.dptr(dev_in[1]), None, None), "gate")
+        e1.record()
+        torch.cuda.synchronize()
+        lat.append(e0.elapsed_time(e1))
+    engine.cleanup()
+
+    br = "br_fp64" if path == "fp64" else "br_int8"
+    rl = None
+    if br in kern:
+        ms, n = kern[br]
+        per_launch_s = ms * 1e-3 / n
+        if path == "fp64":
+            work = FLOP_FP64[bool(kb)] * nb
+            peak = engine_peak_fp64(engine)
+            rl = {"bound": "fp64", "achieved": work / per_launch_s / 1e12, "peak": peak,
+                  "unit": "TFLOP/s", "frac": work / per_launch_s / 1e12 / peak,
+                  "traffic": ncu_traffic("br_fp64_kb" if kb else "br_fp64"),
+                  "kernel": "k_br_fp64 (FP64 FFNT blind rotation + SampleExtract)",
+                  "work_per_launch": work,
+                  "peak_source": "measured FP64 FMA probe on this GPU "
+                                 "(cufhe_measure_fp64_peak; the peaks file has no FP64 figure)"}
+        else:
+            work = OPS_INT8[False] * nb
+            peak = int8_peak(torch)
+            rl = {"bound": "tensor", "achieved": work / per_launch_s / 1e12, "peak": peak,
+                  "unit": "TOP/s", "frac": work / per_launch_s / 1e12 / peak,
+                  "traffic": ncu_traffic("br_int8"),
+                  "kernel": "INT8 blind rotation (decompose + tcgen05 Toeplitz GEMM per step)",
+                  "work_per_launch": work,
+                  "peak_source": "measured torch._int_mm int8 GEMM 8192^3 on this GPU"}
+    res = {
+        "value": value, "ms_per_step": total.item() / args.steps,
+        "p50_gate_latency_ms": statistics.median(step_ms),
+        "p99_gate_latency_ms": float(np.percentile(step_ms, 99)),
+        "single_gate_latency_ms": statistics.median(lat),
+        "decrypt_failures": fails, "gates_checked": 2 * B,
+        "e2e": {"value": nb * ws * args.steps / (e2e_ms.item() * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": int(sum(x.nbytes for x in cts)),
+                "d2h_bytes_per_step": int(B * words * 4)},
+        "gpu_launches": launches,
+        "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
+        "roofline": rl, "clocks": clocks, "bootstraps_per_step": nb, "keybundle": bool(kb),
+    }
+    return res
+
+
+_PEAK = {}
+
+
+def engine_peak_fp64(engine):
+    if "fp64" not in _PEAK:
+        _PEAK["fp64"] = max(engine.measure_fp64_peak() for _ in range(3))
+    return _PEAK["fp64"]
+
+
+def int8_peak(torch):
+    if "int8" not in _PEAK:
+        a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda").t()
+        for _ in range(2):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        _PEAK["int8"] = 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    return _PEAK["int8"]
+
+
+def run_ours(args):
+    ws, rank, local = dist_env()
+    if ws > 1:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    import torch
+    from cufhepp_b200 import client, engine, params as P
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    rng = np.random.default_rng(args.seed + rank)
+    workload = make_workload(rng, args.batch)
+    sk = client.SecretKey.generate(args.seed)
+    paths = ["fp64", "int8"] if args.path == "both" else [args.path]
+    results = {}
+    for p in paths:
+        ek = client.EvalKey.generate(sk, keybundle=(p == "fp64"))
+        results[p] = run_path(args, p, torch, engine, client, P, sk, ek, workload, rank, ws, flush)
+    primary = results[paths[0]]
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_gate_rate(args.cpu_seconds, args.seed)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": primary["value"], "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": primary["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if paths[0] == "fp64" else "int8",
+            "data": "synthetic: seeded keys, random bits",
+            "config": {"workload": WORKLOAD, "gates_per_step": args.batch,
+                       "bootstraps_per_step": primary["bootstraps_per_step"],
+                       "keybundle": primary["keybundle"],
+                       "path": {"fp64": "FP64 FFNT", "int8": "INT8 exact (tcgen05)"}[paths[0]],
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "parallelism": f"{ws} replica(s): independent gate batch per GPU"},
+            "p50_gate_latency_ms": primary["p50_gate_latency_ms"],
+            "p99_gate_latency_ms": primary["p99_gate_latency_ms"],
+            "single_gate_latency_ms": primary["single_gate_latency_ms"],
+            "decrypt_failures": primary["decrypt_failures"],
+            "roofline": primary["roofline"], "cpu_baseline": cpu, "e2e": primary["e2e"],
+            "gpu_launches": primary["gpu_launches"], "clocks": primary["clocks"],
+            "kernel_ms_per_step": primary["kernel_ms_per_step"],
+            "vs_reference_a100_published": primary["value"] / A100_PUBLISHED,
+        }
+        if len(paths) > 1:
+            line["paths"] = {p: {k: results[p][k] for k in
+                                 ("value", "ms_per_step", "p50_gate_latency_ms",
+                                  "single_gate_latency_ms", "decrypt_failures", "roofline",
+                                  "kernel_ms_per_step", "keybundle", "e2e", "gpu_launches")}
+                             for p in paths}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

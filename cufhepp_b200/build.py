@@ -29,6 +29,7 @@ ENGINE_SOURCES = [
     "br_fp64.cu",
     "br_int8.cu",
     "gates_misc.cu",
+    "peaks.cu",
 ]
 
 

@@ -68,6 +68,33 @@ cufhe_stream_s g_default[kMaxDev];
 char g_err[512] = "";
 std::atomic<uint64_t> g_launches{0};
 
+// optional per-kernel-class event timing (cufhe_profile_*)
+struct ProfRec {
+    cudaEvent_t a, b;
+    int cls;
+};
+bool g_prof = false;
+std::vector<ProfRec> g_prof_recs;
+double g_prof_ms[CUFHE_K_CLASSES] = {};
+uint64_t g_prof_n[CUFHE_K_CLASSES] = {};
+
+void prof_begin(cudaStream_t st, ProfRec& r, int cls)
+{
+    r.cls = cls;
+    r.a = r.b = nullptr;
+    if (!g_prof) return;
+    cudaEventCreate(&r.a);
+    cudaEventCreate(&r.b);
+    cudaEventRecord(r.a, st);
+}
+
+void prof_end(cudaStream_t st, ProfRec& r)
+{
+    if (!r.a) return;
+    cudaEventRecord(r.b, st);
+    g_prof_recs.push_back(r);
+}
+
 int fail(int code, const char* fmt, ...)
 {
     va_list ap;
@@ -89,6 +116,15 @@ int fail(int code, const char* fmt, ...)
     do {                       \
         CK(call);              \
         g_launches.fetch_add(1); \
+    } while (0)
+
+// launch one engine kernel of class `cls` on stream `st` (timed when profiling)
+#define LAUNCH(cls, st, call)      \
+    do {                           \
+        ProfRec pr_;               \
+        prof_begin((st), pr_, (cls)); \
+        CKL(call);                 \
+        prof_end((st), pr_);       \
     } while (0)
 
 void free_ws(Workspace& w)
@@ -283,14 +319,18 @@ int run_br(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint32_t mu, i
         if (D.kb || !D.i8.ready)
             return fail(CUFHE_ERR_STATE, "INT8_EXACT needs a bootstrapping key without KeyBundle");
         int launches = 0;
+        ProfRec pr;
+        prof_begin(s->st, pr, CUFHE_K_BR_INT8);
         cudaError_t e = launch_br_int8(D.i8, s->ws.i8, lane_in, lanes, mu, steps, acc_out,
                                        lane_out, s->st, &launches);
+        prof_end(s->st, pr);
         g_launches.fetch_add(launches);
         if (e != cudaSuccess) return fail(CUFHE_ERR_CUDA, "INT8 blind rotation: %s", cudaGetErrorString(e));
         return CUFHE_OK;
     }
     const Fp64Tables t = {D.psi, D.tw512};
-    CKL(launch_br_fp64(D.kb != 0, lane_in, lanes, mu, D.bkf, t, steps, acc_out, lane_out, s->st));
+    LAUNCH(CUFHE_K_BR_FP64, s->st,
+           launch_br_fp64(D.kb != 0, lane_in, lanes, mu, D.bkf, t, steps, acc_out, lane_out, s->st));
     return CUFHE_OK;
 }
 
@@ -321,22 +361,26 @@ int run_batch(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count
     Workspace& w = s->ws;
     if (plan.lanes) {
         if (level == CUFHE_LVL1)
-            CKL(launch_iks(0, plan, in0, in1, in2, nullptr, D.ksk, w.lane_in, s->st));
+            LAUNCH(CUFHE_K_IKS, s->st,
+                   launch_iks(0, plan, in0, in1, in2, nullptr, D.ksk, w.lane_in, s->st));
         else
-            CKL(launch_preadd_lvl0(plan, in0, in1, in2, w.lane_in, s->st));
+            LAUNCH(CUFHE_K_PREADD, s->st, launch_preadd_lvl0(plan, in0, in1, in2, w.lane_in, s->st));
         rc = run_br(s, w.lane_in, plan.lanes, kMu, -1, nullptr, w.lane_out);
         if (rc) return rc;
         if (level == CUFHE_LVL1)
-            CKL(launch_finalize_lvl1(plan, w.lane_out, out, s->st));
+            LAUNCH(CUFHE_K_FINALIZE, s->st, launch_finalize_lvl1(plan, w.lane_out, out, s->st));
         else
-            CKL(launch_iks(1, plan, nullptr, nullptr, nullptr, w.lane_out, D.ksk, out, s->st));
+            LAUNCH(CUFHE_K_IKS, s->st,
+                   launch_iks(1, plan, nullptr, nullptr, nullptr, w.lane_out, D.ksk, out, s->st));
     }
     const bool any_nc = gates ? true : (uniform == kNot || uniform == kCopy);
     if (any_nc) {
         bool has = !gates;
         for (size_t b = 0; gates && b < count && !has; b++)
             has = gates[b] == kNot || gates[b] == kCopy;
-        if (has) CKL(launch_not_copy(plan, level == CUFHE_LVL1 ? kTlwe1 : kTlwe0, in0, out, s->st));
+        if (has)
+            LAUNCH(CUFHE_K_FINALIZE, s->st,
+                   launch_not_copy(plan, level == CUFHE_LVL1 ? kTlwe1 : kTlwe0, in0, out, s->st));
     }
     return CUFHE_OK;
 }
@@ -599,8 +643,49 @@ int cufhe_identity_keyswitch(const uint32_t* tlwe1, size_t count, uint32_t* tlwe
     // mode 1 reads the inputs as lane outputs; a binary gate id gives one lane
     // per input and the identity combination (1, 0, 0)
     plan.uniform_op = kAnd;
-    CKL(launch_iks(1, plan, nullptr, nullptr, nullptr, tlwe1, g_dev[s->device].ksk, tlwe0_out,
-                   s->st));
+    LAUNCH(CUFHE_K_IKS, s->st,
+           launch_iks(1, plan, nullptr, nullptr, nullptr, tlwe1, g_dev[s->device].ksk, tlwe0_out,
+                      s->st));
+    return CUFHE_OK;
+}
+
+int cufhe_profile_enable(int on)
+{
+    g_prof = on != 0;
+    return CUFHE_OK;
+}
+
+int cufhe_profile_reset(void)
+{
+    for (auto& r : g_prof_recs) {
+        cudaEventSynchronize(r.b);
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    g_prof_recs.clear();
+    for (int i = 0; i < CUFHE_K_CLASSES; i++) {
+        g_prof_ms[i] = 0;
+        g_prof_n[i] = 0;
+    }
+    return CUFHE_OK;
+}
+
+int cufhe_profile_read(int cls, double* total_ms, uint64_t* launches)
+{
+    if (cls < 0 || cls >= CUFHE_K_CLASSES || !total_ms || !launches)
+        return fail(CUFHE_ERR_ARG, "bad profile query");
+    for (auto& r : g_prof_recs) {
+        CK(cudaEventSynchronize(r.b));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, r.a, r.b));
+        g_prof_ms[r.cls] += ms;
+        g_prof_n[r.cls] += 1;
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    g_prof_recs.clear();
+    *total_ms = g_prof_ms[cls];
+    *launches = g_prof_n[cls];
     return CUFHE_OK;
 }
 

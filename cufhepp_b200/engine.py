@@ -49,7 +49,14 @@ SIGNATURES = {
     "cufhe_last_error": ([], C.c_char_p),
     "cufhe_kernel_launches": ([], _u64),
     "cufhe_device_ok": ([], _i),
+    "cufhe_profile_enable": ([_i], _i),
+    "cufhe_profile_reset": ([], _i),
+    "cufhe_profile_read": ([_i, _vp, _vp], _i),
+    "cufhe_measure_fp64_peak": ([_vp], _i),
 }
+
+K_IKS, K_PREADD, K_BR_FP64, K_BR_INT8, K_FINALIZE = range(5)
+K_NAMES = ["iks", "preadd", "br_fp64", "br_int8", "finalize"]
 
 
 class KeyView(C.Structure):
@@ -222,6 +229,27 @@ def blind_rotate(tlwe0, count: int, mu: int, steps: int, acc_out=None, tlwe_out=
 def identity_keyswitch(tlwe1, count: int, out, stream=None) -> None:
     check(load().cufhe_identity_keyswitch(dptr(tlwe1), count, dptr(out), stream),
           "identity_keyswitch")
+
+
+def profile_enable(on: bool = True) -> None:
+    check(load().cufhe_profile_enable(int(on)), "profile_enable")
+
+
+def profile_reset() -> None:
+    check(load().cufhe_profile_reset(), "profile_reset")
+
+
+def profile_read(cls: int) -> tuple[float, int]:
+    ms = C.c_double()
+    n = C.c_uint64()
+    check(load().cufhe_profile_read(cls, C.byref(ms), C.byref(n)), "profile_read")
+    return ms.value, n.value
+
+
+def measure_fp64_peak() -> float:
+    t = C.c_double()
+    check(load().cufhe_measure_fp64_peak(C.byref(t)), "measure_fp64_peak")
+    return t.value
 
 
 def kernel_launches() -> int:

@@ -167,6 +167,22 @@ int cufhe_identity_keyswitch(const uint32_t* tlwe1, size_t count, uint32_t* tlwe
                              cufhe_stream_t st);
 
 /* ---- diagnostics ----------------------------------------------------- */
+/* Per-kernel timing: when enabled, every engine kernel launch is bracketed
+ * by CUDA events on its stream; cufhe_profile_read() sums the durations of
+ * one kernel class (waits for the recorded events).  Classes: */
+#define CUFHE_K_IKS 0        /* identity key switching */
+#define CUFHE_K_PREADD 1     /* lvl0 pre-add (BR->IKS order) */
+#define CUFHE_K_BR_FP64 2    /* FP64 FFNT blind rotation + SampleExtract */
+#define CUFHE_K_BR_INT8 3    /* INT8 exact blind rotation step kernels */
+#define CUFHE_K_FINALIZE 4   /* lane combination (Mux) and Not/Copy */
+#define CUFHE_K_CLASSES 5
+int cufhe_profile_enable(int on);
+int cufhe_profile_reset(void);
+int cufhe_profile_read(int kernel_class, double* total_ms, uint64_t* launches);
+/* FP64 FMA throughput of the current device in TFLOP/s (roof of the FFNT
+ * path; runs a short probe kernel) */
+int cufhe_measure_fp64_peak(double* tflops);
+
 const char* cufhe_last_error(void);
 /* kernels launched by this process so far (all devices) */
 uint64_t cufhe_kernel_launches(void);
