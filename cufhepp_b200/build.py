@@ -30,6 +30,7 @@ ENGINE_SOURCES = [
     "br_int8.cu",
     "gates_misc.cu",
     "peaks.cu",
+    "noalloc.cu",
 ]
 
 

@@ -386,6 +386,25 @@ int run_batch(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count
 }
 
 }  // namespace
+
+int engine_view(void* st, EngineView* v)
+{
+    cufhe_stream_s* s = resolve(static_cast<cufhe_stream_t>(st));
+    const DeviceState& D = g_dev[s->device];
+    if (!D.ready) return fail(CUFHE_ERR_STATE, "cufhe_initialize() not called");
+    v->device = s->device;
+    v->stream = s->st;
+    v->keybundle = D.kb;
+    v->ksk = D.ksk;
+    v->bkf = D.bkf;
+    v->tables = {D.psi, D.tw512};
+    return CUFHE_OK;
+}
+
+int engine_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+
+void engine_count_launches(int n) { g_launches.fetch_add(n); }
+
 }  // namespace cufhe
 
 using namespace cufhe;

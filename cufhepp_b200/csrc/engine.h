@@ -163,4 +163,21 @@ cudaError_t launch_bk_to_fft(const uint32_t* bk, int npolys, const Fp64Tables& t
                              cudaStream_t st);
 cudaError_t upload_fft_constants(void);
 
+// Read-only view of the engine state that a gate call on stream `st` uses
+// (keys of the stream's device and the CUDA stream).  Returns 0 or a
+// CUFHE_ERR_* code (and sets the last error).
+struct EngineView {
+    int device;
+    cudaStream_t stream;
+    int keybundle;
+    const uint32_t* ksk;
+    const double2* bkf;
+    Fp64Tables tables;
+};
+int engine_view(void* st, EngineView* v);
+// sets the message returned by cufhe_last_error() and returns code
+int engine_fail(int code, const char* msg);
+// counts kernel launches reported by cufhe_kernel_launches()
+void engine_count_launches(int n);
+
 }  // namespace cufhe

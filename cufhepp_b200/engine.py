@@ -44,6 +44,7 @@ SIGNATURES = {
     "cufhe_gate_copy": ([_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], _i),
     "cufhe_gate_batch": ([_vp, _i, _sz, _i, _vp, _vp, _vp, _vp, _vp], _i),
     "cufhe_gate_batch_host": ([_vp, _i, _sz, _i, _vp, _vp, _vp, _vp, _vp], _i),
+    "cufhe_gate_batch_noalloc": ([_i, _sz, _i, _vp, _vp, _vp, _vp, _vp], _i),
     "cufhe_blind_rotate": ([_vp, _sz, _u32, _i, _vp, _vp, _vp], _i),
     "cufhe_identity_keyswitch": ([_vp, _sz, _vp, _vp], _i),
     "cufhe_last_error": ([], C.c_char_p),

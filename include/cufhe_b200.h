@@ -150,6 +150,26 @@ int cufhe_gate_batch_host(const int32_t* gates_host, int uniform_gate, size_t co
                           uint32_t* out_host, const uint32_t* in0_host, const uint32_t* in1_host,
                           const uint32_t* in2_host, cufhe_stream_t st);
 
+/* Batched uniform gates that allocate no device memory.  This entry point
+ * has no counterpart in the reference.  It is for callers that cannot let
+ * the library allocate: services with a device-memory budget fixed at start,
+ * hosts whose own allocator owns all device memory, and latency-critical
+ * code that cannot absorb the synchronisation an allocation may cause.
+ * cufhe_gate_batch grows a per-stream workspace with cudaMalloc; this one
+ * keeps its lane buffers in a fixed array compiled into the library (about
+ * 1.7 MB on every GPU that loads it, held until exit) and therefore accepts
+ * at most 256 blind rotations per call (256 binary gates or 128 Mux/NMux);
+ * larger calls return CUFHE_ERR_ARG.  Always uses the FP64 FFNT form.
+ * Arguments as cufhe_gate_batch with every gate equal to `gate`; the caller
+ * passes device inputs and outputs.  The first call on a device looks up the
+ * array's device address, so make it before any stream capture.  All calls
+ * share the array: calls whose work overlaps on the GPU race and corrupt
+ * each other's results, so keep them on one stream or synchronise between
+ * them. */
+int cufhe_gate_batch_noalloc(int gate, size_t count, int level, uint32_t* out,
+                             const uint32_t* in0, const uint32_t* in1, const uint32_t* in2,
+                             cufhe_stream_t st);
+
 /* ---- lower-level path pieces (used by the parity tests) --------------- */
 /* Blind rotation of count lvl0 TLWEs (device [count][637]) with test
  * polynomial mu, first `steps` CMUX steps (KeyBundle pairs) when steps >= 0;

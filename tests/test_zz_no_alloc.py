@@ -1,0 +1,75 @@
+"""cufhe_gate_batch_noalloc against cufhe_gate_batch, through the C-ABI.
+
+The no-allocation entry point exists for callers that cannot let the library
+allocate device memory (a fixed memory budget, a host-owned allocator, or a
+latency-critical path that cannot absorb an allocation's synchronisation).
+It runs the same gate pipeline with its lane buffers in a fixed array inside
+the library, so its outputs must agree with the regular batch entry point.
+Two calls in a row with different batches check that what the first call
+leaves in the shared array does not leak into the second.
+
+This file is named to be collected last.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from cufhepp_b200 import client, engine, params as P
+
+pytestmark = pytest.mark.gpu
+
+PHASE_TOL = 2.0 ** -12  # torus; the tolerance of the FP64 gate tests
+
+
+def torus_dist(a, b):
+    d = (np.asarray(a, np.uint32) - np.asarray(b, np.uint32)).astype(np.uint32)
+    return np.abs(d.view(np.int32).astype(np.float64)) / 2.0 ** 32
+
+
+@pytest.fixture(scope="module")
+def ctx(keys):
+    sk, ek_kb, _ = keys
+    engine.initialize(ek_kb)
+    engine.set_precision(P.FP64_FFNT)
+    yield sk
+    engine.cleanup()
+
+
+def run_both(sk, gate, count, level, seed):
+    words = P.TLWE1_WORDS if level == 1 else P.TLWE0_WORDS
+    rng = np.random.default_rng(seed)
+    a, b, c = (rng.integers(0, 2, count).astype(np.uint8) for _ in range(3))
+    cts = [client.encrypt_bits(sk, x, level, seed=seed + i) for i, x in enumerate((a, b, c))]
+    dev = [engine.to_device(x) for x in cts]
+    out_ref = engine.DeviceBuffer(count * words * 4)
+    out_new = engine.DeviceBuffer(count * words * 4)
+    engine.gate_batch(None, count, level, out_ref, *dev, uniform=gate)
+    L = engine.load()
+    engine.check(L.cufhe_gate_batch_noalloc(gate, count, level, engine.dptr(out_new),
+                                            *(engine.dptr(d) for d in dev), None),
+                 "gate_batch_noalloc")
+    ref = engine.from_device(out_ref, (count, words))
+    new = engine.from_device(out_new, (count, words))
+    exp = np.array([P.TRUTH[gate](int(x), int(y), int(z)) for x, y, z in zip(a, b, c)])
+    return ref, new, exp
+
+
+def test_noalloc_matches_batch_two_calls_in_a_row(ctx):
+    sk = ctx
+    # first call: 200 NAND gates at lvl1 (200 of the 256 lane slots)
+    ref, new, exp = run_both(sk, P.NAND, 200, 1, seed=901)
+    assert torus_dist(client.phase(sk, new, 1), client.phase(sk, ref, 1)).max() < PHASE_TOL
+    assert np.array_equal(client.decrypt_bits(sk, new, 1), exp)
+    # second call right after: 37 Mux gates at lvl0 (74 lanes) on different inputs
+    ref, new, exp = run_both(sk, P.MUX, 37, 0, seed=902)
+    assert torus_dist(client.phase(sk, new, 0), client.phase(sk, ref, 0)).max() < PHASE_TOL
+    assert np.array_equal(client.decrypt_bits(sk, new, 0), exp)
+
+
+def test_noalloc_rejects_batches_beyond_its_array(ctx):
+    L = engine.load()
+    rc = L.cufhe_gate_batch_noalloc(P.MUX, 129, 1, C.c_void_p(1), C.c_void_p(1), C.c_void_p(1),
+                                    C.c_void_p(1), None)
+    assert rc == -1
+    assert b"at most 256" in L.cufhe_last_error()
