@@ -17,6 +17,7 @@ struct Int8Workspace {
     uint32_t* acc = nullptr;
     int8_t* digits = nullptr;
     uint16_t* abar = nullptr;
+    int* err = nullptr;   // set by a kernel whose bounded wait gave up
 };
 
 cudaError_t int8_key_build(Int8Key& k, const uint32_t* bk_dev, cudaStream_t st);

@@ -1,0 +1,77 @@
+"""GPU parity of the exact INT8 tensor-core path (tcgen05), through the C-ABI.
+
+The external product runs as INT8 Toeplitz GEMMs on byte limbs with INT32
+accumulation, so the whole blind rotation -- and with the integer key switch,
+the whole gate -- must be bit-identical to the exact schoolbook oracle.
+"""
+import numpy as np
+import pytest
+
+from cufhepp_b200 import client, engine, params as P
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(keys):
+    sk, _, ek = keys  # INT8 exact form uses the plain (non-KeyBundle) key
+    engine.initialize(ek)
+    engine.set_precision(P.INT8_EXACT)
+    yield sk, ek
+    engine.set_precision(P.FP64_FFNT)
+    engine.cleanup()
+
+
+def rotate(x, steps, count):
+    d_in = engine.to_device(x)
+    d_acc = engine.DeviceBuffer(count * P.TRLWE1_WORDS * 4)
+    engine.blind_rotate(d_in, count, P.MU32, steps, acc_out=d_acc)
+    return engine.from_device(d_acc, (count, P.TRLWE1_WORDS))
+
+
+def lvl0(sk, count, seed):
+    rng = np.random.default_rng(seed)
+    bits = rng.integers(0, 2, count).astype(np.uint8)
+    return bits, client.encrypt_bits(sk, bits, 0, seed=seed)
+
+
+@pytest.mark.parametrize("steps", [1, 2, 7])
+def test_int8_steps_bit_exact(ctx, steps):
+    sk, ek = ctx
+    _, x = lvl0(sk, 8, 100 + steps)
+    got = rotate(x, steps, 8)
+    ref = O.blind_rotate(x, P.MU32, ek.bk, False, O.EXACT, steps=steps)
+    assert np.array_equal(got, ref)
+
+
+def test_int8_two_lane_groups_bit_exact(ctx):
+    sk, ek = ctx
+    # 300 lanes span two 256-lane MMA groups (the second one partial)
+    _, x = lvl0(sk, 300, 7)
+    got = rotate(x, 2, 300)
+    ref = O.blind_rotate(x, P.MU32, ek.bk, False, O.EXACT, steps=2)
+    assert np.array_equal(got, ref)
+
+
+def test_int8_full_rotation_bit_exact(ctx):
+    sk, ek = ctx
+    bits, x = lvl0(sk, 4, 8)
+    got = rotate(x, -1, 4)
+    ref = O.blind_rotate(x, P.MU32, ek.bk, False, O.EXACT)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("level", [1, 0])
+def test_int8_gates_bit_exact(ctx, level):
+    sk, ek = ctx
+    gates = np.array([P.NAND, P.AND, P.OR, P.XOR, P.XNOR, P.MUX, P.NMUX, P.NOT], np.int32)
+    rng = np.random.default_rng(50 + level)
+    a, b, c = (rng.integers(0, 2, gates.size).astype(np.uint8) for _ in range(3))
+    cts = [client.encrypt_bits(sk, x, level, seed=60 + i) for i, x in enumerate((a, b, c))]
+    out = engine.gate_batch_host(gates, level, *cts)
+    engine.synchronize()
+    ref = O.gate_batch(gates, level, *cts, ek.bk, ek.ksk, False, O.EXACT)
+    assert np.array_equal(out, ref)
+    exp = np.array([P.TRUTH[g](int(x), int(y), int(z)) for g, x, y, z in zip(gates, a, b, c)])
+    assert np.array_equal(client.decrypt_bits(sk, out, level), exp)
