@@ -1,0 +1,57 @@
+"""Runs one engine stage on seeded synthetic inputs, for profilers.
+
+    python -m cufhepp_b200.kernel_driver br_fp64 LANES [REPS]   # FP64 blind rotation (KeyBundle)
+    python -m cufhepp_b200.kernel_driver br_int8 LANES [REPS] [STEPS]  # INT8 exact rotation
+    python -m cufhepp_b200.kernel_driver iks LANES [REPS]       # identity key switching
+    python -m cufhepp_b200.kernel_driver gates LANES [REPS]     # full mixed-gate batch (lvl1)
+
+Each stage is launched REPS times on LANES inputs, so a capture can skip the
+first (cold) launch.  Prints one line and exits 0.
+"""
+from __future__ import annotations
+
+import sys
+
+import numpy as np
+
+from . import client, engine, params as P
+
+
+def main(argv: list[str]) -> None:
+    stage = argv[0]
+    lanes = int(argv[1])
+    reps = int(argv[2]) if len(argv) > 2 else 2
+    sk = client.SecretKey.generate(5)
+    ek = client.EvalKey.generate(sk, keybundle=(stage != "br_int8"))
+    engine.initialize(ek)
+    rng = np.random.default_rng(1)
+    bits = rng.integers(0, 2, lanes).astype(np.uint8)
+    if stage in ("br_fp64", "br_int8"):
+        engine.set_precision(P.FP64_FFNT if stage == "br_fp64" else P.INT8_EXACT)
+        steps = int(argv[3]) if len(argv) > 3 else -1
+        x = client.encrypt_bits(sk, bits, 0, seed=3)
+        d_in = engine.to_device(x)
+        d_out = engine.DeviceBuffer(lanes * P.TLWE1_WORDS * 4)
+        for _ in range(reps):
+            engine.blind_rotate(d_in, lanes, P.MU32, steps, tlwe_out=d_out)
+    elif stage == "iks":
+        x = client.encrypt_bits(sk, bits, 1, seed=3)
+        d_in = engine.to_device(x)
+        d_out = engine.DeviceBuffer(lanes * P.TLWE0_WORDS * 4)
+        for _ in range(reps):
+            engine.identity_keyswitch(d_in, lanes, d_out)
+    elif stage == "gates":
+        gates = rng.choice([P.NAND, P.AND, P.OR, P.XOR, P.XNOR, P.MUX], size=lanes).astype(np.int32)
+        cts = [engine.to_device(client.encrypt_bits(sk, bits, 1, seed=3 + i)) for i in range(3)]
+        d_out = engine.DeviceBuffer(lanes * P.TLWE1_WORDS * 4)
+        for _ in range(reps):
+            engine.gate_batch(gates, lanes, 1, d_out, *cts)
+    else:
+        raise SystemExit(f"unknown stage {stage}")
+    engine.synchronize()
+    engine.cleanup()
+    print(f"ok {stage} lanes={lanes} reps={reps}")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])
