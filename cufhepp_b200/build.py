@@ -26,6 +26,7 @@ GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 ENGINE_SOURCES = [
     "engine.cu",
     "keyswitch.cu",
+    "iks_tc.cu",
     "br_fp64.cu",
     "br_int8.cu",
     "gates_misc.cu",

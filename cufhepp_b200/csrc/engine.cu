@@ -32,6 +32,8 @@ struct DeviceState {
     double2* psi = nullptr;
     double2* tw512 = nullptr;
     Int8Key i8;              // INT8 exact-path key (non-KeyBundle only)
+    uint8_t* iks_key = nullptr;  // KSK as signed byte-limb tiles (tensor-core IKS)
+    int* err = nullptr;          // set by a device wait that timed out
 };
 
 struct Workspace {
@@ -46,6 +48,7 @@ struct Workspace {
     unsigned char* stage = nullptr;  // pinned host staging for plan uploads
     cudaEvent_t stage_ev = nullptr;
     Int8Workspace i8;
+    IksWorkspace iks;
 };
 
 }  // namespace
@@ -139,6 +142,7 @@ void free_ws(Workspace& w)
     if (w.stage) cudaFreeHost(w.stage);
     if (w.stage_ev) cudaEventDestroy(w.stage_ev);
     int8_workspace_free(w.i8);
+    iks_tc_workspace_free(w.iks);
     w = Workspace();
 }
 
@@ -207,6 +211,8 @@ void release_device(int d)
     cudaFree(D.bkf);
     cudaFree(D.psi);
     cudaFree(D.tw512);
+    cudaFree(D.iks_key);
+    cudaFree(D.err);
     int8_key_free(D.i8);
     D = DeviceState();
     free_ws(g_default[d].ws);
@@ -226,6 +232,10 @@ int init_device(int d, const cufhe_keyview* ek)
 
     CK(cudaMalloc(&D.ksk, ek->ksk_words * sizeof(uint32_t)));
     CK(cudaMemcpy(D.ksk, ek->ksk, ek->ksk_words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&D.iks_key, iks_tc_key_bytes()));
+    CKL(iks_tc_key_build(D.ksk, D.iks_key, 0));
+    CK(cudaMalloc(&D.err, sizeof(int)));
+    CK(cudaMemset(D.err, 0, sizeof(int)));
 
     uint32_t* raw = nullptr;
     CK(cudaMalloc(&raw, ek->bk_words * sizeof(uint32_t)));
@@ -310,6 +320,36 @@ int build_plan(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t coun
     return CUFHE_OK;
 }
 
+// identity key switching of lanes (mode 0) or gates (mode 1) on the tensor cores
+int run_iks(cufhe_stream_s* s, int mode, const Plan& plan, const uint32_t* in0, const uint32_t* in1,
+            const uint32_t* in2, const uint32_t* lane_out, uint32_t* dst)
+{
+    DeviceState& D = g_dev[s->device];
+    int launches = 0;
+    ProfRec pr;
+    prof_begin(s->st, pr, CUFHE_K_IKS);
+    cudaError_t e = launch_iks_tc(mode, plan, in0, in1, in2, lane_out, D.iks_key, dst, s->ws.iks,
+                                  D.err, s->st, &launches);
+    prof_end(s->st, pr);
+    g_launches.fetch_add(launches);
+    if (e != cudaSuccess) return fail(CUFHE_ERR_CUDA, "key switching: %s", cudaGetErrorString(e));
+    return CUFHE_OK;
+}
+
+// reports (and clears) a device-side wait timeout recorded on device d
+int check_device_error(int d)
+{
+    DeviceState& D = g_dev[d];
+    if (!D.ready || !D.err) return CUFHE_OK;
+    int h = 0;
+    CK(cudaMemcpy(&h, D.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        cudaMemset(D.err, 0, sizeof(int));
+        return fail(CUFHE_ERR_CUDA, "a tensor-core kernel's bounded wait timed out (code %d)", h);
+    }
+    return CUFHE_OK;
+}
+
 // blind rotation of plan.lanes lanes with the selected precision form
 int run_br(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint32_t mu, int steps,
            uint32_t* acc_out, uint32_t* lane_out)
@@ -360,18 +400,19 @@ int run_batch(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count
     DeviceState& D = g_dev[s->device];
     Workspace& w = s->ws;
     if (plan.lanes) {
-        if (level == CUFHE_LVL1)
-            LAUNCH(CUFHE_K_IKS, s->st,
-                   launch_iks(0, plan, in0, in1, in2, nullptr, D.ksk, w.lane_in, s->st));
-        else
+        if (level == CUFHE_LVL1) {
+            rc = run_iks(s, 0, plan, in0, in1, in2, nullptr, w.lane_in);
+            if (rc) return rc;
+        } else
             LAUNCH(CUFHE_K_PREADD, s->st, launch_preadd_lvl0(plan, in0, in1, in2, w.lane_in, s->st));
         rc = run_br(s, w.lane_in, plan.lanes, kMu, -1, nullptr, w.lane_out);
         if (rc) return rc;
-        if (level == CUFHE_LVL1)
+        if (level == CUFHE_LVL1) {
             LAUNCH(CUFHE_K_FINALIZE, s->st, launch_finalize_lvl1(plan, w.lane_out, out, s->st));
-        else
-            LAUNCH(CUFHE_K_IKS, s->st,
-                   launch_iks(1, plan, nullptr, nullptr, nullptr, w.lane_out, D.ksk, out, s->st));
+        } else {
+            rc = run_iks(s, 1, plan, nullptr, nullptr, nullptr, w.lane_out, out);
+            if (rc) return rc;
+        }
     }
     const bool any_nc = gates ? true : (uniform == kNot || uniform == kCopy);
     if (any_nc) {
@@ -462,6 +503,8 @@ int cufhe_synchronize(void)
     for (int d = 0; d < g_gpu_num; d++) {
         CK(cudaSetDevice(d));
         CK(cudaDeviceSynchronize());
+        const int rc = check_device_error(d);
+        if (rc) return rc;
     }
     return CUFHE_OK;
 }
@@ -522,7 +565,7 @@ int cufhe_stream_synchronize(cufhe_stream_t st)
     cufhe_stream_s* s = resolve(st);
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->st));
-    return CUFHE_OK;
+    return check_device_error(s->device);
 }
 
 int cufhe_ctxt_alloc(void** dptr, size_t bytes, int device)
@@ -662,10 +705,7 @@ int cufhe_identity_keyswitch(const uint32_t* tlwe1, size_t count, uint32_t* tlwe
     // mode 1 reads the inputs as lane outputs; a binary gate id gives one lane
     // per input and the identity combination (1, 0, 0)
     plan.uniform_op = kAnd;
-    LAUNCH(CUFHE_K_IKS, s->st,
-           launch_iks(1, plan, nullptr, nullptr, nullptr, tlwe1, g_dev[s->device].ksk, tlwe0_out,
-                      s->st));
-    return CUFHE_OK;
+    return run_iks(s, 1, plan, nullptr, nullptr, nullptr, tlwe1, tlwe0_out);
 }
 
 int cufhe_profile_enable(int on)

@@ -163,6 +163,23 @@ cudaError_t launch_bk_to_fft(const uint32_t* bk, int npolys, const Fp64Tables& t
                              cudaStream_t st);
 cudaError_t upload_fft_constants(void);
 
+// Tensor-core identity key switching (iks_tc.cu).  Key tiles are built once
+// per device from the raw KSK; the workspace holds per-batch one-hot digit
+// tiles.  A timed-out device wait sets *err (checked at synchronisation).
+struct IksWorkspace {
+    size_t cap = 0;  // units
+    uint8_t* atiles = nullptr;
+    uint32_t* xb = nullptr;
+    int* valid = nullptr;
+};
+size_t iks_tc_key_bytes();
+cudaError_t iks_tc_key_build(const uint32_t* ksk_dev, uint8_t* key_tiles, cudaStream_t st);
+void iks_tc_workspace_free(IksWorkspace& w);
+cudaError_t launch_iks_tc(int mode, const Plan& plan, const uint32_t* in0, const uint32_t* in1,
+                          const uint32_t* in2, const uint32_t* lane_out, const uint8_t* key_tiles,
+                          uint32_t* dst, IksWorkspace& w, int* err, cudaStream_t st,
+                          int* launches);
+
 // Read-only view of the engine state that a gate call on stream `st` uses
 // (keys of the stream's device and the CUDA stream).  Returns 0 or a
 // CUFHE_ERR_* code (and sets the last error).

@@ -1,0 +1,313 @@
+// Identity key switching lvl1 -> lvl0 on the tensor cores (integer,
+// bit-exact).
+//
+// IdentityKeySwitchPreAdd / KeySwitchFromTLWE (include/keyswitch_gpu.cuh:
+// 128-256) compute, for x = ca*A + cb*B (+off on b),
+//   res[o] = [o == n0] x_b + sum_{i < 1024, j < 7} c(v_ij) . KSK[i][j][.][o]
+// with digits v_ij in [-2, 1]: v = -1 adds KSK[i][j][0], v = +1 subtracts it,
+// v = -2 adds KSK[i][j][1].  Written over K = (i, j, e) with e in {0, 1} this
+// is an exact GEMM with a one-hot operand:
+//   A[gate][k] in {-1, 0, +1}  (per gate, from the digits)
+//   B[k][(o, c)] = limb_c(KSK[k][o])  (balanced signed bytes, shared by all gates)
+//   res[o] = x_b[o == n0] + sum_c (A B_c)[o] << 8c   mod 2^32
+// K = 14336, |sum| <= 7168 * 128, so INT32 accumulation is exact.
+//
+// The SIMT kernel in keyswitch.cu spends ~800 K integer instructions per key
+// switch; here one 128-gate x 256-column tile is 448 tcgen05.mma.kind::i8
+// (M = 128, N = 256, K = 32) with both operands streamed from pre-swizzled
+// tiles by cp.async.bulk through a 4-stage shared-memory ring, INT32
+// accumulators in TMEM, and the limb recombination in the epilogue.
+#include "engine.h"
+#include "tc_util.cuh"
+
+namespace cufhe {
+
+namespace {
+
+constexpr int kT = CUFHE_LVL10_T;
+constexpr int kK = kN * kT * 2;             // 14336
+constexpr int kChunkK = 128;
+constexpr int kChunks = kK / kChunkK;       // 112
+constexpr int kMGates = 128;                // gates per tile (M)
+constexpr int kNCols = 256;                 // 64 outputs x 4 limbs per tile (N)
+constexpr int kOutPerTile = kNCols / 4;     // 64
+constexpr int kNTiles = (kTlwe0 + kOutPerTile - 1) / kOutPerTile;  // 10
+constexpr int kATile = kMGates * kChunkK;   // 16 KB
+constexpr int kBTile = kNCols * kChunkK;    // 32 KB
+constexpr int kStageBytes = kATile + kBTile;
+constexpr int kStages = 4;
+constexpr size_t kSmem = 1024 + (size_t)kStages * kStageBytes + 256;
+constexpr uint32_t kIdescIks = idesc_i8(kMGates, kNCols);
+constexpr uint32_t kTmemColsIks = 256;
+
+__host__ __device__ constexpr uint32_t iks_offset_tc()
+{
+    uint32_t off = 0;
+    for (int i = 1; i <= kT; i++) off += 2u << (32 - i * CUFHE_LVL10_BASEBIT);
+    return off + (1u << (32 - (1 + CUFHE_LVL10_BASEBIT * kT)));
+}
+
+// key tiles [nt][kc][32 KB]: row = o_local * 4 + c, K-major, 128B-swizzled
+__global__ void k_iks_key(const uint32_t* __restrict__ ksk, uint8_t* __restrict__ out)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t total = (size_t)kNTiles * kChunks * kBTile / 4;
+    if (q >= total) return;
+    const size_t byte = q * 4;
+    const int tile = (int)(byte / kBTile);
+    const uint32_t w = (uint32_t)(byte % kBTile);
+    const int nt = tile / kChunks, kc = tile % kChunks;
+    const uint32_t row = (w / 1024) * 8 + (w % 1024) / 128;
+    const uint32_t kl = ((((w % 128) / 16) ^ (row & 7)) << 4) + (w % 16);
+    const int o = nt * kOutPerTile + (int)(row / 4);
+    const int c = (int)(row % 4);
+    uint32_t packed = 0;
+    for (int e = 0; e < 4; e++) {
+        const size_t k = (size_t)kc * kChunkK + kl + e;
+        const int8_t v = o < kTlwe0 ? limb(ksk[k * kTlwe0 + o], c) : (int8_t)0;
+        packed |= (uint32_t)(uint8_t)v << (8 * e);
+    }
+    reinterpret_cast<uint32_t*>(out)[q] = packed;
+}
+
+// one-hot digit tiles of unit u (a lane in mode 0, a gate in mode 1):
+// atiles[u / 128][kc][16 KB], row u % 128; xb[u] = b part; valid[u]
+__global__ void __launch_bounds__(256) k_iks_prep(int mode, Plan plan, const uint32_t* __restrict__ in0,
+                                                  const uint32_t* __restrict__ in1,
+                                                  const uint32_t* __restrict__ in2,
+                                                  const uint32_t* __restrict__ lane_out,
+                                                  uint8_t* __restrict__ atiles,
+                                                  uint32_t* __restrict__ xb, int* __restrict__ valid)
+{
+    const int u = blockIdx.x;
+    LanePreadd p = {nullptr, nullptr, 0, 0, 0};
+    int ok = 0;
+    if (mode == 0) {
+        int b, sub;
+        plan_lane(plan, u, b, sub);
+        const size_t o = (size_t)b * kTlwe1;
+        p = lane_preadd(plan_op(plan, b), sub, in0 + o, in1 ? in1 + o : nullptr,
+                        in2 ? in2 + o : nullptr);
+        ok = 1;
+    } else {
+        const int l0 = plan_lane0(plan, u);
+        if (l0 >= 0) {
+            p = gate_combine(plan_op(plan, u), lane_out + (size_t)l0 * kTlwe1,
+                             lane_out + (size_t)(l0 + 1) * kTlwe1);
+            ok = 1;
+        }
+    }
+    if (threadIdx.x == 0) {
+        uint32_t b = 0;
+        if (ok) {
+            b = (uint32_t)p.ca * p.a[kN] + p.off;
+            if (p.cb) b += (uint32_t)p.cb * p.b[kN];
+        }
+        xb[u] = b;
+        valid[u] = ok;
+    }
+    const uint32_t row = (uint32_t)(u % kMGates);
+    uint8_t* tb = atiles + (size_t)(u / kMGates) * kChunks * kATile;
+    for (int q = threadIdx.x; q < kK / 16; q += blockDim.x) {
+        // 16 bytes = 8 (i, j) pairs x (e = 0, e = 1)
+        uint32_t wv[4] = {0, 0, 0, 0};
+        int ci = -1;
+        uint32_t t = 0;
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int pr = 8 * q + e, i = pr / kT, j = pr % kT;
+            if (i != ci) {
+                ci = i;
+                uint32_t x = 0;
+                if (ok) {
+                    x = (uint32_t)p.ca * p.a[i];
+                    if (p.cb) x += (uint32_t)p.cb * p.b[i];
+                }
+                t = x + iks_offset_tc();
+            }
+            const uint32_t code = ok ? (t >> (30 - 2 * j)) & 3u : 2u;  // v = code - 2
+            const uint32_t b0 = code == 1 ? 0x01u : (code == 3 ? 0xFFu : 0u);
+            const uint32_t b1 = code == 0 ? 0x01u : 0u;
+            wv[e >> 1] |= (b0 | (b1 << 8)) << (16 * (e & 1));
+        }
+        const int k0 = 16 * q;
+        *reinterpret_cast<uint4*>(tb + (size_t)(k0 / kChunkK) * kATile +
+                                  swz_offset(row, (uint32_t)(k0 % kChunkK))) =
+            make_uint4(wv[0], wv[1], wv[2], wv[3]);
+    }
+}
+
+__global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__ atiles,
+                                                     const uint8_t* __restrict__ btiles,
+                                                     const uint32_t* __restrict__ xb,
+                                                     const int* __restrict__ valid, int units,
+                                                     uint32_t* __restrict__ dst, int* __restrict__ err)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t raw_addr = smem_u32(smem_raw);
+    unsigned char* smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)kStages * kStageBytes);
+    uint64_t* empty = full + kStages;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(empty + kStages);
+    __shared__ int s_fail;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int gt = blockIdx.x / kNTiles, nt = blockIdx.x % kNTiles;
+    const uint8_t* ga = atiles + (size_t)gt * kChunks * kATile;
+    const uint8_t* gb = btiles + (size_t)nt * kChunks * kBTile;
+    int pend[kStages] = {0, 0, 0, 0};  // thread 0: 1 + parity of an outstanding fill
+    int last_commit = -1;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(tmem_slot)), "r"(kTmemColsIks));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        s_fail = 0;
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (tid == 0) {
+        auto fill = [&](int s, int kc) {
+            unsigned char* st = smem + (size_t)s * kStageBytes;
+            mbar_expect_tx(&full[s], kStageBytes);
+            bulk_g2s(st, ga + (size_t)kc * kATile, kATile, &full[s]);
+            bulk_g2s(st + kATile, gb + (size_t)kc * kBTile, kBTile, &full[s]);
+            pend[s] = 1 + ((kc / kStages) & 1);
+        };
+        for (int s = 0; s < kStages; s++) fill(s, s);
+        for (int kc = 0; kc < kChunks; kc++) {
+            const int s = kc % kStages;
+            if (!mbar_wait(&full[s], (kc / kStages) & 1)) {
+                s_fail = 1;
+                break;
+            }
+            pend[s] = 0;
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(smem + (size_t)s * kStageBytes);
+            const uint32_t b0 = a0 + kATile;
+#pragma unroll
+            for (int k = 0; k < kChunkK / 32; k++)
+                tc_mma_i8_ss(tmem, desc_kmajor_sw128(a0 + 32 * k), desc_kmajor_sw128(b0 + 32 * k),
+                             kIdescIks, (kc | k) != 0);
+            tc_commit(&empty[s]);
+            last_commit = kc;
+            // refill the stage of chunk kc-1 with chunk kc+3 once its MMAs are done
+            if (kc >= 1 && kc + kStages - 1 < kChunks) {
+                const int sp = (kc - 1) % kStages;
+                if (!mbar_wait(&empty[sp], ((kc - 1) / kStages) & 1)) {
+                    s_fail = 1;
+                    break;
+                }
+                fill(sp, kc + kStages - 1);
+            }
+        }
+        if (!s_fail && !mbar_wait(&empty[(kChunks - 1) % kStages], ((kChunks - 1) / kStages) & 1))
+            s_fail = 1;
+        if (s_fail) {
+            atomicOr(err, 1);
+            for (int s = 0; s < kStages; s++)
+                if (pend[s]) mbar_wait(&full[s], (uint32_t)(pend[s] - 1));
+            if (last_commit >= 0)
+                mbar_wait(&empty[last_commit % kStages], (uint32_t)((last_commit / kStages) & 1));
+        }
+    }
+    __syncthreads();
+    tc_fence_after();
+    if (!s_fail) {
+        const int u = gt * kMGates + warp * 32 + lane;  // this thread's TMEM lane = gate row
+        const bool live = u < units && valid[u];
+        const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+#pragma unroll 1
+        for (int cc = 0; cc < kNCols / 32; cc++) {
+            uint32_t v[32];
+            tmem_ld32(tmem + lane_base + 32 * cc, v);
+            tmem_wait_ld();
+            if (live) {
+#pragma unroll
+                for (int oo = 0; oo < 8; oo++) {
+                    const int o = nt * kOutPerTile + cc * 8 + oo;
+                    uint32_t r = v[4 * oo] + (v[4 * oo + 1] << 8) + (v[4 * oo + 2] << 16) +
+                                 (v[4 * oo + 3] << 24);
+                    if (o == kN0) r += xb[u];
+                    if (o < kTlwe0) dst[(size_t)u * kTlwe0 + o] = r;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemColsIks));
+}
+
+}  // namespace
+
+size_t iks_tc_key_bytes() { return (size_t)kNTiles * kChunks * kBTile; }
+
+cudaError_t iks_tc_key_build(const uint32_t* ksk_dev, uint8_t* key_tiles, cudaStream_t st)
+{
+    const size_t units = iks_tc_key_bytes() / 4;
+    k_iks_key<<<(unsigned)((units + 255) / 256), 256, 0, st>>>(ksk_dev, key_tiles);
+    return cudaGetLastError();
+}
+
+cudaError_t iks_tc_workspace(IksWorkspace& w, int units)
+{
+    if ((size_t)units <= w.cap) return cudaSuccess;
+    iks_tc_workspace_free(w);
+    const size_t tiles = (size_t)(units + kMGates - 1) / kMGates;
+    cudaError_t e;
+    if ((e = cudaMalloc(&w.atiles, tiles * kChunks * kATile)) != cudaSuccess) return e;
+    if ((e = cudaMemset(w.atiles, 0, tiles * kChunks * kATile)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&w.xb, (size_t)units * 4)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&w.valid, (size_t)units * 4)) != cudaSuccess) return e;
+    w.cap = (size_t)units;
+    return cudaSuccess;
+}
+
+void iks_tc_workspace_free(IksWorkspace& w)
+{
+    cudaFree(w.atiles);
+    cudaFree(w.xb);
+    cudaFree(w.valid);
+    w = IksWorkspace();
+}
+
+cudaError_t launch_iks_tc(int mode, const Plan& plan, const uint32_t* in0, const uint32_t* in1,
+                          const uint32_t* in2, const uint32_t* lane_out, const uint8_t* key_tiles,
+                          uint32_t* dst, IksWorkspace& w, int* err, cudaStream_t st,
+                          int* launches)
+{
+    *launches = 0;
+    const int units = mode == 0 ? plan.lanes : plan.count;
+    if (units <= 0) return cudaSuccess;
+    cudaError_t e = iks_tc_workspace(w, units);
+    if (e != cudaSuccess) return e;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr[64] = {};
+    if (!attr[dev & 63]) {
+        e = cudaFuncSetAttribute(k_iks_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+        if (e != cudaSuccess) return e;
+        attr[dev & 63] = true;
+    }
+    k_iks_prep<<<units, 256, 0, st>>>(mode, plan, in0, in1, in2, lane_out, w.atiles, w.xb, w.valid);
+    const int gtiles = (units + kMGates - 1) / kMGates;
+    k_iks_gemm<<<gtiles * kNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, w.xb, w.valid, units, dst,
+                                                     err);
+    *launches = 2;
+    return cudaGetLastError();
+}
+
+}  // namespace cufhe
