@@ -35,8 +35,8 @@ constexpr uint32_t kDecOffset = (128u << 24) + (128u << 16) + (1u << 15);  // of
 template <int G>
 constexpr size_t br_smem_bytes()
 {
-    return sizeof(double2) * G * 4 * kSlotStride + sizeof(uint32_t) * G * kTrlwe +
-           sizeof(uint16_t) * G * kAbarStride;
+    return sizeof(double2) * G * 4 * kSlotStride + sizeof(double2) * 2 * kN +
+           sizeof(uint32_t) * G * kTrlwe + sizeof(uint16_t) * G * kAbarStride;
 }
 
 // signed digit d (0 = most significant) of an offset Torus32 value
@@ -55,12 +55,14 @@ __global__ void __launch_bounds__(G * 128) k_br_fp64(const uint32_t* __restrict_
 {
     extern __shared__ __align__(16) unsigned char smem[];
     double2* spec = reinterpret_cast<double2*>(smem);
-    uint32_t* acc = reinterpret_cast<uint32_t*>(spec + G * 4 * kSlotStride);
+    double2* psi_s = spec + G * 4 * kSlotStride;  // root table, interleaved (psi_pos)
+    uint32_t* acc = reinterpret_cast<uint32_t*>(psi_s + 2 * kN);
     uint16_t* abar = reinterpret_cast<uint16_t*>(acc + G * kTrlwe);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int lane_base = blockIdx.x * G;
 
+    for (int t = tid; t < 2 * kN; t += blockDim.x) psi_s[psi_pos((uint32_t)t)] = psi[t];
     // ---- prologue: modulus switch and test vector (RotatedTestVector)
 #pragma unroll 1
     for (int g = 0; g < G; g++) {
@@ -108,12 +110,10 @@ __global__ void __launch_bounds__(G * 128) k_br_fp64(const uint32_t* __restrict_
                     lo = rl - lo;
                     hi = rh - hi;
                 }
-                const double2 z = make_double2(digit_of(lo + kDecOffset, d),
-                                               digit_of(hi + kDecOffset, d));
-                v[n2] = cmul(z, __ldg(&psi[n]));
+                v[n2] = make_double2(digit_of(lo + kDecOffset, d), digit_of(hi + kDecOffset, d));
             }
             double2* slot = spec + (g * 4 + r) * kSlotStride;
-            fft512_warp<1>(v, slot, tw512, lane);
+            ffnt_forward_warp(v, slot, psi_s, lane);
 #pragma unroll
             for (int m = 0; m < 16; m++) slot[(lane & 15) + 16 * m + 256 * (lane >> 4)] = v[m];
         }
@@ -140,9 +140,9 @@ __global__ void __launch_bounds__(G * 128) k_br_fp64(const uint32_t* __restrict_
                         for (int r = 0; r < 4; r++) D[r] = spec[(g * 4 + r) * kSlotStride + f];
                         const uint32_t a0 = abar[g * kAbarStride + 2 * p];
                         const uint32_t a1 = abar[g * kAbarStride + 2 * p + 1];
-                        double2 x0 = __ldg(&psi[(ef * a0) & 2047u]);
-                        double2 x1 = __ldg(&psi[(ef * a1) & 2047u]);
-                        double2 x01 = __ldg(&psi[(ef * (a0 + a1)) & 2047u]);
+                        double2 x0 = psi_s[psi_pos(ef * a0)];
+                        double2 x1 = psi_s[psi_pos(ef * a1)];
+                        double2 x01 = psi_s[psi_pos(ef * (a0 + a1))];
                         x0.x -= 1.0;
                         x1.x -= 1.0;
                         x01.x -= 1.0;
@@ -203,13 +203,13 @@ __global__ void __launch_bounds__(G * 128) k_br_fp64(const uint32_t* __restrict_
 #pragma unroll
             for (int n2 = 0; n2 < 16; n2++) v[n2] = slot[lane + 32 * n2];
             __syncwarp();
-            fft512_warp<-1>(v, slot, tw512, lane);
+            ffnt_inverse_warp(v, slot, psi_s, lane);
             uint32_t* a = acc + g * kTrlwe + j * kN;
 #pragma unroll
             for (int m = 0; m < 16; m++) {
                 const int n = (lane & 15) + 16 * m + 256 * (lane >> 4);
-                // untwist = conj(psi^n) / 512; then x 2^32  =>  x 2^23
-                const double2 u = cmulc(v[m], __ldg(&psi[n]));
+                // untwisted value / 512, then x 2^32  =>  x 2^23
+                const double2 u = v[m];
                 const uint32_t lo = (uint32_t)__double2ll_rn(u.x * 0x1p23);
                 const uint32_t hi = (uint32_t)__double2ll_rn(u.y * 0x1p23);
                 if (KB) {
@@ -308,13 +308,20 @@ cudaError_t launch_bk_to_fft(const uint32_t* bk, int npolys, const Fp64Tables& t
 
 cudaError_t upload_fft_constants(void)
 {
-    double2 w[16];
+    double2 w[16], t32[16], u16[16];
     const long double pi = 3.141592653589793238462643383279502884L;
     for (int k = 0; k < 16; k++) {
         const long double a = 2 * pi * k / 32;
         w[k] = make_double2((double)cosl(a), (double)sinl(a));
+        const long double b = pi * k / 32;  // psi^{32 k}
+        t32[k] = make_double2((double)cosl(b), (double)sinl(b));
+        const long double c = -pi * k / 64;  // conj(psi^{16 k})
+        u16[k] = make_double2((double)cosl(c), (double)sinl(c));
     }
-    return cudaMemcpyToSymbol(c_w32, w, sizeof(w));
+    cudaError_t e = cudaMemcpyToSymbol(c_w32, w, sizeof(w));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tw32, t32, sizeof(t32));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_utw16, u16, sizeof(u16));
+    return e;
 }
 
 }  // namespace cufhe

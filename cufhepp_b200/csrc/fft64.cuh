@@ -152,4 +152,93 @@ __device__ __forceinline__ void fft512_warp(double2 (&v)[16], double2* tile,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Table-light transforms for the blind-rotation kernel.  The root table
+// psi^t (t < 2N, psi = e^{i pi / N}) lives in shared memory in the
+// interleaved order pos(t) = (t mod 4) * 512 + t / 4, which makes the
+// KeyBundle gathers psi^{(1+4f) a} (stride 4a across lanes) bank-conflict
+// free for odd a.
+__device__ __forceinline__ int psi_pos(uint32_t t) { return (int)((t & 3u) * 512u + ((t >> 2) & 511u)); }
+
+// e^{i pi n2 / 32} (= psi^{32 n2}) and e^{-i pi m / 64} (= psi^{-16 m})
+static __constant__ double2 c_tw32[16];
+static __constant__ double2 c_utw16[16];
+
+// Forward FFNT of one folded polynomial: in v[n2] = d[n] + i d[n + 512] for
+// n = lane + 32 n2; out as fft512_warp.  The twist psi^n = psi^lane psi^{32 n2}
+// is split into a compile-time factor (before the 16-point DFT) and a per-lane
+// factor merged with the w512^{lane k2} twiddle: psi^{lane (1 + 4 k2)},
+// generated by recurrence from two table reads.
+__device__ __forceinline__ void ffnt_forward_warp(double2 (&v)[16], double2* tile,
+                                                  const double2* psi_s, int lane)
+{
+#pragma unroll
+    for (int n2 = 1; n2 < 16; n2++) v[n2] = cmul(v[n2], c_tw32[n2]);
+    dft16<1>(v);
+    double2 t = psi_s[psi_pos((uint32_t)lane)];
+    const double2 st = psi_s[psi_pos(4u * (uint32_t)lane)];
+#pragma unroll
+    for (int k2 = 0; k2 < 16; k2++) {
+        v[k2] = cmul(v[k2], t);
+        if (k2 < 15) t = cmul(t, st);
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < 16; k2++) tile[k2 * 33 + lane] = v[k2];
+    __syncwarp();
+    const int k2 = lane & 15, h = lane >> 4;
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = tile[k2 * 33 + h + 2 * m];
+    __syncwarp();
+    dft16<1>(v);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const double2 w = c_w32[m];
+        double2 tt = h ? cmul(v[m], w) : v[m];
+        double2 o;
+        o.x = __shfl_xor_sync(0xffffffffu, tt.x, 16);
+        o.y = __shfl_xor_sync(0xffffffffu, tt.y, 16);
+        v[m] = h ? csub(o, tt) : cadd(tt, o);
+    }
+}
+
+// Inverse FFNT: in v[n2] = Z[lane + 32 n2] (natural bins); out v[m] holds
+// z'[n] * conj(psi^n) (untwisted, without the 1/512 scale) for
+// n = (lane & 15) + 16 m + 256 (lane >> 4).
+__device__ __forceinline__ void ffnt_inverse_warp(double2 (&v)[16], double2* tile,
+                                                  const double2* psi_s, int lane)
+{
+    dft16<-1>(v);
+    {
+        const double2 st = psi_s[psi_pos(4u * (uint32_t)lane)];  // w512^{lane} = psi^{4 lane}
+        double2 t = st;
+#pragma unroll
+        for (int k2 = 1; k2 < 16; k2++) {
+            v[k2] = cmulc(v[k2], t);
+            if (k2 < 15) t = cmul(t, st);
+        }
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < 16; k2++) tile[k2 * 33 + lane] = v[k2];
+    __syncwarp();
+    const int k2 = lane & 15, h = lane >> 4;
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = tile[k2 * 33 + h + 2 * m];
+    __syncwarp();
+    dft16<-1>(v);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        double2 w = c_w32[m];
+        w.y = -w.y;
+        double2 tt = h ? cmul(v[m], w) : v[m];
+        double2 o;
+        o.x = __shfl_xor_sync(0xffffffffu, tt.x, 16);
+        o.y = __shfl_xor_sync(0xffffffffu, tt.y, 16);
+        v[m] = h ? csub(o, tt) : cadd(tt, o);
+    }
+    // untwist conj(psi^{k2 + 256 h}) conj(psi^{16 m})
+    const double2 u = psi_s[psi_pos((uint32_t)(k2 + 256 * h))];
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = cmul(cmulc(v[m], u), c_utw16[m]);
+}
+
 }  // namespace cufhe
