@@ -22,6 +22,8 @@
 //            (psi^{(1+4f) a} - 1) instead of the reference's 16 MB xai table
 //   phase 3  warp (g, j): inverse FFT, untwist, round, write acc[g][j]
 // Epilogue: SampleExtract straight from shared memory to the lane output.
+#include <stdlib.h>
+
 #include "engine.h"
 #include "fft64.cuh"
 
@@ -29,13 +31,14 @@ namespace cufhe {
 
 namespace {
 
+constexpr int kDefaultBrGates = 2;
 constexpr int kAbarStride = 640;
 constexpr uint32_t kDecOffset = (128u << 24) + (128u << 16) + (1u << 15);  // offsetgen + round
 
 template <int G>
 constexpr size_t br_smem_bytes()
 {
-    return sizeof(double2) * G * 4 * kSlotStride + sizeof(double2) * 2 * kN +
+    return sizeof(double2) * G * 4 * kSlotStride + sizeof(double2) * kN +
            sizeof(uint32_t) * G * kTrlwe + sizeof(uint16_t) * G * kAbarStride;
 }
 
@@ -46,7 +49,7 @@ __device__ __forceinline__ double digit_of(uint32_t t, int d)
 }
 
 template <bool KB, int G>
-__global__ void __launch_bounds__(G * 128) k_br_fp64(const uint32_t* __restrict__ lane_in, int lanes,
+__global__ void __launch_bounds__(G * 128, G == 2 ? 2 : 1) k_br_fp64(const uint32_t* __restrict__ lane_in, int lanes,
                                                      uint32_t mu, const double2* __restrict__ bkf,
                                                      const double2* __restrict__ psi,
                                                      const double2* __restrict__ tw512, int steps,
@@ -56,13 +59,13 @@ __global__ void __launch_bounds__(G * 128) k_br_fp64(const uint32_t* __restrict_
     extern __shared__ __align__(16) unsigned char smem[];
     double2* spec = reinterpret_cast<double2*>(smem);
     double2* psi_s = spec + G * 4 * kSlotStride;  // root table, interleaved (psi_pos)
-    uint32_t* acc = reinterpret_cast<uint32_t*>(psi_s + 2 * kN);
+    uint32_t* acc = reinterpret_cast<uint32_t*>(psi_s + kN);
     uint16_t* abar = reinterpret_cast<uint16_t*>(acc + G * kTrlwe);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int lane_base = blockIdx.x * G;
 
-    for (int t = tid; t < 2 * kN; t += blockDim.x) psi_s[psi_pos((uint32_t)t)] = psi[t];
+    for (int t = tid; t < kN; t += blockDim.x) psi_s[psi_pos((uint32_t)t)] = psi[t];
     // ---- prologue: modulus switch and test vector (RotatedTestVector)
 #pragma unroll 1
     for (int g = 0; g < G; g++) {
@@ -140,9 +143,9 @@ __global__ void __launch_bounds__(G * 128) k_br_fp64(const uint32_t* __restrict_
                         for (int r = 0; r < 4; r++) D[r] = spec[(g * 4 + r) * kSlotStride + f];
                         const uint32_t a0 = abar[g * kAbarStride + 2 * p];
                         const uint32_t a1 = abar[g * kAbarStride + 2 * p + 1];
-                        double2 x0 = psi_s[psi_pos(ef * a0)];
-                        double2 x1 = psi_s[psi_pos(ef * a1)];
-                        double2 x01 = psi_s[psi_pos(ef * (a0 + a1))];
+                        double2 x0 = psi_at(psi_s, ef * a0);
+                        double2 x1 = psi_at(psi_s, ef * a1);
+                        double2 x01 = psi_at(psi_s, ef * (a0 + a1));
                         x0.x -= 1.0;
                         x1.x -= 1.0;
                         x01.x -= 1.0;
@@ -288,15 +291,29 @@ cudaError_t launch_g(const uint32_t* lane_in, int lanes, uint32_t mu, const doub
 
 }  // namespace
 
-constexpr int kBrGates = 4;
+// Lanes per CTA: 2 (two CTAs per SM, whose phases overlap) or 4 (one CTA per
+// SM, key rows shared by 4 lanes).  CUFHE_BR_LANES_PER_CTA overrides the
+// default for tuning.
+static int br_lanes_per_cta()
+{
+    static int g = 0;
+    if (!g) {
+        const char* e = getenv("CUFHE_BR_LANES_PER_CTA");
+        g = (e && atoi(e) == 4) ? 4 : (e && atoi(e) == 2) ? 2 : kDefaultBrGates;
+    }
+    return g;
+}
 
 cudaError_t launch_br_fp64(bool kb, const uint32_t* lane_in, int lanes, uint32_t mu,
                            const double2* bkf, const Fp64Tables& t, int steps, uint32_t* acc_out,
                            uint32_t* lane_out, cudaStream_t st)
 {
     if (lanes <= 0) return cudaSuccess;
-    return kb ? launch_g<true, kBrGates>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st)
-              : launch_g<false, kBrGates>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st);
+    if (br_lanes_per_cta() == 2)
+        return kb ? launch_g<true, 2>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st)
+                  : launch_g<false, 2>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st);
+    return kb ? launch_g<true, 4>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st)
+              : launch_g<false, 4>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st);
 }
 
 cudaError_t launch_bk_to_fft(const uint32_t* bk, int npolys, const Fp64Tables& t, double2* out,

@@ -154,11 +154,22 @@ __device__ __forceinline__ void fft512_warp(double2 (&v)[16], double2* tile,
 
 // ---------------------------------------------------------------------------
 // Table-light transforms for the blind-rotation kernel.  The root table
-// psi^t (t < 2N, psi = e^{i pi / N}) lives in shared memory in the
-// interleaved order pos(t) = (t mod 4) * 512 + t / 4, which makes the
-// KeyBundle gathers psi^{(1+4f) a} (stride 4a across lanes) bank-conflict
-// free for odd a.
-__device__ __forceinline__ int psi_pos(uint32_t t) { return (int)((t & 3u) * 512u + ((t >> 2) & 511u)); }
+// psi^t (t < N, psi = e^{i pi / N}; psi^{t+N} = -psi^t) lives in shared
+// memory in the interleaved order pos(t) = (t mod 4) * 256 + t / 4, which
+// makes the KeyBundle gathers psi^{(1+4f) a} (stride 4a across lanes)
+// bank-conflict free for odd a.
+__device__ __forceinline__ int psi_pos(uint32_t t) { return (int)((t & 3u) * 256u + ((t >> 2) & 255u)); }
+
+// psi^t for any t (mod 2N)
+__device__ __forceinline__ double2 psi_at(const double2* psi_s, uint32_t t)
+{
+    double2 v = psi_s[psi_pos(t)];
+    if (t & 1024u) {
+        v.x = -v.x;
+        v.y = -v.y;
+    }
+    return v;
+}
 
 // e^{i pi n2 / 32} (= psi^{32 n2}) and e^{-i pi m / 64} (= psi^{-16 m})
 static __constant__ double2 c_tw32[16];
