@@ -49,7 +49,7 @@ __device__ __forceinline__ double digit_of(uint32_t t, int d)
 }
 
 template <bool KB, int G>
-__global__ void __launch_bounds__(G * 128, G == 2 ? 2 : 1) k_br_fp64(const uint32_t* __restrict__ lane_in, int lanes,
+__global__ void __launch_bounds__(G * 128, G == 1 ? 3 : (G == 2 ? 2 : 1)) k_br_fp64(const uint32_t* __restrict__ lane_in, int lanes,
                                                      uint32_t mu, const double2* __restrict__ bkf,
                                                      const double2* __restrict__ psi,
                                                      const double2* __restrict__ tw512, int steps,
@@ -291,15 +291,15 @@ cudaError_t launch_g(const uint32_t* lane_in, int lanes, uint32_t mu, const doub
 
 }  // namespace
 
-// Lanes per CTA: 2 (two CTAs per SM, whose phases overlap) or 4 (one CTA per
-// SM, key rows shared by 4 lanes).  CUFHE_BR_LANES_PER_CTA overrides the
+// Lanes per CTA: 1 (three CTAs per SM), 2 (two CTAs per SM, whose phases
+// overlap) or 4 (one CTA per SM, key rows shared by 4 lanes).  CUFHE_BR_LANES_PER_CTA overrides the
 // default for tuning.
 static int br_lanes_per_cta()
 {
     static int g = 0;
     if (!g) {
         const char* e = getenv("CUFHE_BR_LANES_PER_CTA");
-        g = (e && atoi(e) == 4) ? 4 : (e && atoi(e) == 2) ? 2 : kDefaultBrGates;
+        g = (e && atoi(e) == 4) ? 4 : (e && atoi(e) == 2) ? 2 : (e && atoi(e) == 1) ? 1 : kDefaultBrGates;
     }
     return g;
 }
@@ -309,7 +309,17 @@ cudaError_t launch_br_fp64(bool kb, const uint32_t* lane_in, int lanes, uint32_t
                            uint32_t* lane_out, cudaStream_t st)
 {
     if (lanes <= 0) return cudaSuccess;
-    if (br_lanes_per_cta() == 2)
+    // small batches: one lane per CTA (3 CTAs per SM) while they fit one wave,
+    // which minimises latency; larger ones: two lanes per CTA for throughput
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int g = getenv("CUFHE_BR_LANES_PER_CTA") ? br_lanes_per_cta()
+                                                   : (lanes <= 3 * sms ? 1 : kDefaultBrGates);
+    if (g == 1)
+        return kb ? launch_g<true, 1>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st)
+                  : launch_g<false, 1>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st);
+    if (g == 2)
         return kb ? launch_g<true, 2>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st)
                   : launch_g<false, 2>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st);
     return kb ? launch_g<true, 4>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st)
