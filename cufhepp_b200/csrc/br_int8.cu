@@ -28,11 +28,12 @@
 //  * acc  : [lanes][2][1024] Torus32.
 //
 // k_i8_gemm: CTA = (256-lane group, 128 output rows = 4 limbs x 32
-// coefficients of one j_out).  The Toeplitz A tile is generated by the 128
-// threads straight into TMEM (tcgen05.st; thread = row), double-buffered;
-// one thread issues 4 tcgen05.mma.kind::i8 (M=128, N=256, K=32) per chunk
-// with the INT32 accumulator in TMEM; the digits stream through a 3-stage
-// shared-memory ring.  Every mbarrier wait is bounded and reports a timeout
+// coefficients of one j_out), warp-specialised: two generator warpgroups
+// write the Toeplitz A tiles of alternate K chunks straight into TMEM
+// (tcgen05.st; thread = row, one TMEM stage per warpgroup), one thread issues
+// 4 tcgen05.mma.kind::i8 (M=128, N=256, K=32) per chunk into the INT32
+// accumulator in TMEM, one thread streams the digit tiles through a 4-stage
+// shared-memory ring; hand-offs go through mbarriers only.  Every mbarrier wait is bounded and reports a timeout
 // through an error flag instead of hanging.
 #include <stdio.h>
 
@@ -52,7 +53,7 @@ constexpr int kRowsCoef = 32;                // coefficients per CTA tile (x4 li
 constexpr int kMTiles = 2 * kN / kRowsCoef;  // 64 tiles per lane group
 constexpr int kVBytesStep = 2 * 4 * 4 * 2 * kN;  // 64 KB of key table per step
 constexpr int kVBytesJ = 4 * 4 * 2 * kN;         // 32 KB per output poly
-constexpr int kBStages = 3;
+constexpr int kBStages = 4;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kAccCol = 0;      // accumulator columns [0, 256)
 constexpr uint32_t kACol = 256;      // A stages at 256 and 288 (32 columns each)
@@ -61,9 +62,9 @@ constexpr uint32_t kACol = 256;      // A stages at 256 and 288 (32 columns each
 constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kGroup >> 3) << 17) |
                             ((uint32_t)(128 >> 4) << 24);
 
-constexpr size_t kSmemB = (size_t)kBStages * kTileBytes;  // 96 KB
+constexpr size_t kSmemB = (size_t)kBStages * kTileBytes;  // 128 KB
 constexpr size_t kSmemV = kVBytesJ;                       // 32 KB
-constexpr size_t kSmemRed = 4 * 32 * 33 * 4;              // 16.5 KB
+constexpr size_t kSmemRed = 8 * 32 * 33 * 4;              // 33 KB (two warpgroups)
 constexpr size_t kSmemGemm = 1024 + kSmemB + kSmemV + kSmemRed + 256;
 
 // ------------------------------------------------------------ kernels ----
@@ -148,34 +149,44 @@ __global__ void __launch_bounds__(256) k_i8_decompose(const uint32_t* __restrict
     }
 }
 
-__global__ void __launch_bounds__(128, 1) k_i8_gemm(const int8_t* __restrict__ vkey,
-                                                    const uint8_t* __restrict__ tiles,
-                                                    uint32_t* __restrict__ acc, int lanes,
-                                                    int* __restrict__ err)
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Warp roles: warps 0-3 and 4-7 are two generator warpgroups (chunks of even
+// / odd index, each with its own TMEM A stage), warp 8 issues the MMAs, warp
+// 9 streams digit tiles.  They hand off through mbarriers only; every wait is
+// bounded and an expired wait sets s_fail, which the other roles poll.
+constexpr int kGemmThreads = 320;
+
+__global__ void __launch_bounds__(kGemmThreads, 1) k_i8_gemm(const int8_t* __restrict__ vkey,
+                                                             const uint8_t* __restrict__ tiles,
+                                                             uint32_t* __restrict__ acc, int lanes,
+                                                             int* __restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    // 1024-aligned base for the swizzled operand stages
     const uint32_t raw_addr = smem_u32(smem_raw);
     unsigned char* smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
-    unsigned char* bst = smem;                                   // 3 x 32 KB
+    unsigned char* bst = smem;                                   // kBStages x 32 KB
     int8_t* vs = reinterpret_cast<int8_t*>(smem + kSmemB);       // 32 KB
     uint32_t* red = reinterpret_cast<uint32_t*>(smem + kSmemB + kSmemV);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kSmemB + kSmemV + kSmemRed);
-    uint64_t* bar_b = bars;           // [3]
-    uint64_t* bar_mma = bars + 3;     // [2]
-    uint64_t* bar_v = bars + 5;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 6);
+    uint64_t* b_full = bars;                    // [kBStages]
+    uint64_t* b_empty = bars + kBStages;        // [kBStages]
+    uint64_t* a_full = bars + 2 * kBStages;     // [2]
+    uint64_t* a_empty = a_full + 2;             // [2]
+    uint64_t* bar_v = a_empty + 2;
+    uint64_t* acc_full = bar_v + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 1);
+    __shared__ volatile int s_fail;
 
-    __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int group = blockIdx.x / kMTiles;
     const int mt = blockIdx.x % kMTiles;
     const int j_out = mt / (kN / kRowsCoef);
     const int n0 = (mt % (kN / kRowsCoef)) * kRowsCoef;
     const uint8_t* gtiles = tiles + (size_t)group * kChunks * kTileBytes;
-    // thread 0's bookkeeping of asynchronous work still in flight
-    int pend_b[kBStages] = {0, 0, 0};   // 1 + parity of an outstanding copy, 0 = none
-    int last_commit = -1;               // last chunk whose MMAs were committed
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -184,10 +195,16 @@ __global__ void __launch_bounds__(128, 1) k_i8_gemm(const int8_t* __restrict__ v
     }
     if (tid == 0) {
         s_fail = 0;
-        for (int s = 0; s < kBStages; s++) mbar_init(&bar_b[s], 1);
-        mbar_init(&bar_mma[0], 1);
-        mbar_init(&bar_mma[1], 1);
+        for (int s = 0; s < kBStages; s++) {
+            mbar_init(&b_full[s], 1);
+            mbar_init(&b_empty[s], 1);
+        }
+        for (int s = 0; s < 2; s++) {
+            mbar_init(&a_full[s], 128);
+            mbar_init(&a_empty[s], 1);
+        }
         mbar_init(bar_v, 1);
+        mbar_init(acc_full, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -195,105 +212,121 @@ __global__ void __launch_bounds__(128, 1) k_i8_gemm(const int8_t* __restrict__ v
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (tid == 0) {
-        mbar_expect_tx(bar_v, kVBytesJ);
-        bulk_g2s(vs, vkey + (size_t)j_out * kVBytesJ, kVBytesJ, bar_v);
-        for (int s = 0; s < kBStages; s++) {
-            mbar_expect_tx(&bar_b[s], kTileBytes);
-            bulk_g2s(bst + s * kTileBytes, gtiles + (size_t)s * kTileBytes, kTileBytes, &bar_b[s]);
-            pend_b[s] = 1;
+    if (warp == 9) {
+        // ---- producer: key table once, then the digit tiles through the ring
+        if (lane == 0) {
+            mbar_expect_tx(bar_v, kVBytesJ);
+            bulk_g2s(vs, vkey + (size_t)j_out * kVBytesJ, kVBytesJ, bar_v);
+            for (int kc = 0; kc < kChunks && !s_fail; kc++) {
+                const int s = kc % kBStages;
+                if (kc >= kBStages && !mbar_wait(&b_empty[s], ((kc / kBStages) - 1) & 1)) {
+                    s_fail = 1;
+                    break;
+                }
+                mbar_expect_tx(&b_full[s], kTileBytes);
+                bulk_g2s(bst + s * kTileBytes, gtiles + (size_t)kc * kTileBytes, kTileBytes,
+                         &b_full[s]);
+            }
         }
-        if (!mbar_wait(bar_v, 0)) s_fail = 1;
-    }
-
-    const int c = warp;                     // limb of this thread's row
-    const int n = n0 + lane;                // output coefficient of this thread's row
-    const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
-
-    for (int kc = 0; kc < kChunks; kc++) {
-        const int sa = kc & 1, sb = kc % kBStages;
-        // stage sa of A is free once chunk kc-2's MMAs completed (thread 0
-        // observes, the barrier publishes it to the block)
-        if (tid == 0 && kc >= 2 && !s_fail && !mbar_wait(&bar_mma[sa], ((kc - 2) >> 1) & 1))
-            s_fail = 1;
-        __syncthreads();
-        if (s_fail) break;
-        tc_fence_after();
-        // Toeplitz rows: A[n][m0 + k] = V_{r,j_out,c}[N - 1 - n + m0 + k]
-        const int r = kc / (kN / kChunkK), m0 = (kc % (kN / kChunkK)) * kChunkK;
-        const uint32_t* vw = reinterpret_cast<const uint32_t*>(vs + (r * 4 + c) * (2 * kN));
-        const int s = kN - 1 - n + m0;
-        const int w0 = s >> 2, sh = (s & 3) * 8;
-        uint32_t w[33];
-#pragma unroll
-        for (int q = 0; q < 33; q++) w[q] = vw[w0 + q];
-        uint32_t a[32];
-#pragma unroll
-        for (int q = 0; q < 32; q++) a[q] = __funnelshift_r(w[q], w[q + 1], sh);
-        tmem_st32(tmem + lane_base + kACol + 32 * sa, a);
-        tmem_wait_st();
-        tc_fence_before();
-        __syncthreads();
-        if (tid == 0) {
-            if (!mbar_wait(&bar_b[sb], (kc / kBStages) & 1)) {
-                s_fail = 1;
-            } else {
-                pend_b[sb] = 0;
+    } else if (warp == 8) {
+        // ---- MMA issue: one thread
+        if (lane == 0) {
+            for (int kc = 0; kc < kChunks; kc++) {
+                const int s = kc % kBStages, sa = kc & 1;
+                if (!mbar_wait(&b_full[s], (kc / kBStages) & 1) ||
+                    !mbar_wait(&a_full[sa], (kc >> 1) & 1)) {
+                    s_fail = 1;
+                    break;
+                }
                 tc_fence_after();
-                const uint32_t bbase = smem_u32(bst + sb * kTileBytes);
+                const uint32_t bbase = smem_u32(bst + s * kTileBytes);
 #pragma unroll
                 for (int k = 0; k < kChunkK / 32; k++)
                     tc_mma_i8(tmem + kAccCol, tmem + kACol + 32 * sa + 8 * k,
                               desc_kmajor_sw128(bbase + 32 * k), kIdesc, (kc | k) != 0);
-                tc_commit(&bar_mma[sa]);
-                last_commit = kc;
-                // refill the stage chunk kc-1 used, once its MMAs are done
-                if (kc >= 1 && kc + 2 < kChunks) {
-                    const int sp = (kc + 2) % kBStages;
-                    if (!mbar_wait(&bar_mma[(kc - 1) & 1], ((kc - 1) >> 1) & 1)) {
-                        s_fail = 1;
-                    } else {
-                        mbar_expect_tx(&bar_b[sp], kTileBytes);
-                        bulk_g2s(bst + sp * kTileBytes, gtiles + (size_t)(kc + 2) * kTileBytes,
-                                 kTileBytes, &bar_b[sp]);
-                        pend_b[sp] = 1 + (((kc + 2) / kBStages) & 1);
-                    }
-                }
+                tc_commit(&b_empty[s]);
+                tc_commit(&a_empty[sa]);
             }
+            tc_commit(acc_full);
         }
+    } else {
+        // ---- generators: warpgroup wg builds A for chunks kc = wg, wg + 2, ...
+        const int wg = warp >> 2, q = warp & 3;  // q: TMEM lane quarter = limb c
+        const int n = n0 + lane;
+        const uint32_t lane_base = (uint32_t)(32 * q) << 16;
+        // every branch below is taken by whole warps (votes), so the
+        // .sync.aligned tcgen05 instructions never run on a partial warp
+        bool ok = __all_sync(0xffffffffu, mbar_wait(bar_v, 0));
+        for (int kc = wg; kc < kChunks && ok; kc += 2) {
+            if (__any_sync(0xffffffffu, s_fail != 0)) {
+                ok = false;
+                break;
+            }
+            if (kc >= 2 && !__all_sync(0xffffffffu, mbar_wait(&a_empty[wg], ((kc >> 1) - 1) & 1))) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            // Toeplitz rows: A[n][m0 + k] = V_{r,j_out,c}[N - 1 - n + m0 + k]
+            const int r = kc / (kN / kChunkK), m0 = (kc % (kN / kChunkK)) * kChunkK;
+            const uint32_t* vw = reinterpret_cast<const uint32_t*>(vs + (r * 4 + q) * (2 * kN));
+            const int sst = kN - 1 - n + m0;
+            const int w0 = sst >> 2, sh = (sst & 3) * 8;
+            uint32_t w[33];
+#pragma unroll
+            for (int i = 0; i < 33; i++) w[i] = vw[w0 + i];
+            uint32_t a[32];
+#pragma unroll
+            for (int i = 0; i < 32; i++) a[i] = __funnelshift_r(w[i], w[i + 1], sh);
+            tmem_st32(tmem + lane_base + kACol + 32 * wg, a);
+            tmem_wait_st();
+            tc_fence_before();
+            mbar_arrive(&a_full[wg]);
+        }
+        if (!ok) s_fail = 1;
     }
 
-    // last chunk's MMAs done -> accumulator complete
-    if (tid == 0 && !s_fail && !mbar_wait(&bar_mma[(kChunks - 1) & 1], ((kChunks - 1) >> 1) & 1))
-        s_fail = 1;
+    // ---- epilogue (generator warps): wait for the accumulator, recombine limbs
+    const bool gen = warp < 8;
+    if (gen) {
+        const bool have_acc = __all_sync(0xffffffffu, s_fail == 0 && mbar_wait(acc_full, 0));
+        if (!have_acc) s_fail = 1;
+    }
     __syncthreads();
     tc_fence_after();
     if (!s_fail) {
-        for (int cc = 0; cc < kGroup / 32; cc++) {
-            uint32_t v[32];
-            tmem_ld32(tmem + lane_base + kAccCol + 32 * cc, v);
-            tmem_wait_ld();
+        // warpgroup wg reads accumulator columns [128 wg, 128 wg + 128)
+        for (int cc = 0; cc < kGroup / 64; cc++) {
+            if (gen) {
+                const int wg = warp >> 2, q = warp & 3;
+                uint32_t v[32];
+                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + kAccCol + 128 * wg + 32 * cc, v);
+                tmem_wait_ld();
 #pragma unroll
-            for (int g = 0; g < 32; g++) red[(warp * 32 + lane) * 33 + g] = v[g] << (8 * warp);
+                for (int g = 0; g < 32; g++)
+                    red[((wg * 4 + q) * 32 + lane) * 33 + g] = v[g] << (8 * q);
+            }
             __syncthreads();
-            const int nl = tid & 31, gs = tid >> 5;
+            if (gen) {
+                const int wg = tid >> 7, t = tid & 127;
+                const int nl = t & 31, gs = t >> 5;
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int g = gs + 4 * k;
-                const int l = group * kGroup + cc * 32 + g;
-                const uint32_t sum = red[(0 * 32 + nl) * 33 + g] + red[(1 * 32 + nl) * 33 + g] +
-                                     red[(2 * 32 + nl) * 33 + g] + red[(3 * 32 + nl) * 33 + g];
-                if (l < lanes) acc[(size_t)l * kTrlwe + j_out * kN + n0 + nl] += sum;
+                for (int k = 0; k < 8; k++) {
+                    const int g = gs + 4 * k;
+                    const int l = group * kGroup + 128 * wg + cc * 32 + g;
+                    const uint32_t* rb = red + (size_t)(wg * 4) * 32 * 33;
+                    const uint32_t sum = rb[(0 * 32 + nl) * 33 + g] + rb[(1 * 32 + nl) * 33 + g] +
+                                         rb[(2 * 32 + nl) * 33 + g] + rb[(3 * 32 + nl) * 33 + g];
+                    if (l < lanes) acc[(size_t)l * kTrlwe + j_out * kN + n0 + nl] += sum;
+                }
             }
             __syncthreads();
         }
     } else if (tid == 0) {
-        // report, then drain what is still in flight (bounded) before TMEM is freed
         atomicOr(err, 1);
-        for (int s = 0; s < kBStages; s++)
-            if (pend_b[s]) mbar_wait(&bar_b[s], (uint32_t)(pend_b[s] - 1));
-        if (last_commit >= 0)
-            mbar_wait(&bar_mma[last_commit & 1], (uint32_t)((last_commit >> 1) & 1));
+        // drain: wait (bounded) for every copy and MMA batch that may be in flight
+        for (int s = 0; s < kBStages; s++) mbar_wait(&b_full[s], 0), mbar_wait(&b_full[s], 1);
+        mbar_wait(acc_full, 0);
     }
     tc_fence_before();
     __syncthreads();
@@ -386,7 +419,7 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
     int n = 1;
     for (int i = 0; i < nsteps; i++) {
         k_i8_decompose<<<lanes, 256, 0, st>>>(w.acc, w.abar, lanes, i, (uint8_t*)w.digits);
-        k_i8_gemm<<<groups * kMTiles, 128, kSmemGemm, st>>>(
+        k_i8_gemm<<<groups * kMTiles, kGemmThreads, kSmemGemm, st>>>(
             (const int8_t*)k.limbs + (size_t)i * kVBytesStep, (const uint8_t*)w.digits, w.acc,
             lanes, w.err);
         n += 2;
