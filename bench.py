@@ -307,7 +307,7 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
             peak = engine_peak_fp64(engine)
             rl = {"bound": "fp64", "achieved": work / per_launch_s / 1e12, "peak": peak,
                   "unit": "TFLOP/s", "frac": work / per_launch_s / 1e12 / peak,
-                  "traffic": ncu_traffic("br_fp64_kb" if kb else "br_fp64"),
+                  "traffic": ncu_traffic("br_fp64_kb") if kb else None,
                   "kernel": "k_br_fp64 (FP64 FFNT blind rotation + SampleExtract)",
                   "work_per_launch": work,
                   "peak_source": "measured FP64 FMA probe on this GPU "
