@@ -78,6 +78,21 @@ def bootstraps(gates):
     return int(gates.size + np.count_nonzero(gates == 12))
 
 
+def max_over_ranks(torch, x: float, device) -> float:
+    """Maximum of x over all ranks (identity without a process group)."""
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if torch.distributed.is_available() and torch.distributed.is_initialized() and \
+            torch.distributed.get_world_size() > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return t.item()
+
+
+def whole_job_rate(units_per_rank_step: int, world: int, steps: int, max_ms: float) -> float:
+    """Units per second of the whole job: every rank processes its own batch
+    each step (weak scaling); the slowest rank's device time sets the pace."""
+    return units_per_rank_step * world * steps / (max_ms * 1e-3)
+
+
 # ---------------------------------------------------------------- clocks ---
 class Clocks:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -254,11 +269,9 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
     if ws > 1:
         torch.distributed.barrier()
     step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
-    total = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        torch.distributed.all_reduce(total, op=torch.distributed.ReduceOp.MAX)
+    total_ms = max_over_ranks(torch, sum(step_ms), "cuda")
     nb = bootstraps(gates)
-    value = nb * ws * args.steps / (total.item() * 1e-3)
+    value = whole_job_rate(nb, ws, args.steps, total_ms)
 
     # e2e through the C-ABI with pinned host buffers
     host_in = [np.ascontiguousarray(x) for x in cts]
@@ -276,10 +289,7 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
         ev2[k][1].record()
         flush.zero_()
     torch.cuda.synchronize()
-    e2e_ms = torch.tensor([sum(e0.elapsed_time(e1) for e0, e1 in ev2)], dtype=torch.float64,
-                          device="cuda")
-    if ws > 1:
-        torch.distributed.all_reduce(e2e_ms, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = max_over_ranks(torch, sum(e0.elapsed_time(e1) for e0, e1 in ev2), "cuda")
     fails += int(np.count_nonzero(client.decrypt_bits(sk, host_out, level) != exp))
     for h in host_in + [host_out]:
         engine.load().cufhe_host_unregister(engine._p(h))
@@ -322,12 +332,12 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
                   "work_per_launch": work,
                   "peak_source": "measured torch._int_mm int8 GEMM 8192^3 on this GPU"}
     res = {
-        "value": value, "ms_per_step": total.item() / args.steps,
+        "value": value, "ms_per_step": total_ms / args.steps,
         "p50_gate_latency_ms": statistics.median(step_ms),
         "p99_gate_latency_ms": float(np.percentile(step_ms, 99)),
         "single_gate_latency_ms": statistics.median(lat),
         "decrypt_failures": fails, "gates_checked": 2 * B,
-        "e2e": {"value": nb * ws * args.steps / (e2e_ms.item() * 1e-3), "unit": UNIT,
+        "e2e": {"value": whole_job_rate(nb, ws, args.steps, e2e_ms), "unit": UNIT,
                 "h2d_bytes_per_step": int(sum(x.nbytes for x in cts)),
                 "d2h_bytes_per_step": int(B * words * 4)},
         "gpu_launches": launches,

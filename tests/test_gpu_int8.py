@@ -75,3 +75,34 @@ def test_int8_gates_bit_exact(ctx, level):
     assert np.array_equal(out, ref)
     exp = np.array([P.TRUTH[g](int(x), int(y), int(z)) for g, x, y, z in zip(gates, a, b, c)])
     assert np.array_equal(client.decrypt_bits(sk, out, level), exp)
+
+
+def test_int8_reproduces_golden_digests(ctx):
+    """The INT8 engine path matches the committed exact-oracle digests bit for bit."""
+    import json
+    import sys
+    from pathlib import Path
+    golden = Path(__file__).resolve().parent / "golden"
+    sys.path.insert(0, str(golden))
+    import make_gate_golden as M
+    want = json.loads((golden / "gates_exact.json").read_text())
+    sk = client.SecretKey.generate(M.SEED)
+    ek = client.EvalKey.generate(sk, keybundle=False)
+    assert M.digest(ek.bk) == want["keys"]["plain"]["bk"]
+    engine.initialize(ek)  # golden keys (the module fixture's keys are reinstated below)
+    try:
+        for level in (1, 0):
+            _, cts = M.inputs(sk, level)
+            out = engine.gate_batch_host(np.array(M.GATES, np.int32), level, *cts)
+            engine.synchronize()
+            assert M.digest(out) == want["cases"][f"plain_lvl{level}"]["outputs"]
+        x = client.encrypt_bits(sk, np.array([0, 1, 1, 0], np.uint8), 0, seed=M.SEED + 99)
+        assert M.digest(rotate(x, 3, 4)) == want["cases"]["plain_br3"]["outputs"]
+        c1 = client.encrypt_bits(sk, np.arange(16, dtype=np.uint8) & 1, 1, seed=M.SEED + 7)
+        d_in = engine.to_device(c1)
+        d_out = engine.DeviceBuffer(16 * P.TLWE0_WORDS * 4)
+        engine.identity_keyswitch(d_in, 16, d_out)
+        assert M.digest(engine.from_device(d_out, (16, P.TLWE0_WORDS))) == \
+            want["cases"]["iks16"]["outputs"]
+    finally:
+        engine.initialize(ctx[1])
