@@ -37,12 +37,16 @@ def _load():
             "tfhe_trgsw32_encrypt": [u64, u64, vp, u32, u32, u32, i32, dbl, vp],
             "tfhe_bk32_gen": [u64, vp, u32, vp, u32, u32, u32, dbl, i, vp],
             "tfhe_ksk32_gen": [u64, vp, u32, vp, u32, u32, u32, dbl, vp],
+            "tfhe_bk64_gen": [u64, vp, u32, vp, u32, u32, u32, dbl, i, vp],
+            "tfhe_trlwe64_phase": [vp, u32, vp, vp],
         }
         for name, argt in sigs.items():
             fn = getattr(lib, name)
             fn.argtypes = argt
             fn.restype = None
         lib.tfhe_tlwe32_phase.restype = u32
+        lib.tfhe_tlwe64_phase.argtypes = [vp, u32, vp]
+        lib.tfhe_tlwe64_phase.restype = u64
         _lib = lib
     return _lib
 
@@ -54,19 +58,22 @@ def _p(a: np.ndarray):
 
 @dataclass
 class SecretKey:
-    """lvl0 (n = 636) and lvl1 (N = 1024) binary keys."""
+    """lvl0 (n = 636), lvl1 (N = 1024) and lvl2 (N = 2048) binary keys."""
     lvl0: np.ndarray  # int32 [636]
     lvl1: np.ndarray  # int32 [1024]
     seed: int
+    lvl2: np.ndarray | None = None  # int32 [2048]
 
     @classmethod
     def generate(cls, seed: int) -> "SecretKey":
         lib = _load()
         k0 = np.empty(P.LVL0_N, np.int32)
         k1 = np.empty(P.LVL1_N, np.int32)
+        k2 = np.empty(P.LVL2_N, np.int32)
         lib.tfhe_keygen_binary(seed, 0, P.LVL0_N, _p(k0))
         lib.tfhe_keygen_binary(seed, 1, P.LVL1_N, _p(k1))
-        return cls(k0, k1, seed)
+        lib.tfhe_keygen_binary(seed, 2, P.LVL2_N, _p(k2))
+        return cls(k0, k1, seed, k2)
 
 
 @dataclass
@@ -90,8 +97,40 @@ class EvalKey:
         return cls(bk, ksk, keybundle)
 
 
-def _level_n(level: int) -> tuple[int, np.ndarray]:
-    return (P.LVL1_N, None) if level == 1 else (P.LVL0_N, None)
+@dataclass
+class EvalKey02:
+    """lvl0 -> lvl2 bootstrapping key (Torus64 TRGSW<lvl2>[636], or [318][3]
+    with KeyBundle) and lvl2 -> lvl0 key-switching key TLWE<lvl0>[2048][7][2]
+    (the keys Initialize_lvl02 takes, src/cufhe_gates_gpu.cu:75-90)."""
+    bk: np.ndarray   # uint64
+    ksk: np.ndarray  # uint32
+    keybundle: bool
+
+    @classmethod
+    def generate(cls, sk: SecretKey, keybundle: bool = True, seed: int | None = None) -> "EvalKey02":
+        lib = _load()
+        seed = sk.seed + 0x5EED02 if seed is None else seed
+        bk = np.empty(P.BK2KB_WORDS if keybundle else P.BK2_WORDS, np.uint64)
+        lib.tfhe_bk64_gen(seed, _p(sk.lvl0), P.LVL0_N, _p(sk.lvl2), P.LVL2_N, P.LVL2_L,
+                          P.LVL2_BGBIT, P.LVL2_ALPHA, int(keybundle), _p(bk))
+        ksk = np.empty(P.KSK20_WORDS, np.uint32)
+        lib.tfhe_ksk32_gen(seed + 1, _p(sk.lvl2), P.LVL2_N, _p(sk.lvl0), P.LVL0_N,
+                           P.LVL20_BASEBIT, P.LVL20_T, P.LVL0_ALPHA, _p(ksk))
+        return cls(bk, ksk, keybundle)
+
+
+def trlwe64_phase(sk: SecretKey, c: np.ndarray) -> np.ndarray:
+    lib = _load()
+    c = np.ascontiguousarray(c, dtype=np.uint64)
+    out = np.empty(P.LVL2_N, np.uint64)
+    lib.tfhe_trlwe64_phase(_p(sk.lvl2), P.LVL2_N, _p(c), _p(out))
+    return out
+
+
+def tlwe64_phase(sk: SecretKey, c: np.ndarray) -> int:
+    lib = _load()
+    c = np.ascontiguousarray(c, dtype=np.uint64)
+    return int(lib.tfhe_tlwe64_phase(_p(sk.lvl2), P.LVL2_N, _p(c)))
 
 
 def encrypt_bits(sk: SecretKey, bits: np.ndarray, level: int, seed: int,

@@ -331,3 +331,23 @@ void tfhe_ksk32_gen(uint64_t seed, const int32_t* key_src, uint32_t n_src,
             }
     }
 }
+
+/* ------------------------------------------------------------ Torus64 --- */
+/* phase polynomial b - a*s of a k = 1 Torus64 TRLWE */
+void tfhe_trlwe64_phase(const int32_t* key, uint32_t N, const uint64_t* c, uint64_t* phase)
+{
+    uint64_t* neg_a = (uint64_t*)malloc(sizeof(uint64_t) * N);
+    for (uint32_t i = 0; i < N; i++) {
+        neg_a[i] = 0ull - c[i];
+        phase[i] = c[N + i];
+    }
+    negacyclic_addmul_binary64(phase, neg_a, key, N);
+    free(neg_a);
+}
+
+uint64_t tfhe_tlwe64_phase(const int32_t* key, uint32_t n, const uint64_t* c)
+{
+    uint64_t p = c[n];
+    for (uint32_t i = 0; i < n; i++) p -= c[i] * (uint64_t)(uint32_t)key[i];
+    return p;
+}

@@ -252,4 +252,74 @@ __device__ __forceinline__ void ffnt_inverse_warp(double2 (&v)[16], double2* til
     for (int m = 0; m < 16; m++) v[m] = cmul(cmulc(v[m], u), c_utw16[m]);
 }
 
+// ---------------------------------------------------------------------------
+// Building blocks for N = 2048 (1024-point transform = two 512-point halves).
+// A forward transform of the even (odd) samples z[2m (+1)], m = lane + 32 n2,
+// whose twist psi2^{2m (+1)} = psi2^{2 lane (+1)} psi2^{64 n2} has the same
+// compile-time factor c_tw32[n2] as the N = 1024 case; the per-lane factor
+// t0 and the 512-point twiddle w512^{lane k2} = psi2^{8 lane k2} are merged
+// into the geometric sequence t0 * step^k2.  In: v[n2] already multiplied by
+// c_tw32[n2].  Out: natural bins, lane (k2 + 16 h), register m -> bin
+// k2 + 16 m + 256 h.
+__device__ __forceinline__ void dft512_fwd_post(double2 (&v)[16], double2* tile, int lane,
+                                                double2 t, const double2 step)
+{
+    dft16<1>(v);
+#pragma unroll
+    for (int k2 = 0; k2 < 16; k2++) {
+        v[k2] = cmul(v[k2], t);
+        if (k2 < 15) t = cmul(t, step);
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < 16; k2++) tile[k2 * 33 + lane] = v[k2];
+    __syncwarp();
+    const int k2 = lane & 15, h = lane >> 4;
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = tile[k2 * 33 + h + 2 * m];
+    __syncwarp();
+    dft16<1>(v);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        const double2 w = c_w32[m];
+        double2 tt = h ? cmul(v[m], w) : v[m];
+        double2 o;
+        o.x = __shfl_xor_sync(0xffffffffu, tt.x, 16);
+        o.y = __shfl_xor_sync(0xffffffffu, tt.y, 16);
+        v[m] = h ? csub(o, tt) : cadd(tt, o);
+    }
+}
+
+// Unscaled inverse 512-point DFT: in v[n2] = X[lane + 32 n2]; out v[m] =
+// sum_k X[k] w512^{-n k} for n = (lane & 15) + 16 m + 256 (lane >> 4).
+// wl = w512^{lane}.
+__device__ __forceinline__ void dft512_inv_raw(double2 (&v)[16], double2* tile, int lane,
+                                               const double2 wl)
+{
+    dft16<-1>(v);
+    double2 t = wl;
+#pragma unroll
+    for (int k2 = 1; k2 < 16; k2++) {
+        v[k2] = cmulc(v[k2], t);
+        if (k2 < 15) t = cmul(t, wl);
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < 16; k2++) tile[k2 * 33 + lane] = v[k2];
+    __syncwarp();
+    const int k2 = lane & 15, h = lane >> 4;
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = tile[k2 * 33 + h + 2 * m];
+    __syncwarp();
+    dft16<-1>(v);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+        double2 w = c_w32[m];
+        w.y = -w.y;
+        double2 tt = h ? cmul(v[m], w) : v[m];
+        double2 o;
+        o.x = __shfl_xor_sync(0xffffffffu, tt.x, 16);
+        o.y = __shfl_xor_sync(0xffffffffu, tt.y, 16);
+        v[m] = h ? csub(o, tt) : cadd(tt, o);
+    }
+}
+
 }  // namespace cufhe

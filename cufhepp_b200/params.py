@@ -20,6 +20,20 @@ BK_WORDS = LVL0_N * TRGSW1_WORDS
 BKKB_WORDS = (LVL0_N // 2) * 3 * TRGSW1_WORDS
 KSK_WORDS = LVL1_N * LVL10_T * 2 * TLWE0_WORDS
 
+LVL2_N = 2048
+LVL2_L = 4
+LVL2_BGBIT = 10
+LVL2_ALPHA = 2.0 ** -44
+MU64 = 1 << 61
+LVL20_BASEBIT = 2
+LVL20_T = 7
+TLWE2_WORDS = LVL2_N + 1           # 2049 (uint64)
+TRLWE2_WORDS = 2 * LVL2_N          # 4096 (uint64)
+TRGSW2_WORDS = 8 * TRLWE2_WORDS
+BK2_WORDS = LVL0_N * TRGSW2_WORDS
+BK2KB_WORDS = (LVL0_N // 2) * 3 * TRGSW2_WORDS
+KSK20_WORDS = LVL2_N * LVL20_T * 2 * TLWE0_WORDS
+
 # gate ids of the C-ABI (include/cufhe_b200.h)
 NAND, OR, ORYN, ORNY, AND, ANDYN, ANDNY, NOR, XOR, XNOR, NOT, COPY, MUX, NMUX = range(14)
 GATE_NAMES = ["Nand", "Or", "OrYN", "OrNY", "And", "AndYN", "AndNY", "Nor", "Xor", "Xnor",

@@ -58,6 +58,20 @@ def lib():
             "orc_ffnt_square": ([vp, vp, vp], None),
             "orc_negacyclic_mul_f64": ([vp, vp, vp], None),
             "orc_negacyclic_mul_exact": ([vp, vp, vp], None),
+            "orc_fft2_create": ([], vp),
+            "orc_fft2_destroy": ([vp], None),
+            "orc2_bk_to_fft": ([vp, vp, i, vp], None),
+            "orc2_decompose": ([vp, vp], None),
+            "orc2_extprod_exact": ([vp, vp, vp], None),
+            "orc2_cmux_step_exact": ([vp, vp, u32], None),
+            "orc2_cmux_step_fp64": ([vp, vp, vp, u32], None),
+            "orc2_blind_rotate_batch": ([vp, C.c_uint64, i64, vp, i, i, vp, i, vp], None),
+            "orc2_sample_extract": ([vp, vp], None),
+            "orc20_iks_batch": ([vp, vp, i64, vp], None),
+            "orc2_gate_batch": ([vp, vp, vp, vp, vp, i64, vp, vp, i, i, vp], None),
+            "orc2_ffnt_roundtrip": ([vp, vp, vp], None),
+            "orc2_ffnt_square": ([vp, vp, vp], None),
+            "orc_double_to_torus64": ([C.c_double], C.c_uint64),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -206,3 +220,109 @@ def negacyclic_mul_exact(d, key) -> np.ndarray:
     out = np.empty(N, np.uint32)
     lib().orc_negacyclic_mul_exact(_p(np.ascontiguousarray(d, np.int32)), _p(u32(key)), _p(out))
     return out
+
+
+# ------------------------------------------------ lvl0 -> lvl2 (Torus64) ---
+N2, HALF2, TRLWE2, TRGSW2, TLWE2 = 2048, 1024, 4096, 8 * 4096, 2049
+
+
+class FFT2:
+    """FFNT tables for N = 2048 (1024-point transform)."""
+
+    def __init__(self):
+        self.h = lib().orc_fft2_create()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_fft2_destroy(self.h)
+            self.h = None
+
+
+def u64(a):
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def bk2_to_fft(fft: FFT2, bk) -> np.ndarray:
+    bk = u64(bk)
+    ntrgsw = bk.size // TRGSW2
+    out = np.empty(ntrgsw * 16 * HALF2, np.complex128)
+    lib().orc2_bk_to_fft(fft.h, _p(bk), ntrgsw, _p(out))
+    return out
+
+
+def decompose2(poly) -> np.ndarray:
+    out = np.empty((4, N2), np.int32)
+    lib().orc2_decompose(_p(u64(poly)), _p(out))
+    return out
+
+
+def extprod2_exact(trgsw, trlwe) -> np.ndarray:
+    out = np.empty(TRLWE2, np.uint64)
+    lib().orc2_extprod_exact(_p(u64(trgsw)), _p(u64(trlwe)), _p(out))
+    return out
+
+
+def cmux2_step_exact(acc, bk_i, abar: int) -> np.ndarray:
+    acc = u64(acc).copy()
+    lib().orc2_cmux_step_exact(_p(acc), _p(u64(bk_i)), abar)
+    return acc
+
+
+def cmux2_step_fp64(fft: FFT2, acc, bkf_i, abar: int) -> np.ndarray:
+    acc = u64(acc).copy()
+    lib().orc2_cmux_step_fp64(fft.h, _p(acc), _p(np.ascontiguousarray(bkf_i, np.complex128)), abar)
+    return acc
+
+
+def blind_rotate2(x, mu: int, bk, kb: bool, mode: int, fft: FFT2 | None = None,
+                  steps: int = -1) -> np.ndarray:
+    x = u32(x).reshape(-1, TLWE0)
+    cnt = x.shape[0]
+    bkp = u64(bk) if mode == EXACT else np.ascontiguousarray(bk, np.complex128)
+    out = np.empty((cnt, TRLWE2), np.uint64)
+    lib().orc2_blind_rotate_batch(_p(x), mu, cnt, _p(bkp), int(kb), mode, fft.h if fft else None,
+                                  steps, _p(out))
+    return out
+
+
+def sample_extract2(acc) -> np.ndarray:
+    out = np.empty(TLWE2, np.uint64)
+    lib().orc2_sample_extract(_p(u64(acc)), _p(out))
+    return out
+
+
+def iks20_batch(tlwe2, ksk) -> np.ndarray:
+    tlwe2 = u64(tlwe2).reshape(-1, TLWE2)
+    out = np.empty((tlwe2.shape[0], TLWE0), np.uint32)
+    lib().orc20_iks_batch(_p(tlwe2), _p(u32(ksk)), tlwe2.shape[0], _p(out))
+    return out
+
+
+def gate2_batch(gates, in0, in1, in2, bk, ksk, kb: bool, mode: int,
+                fft: FFT2 | None = None) -> np.ndarray:
+    gates = np.ascontiguousarray(gates, np.int32)
+    cnt = gates.size
+    in0 = u32(in0).reshape(cnt, TLWE0)
+    in1 = None if in1 is None else u32(in1).reshape(cnt, TLWE0)
+    in2 = None if in2 is None else u32(in2).reshape(cnt, TLWE0)
+    bkp = u64(bk) if mode == EXACT else np.ascontiguousarray(bk, np.complex128)
+    out = np.empty((cnt, TLWE0), np.uint32)
+    lib().orc2_gate_batch(_p(gates), _p(in0), _p(in1), _p(in2), _p(out), cnt, _p(bkp),
+                          _p(u32(ksk)), int(kb), mode, fft.h if fft else None)
+    return out
+
+
+def ffnt2_roundtrip(fft: FFT2, x) -> np.ndarray:
+    out = np.empty(N2, np.float64)
+    lib().orc2_ffnt_roundtrip(fft.h, _p(np.ascontiguousarray(x, np.float64)), _p(out))
+    return out
+
+
+def ffnt2_square(fft: FFT2, x) -> np.ndarray:
+    out = np.empty(N2, np.float64)
+    lib().orc2_ffnt_square(fft.h, _p(np.ascontiguousarray(x, np.float64)), _p(out))
+    return out
+
+
+def double_to_torus64(d: float) -> int:
+    return int(lib().orc_double_to_torus64(d))

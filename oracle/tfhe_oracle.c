@@ -611,3 +611,454 @@ void orc_negacyclic_mul_exact(const int32_t* d, const uint32_t* key, uint32_t* o
     memset(out, 0, sizeof(uint32_t) * O_N);
     negacyclic_mac_exact(out, d, key);
 }
+
+/* ===================================================================== */
+/* lvl0 -> lvl2 gate bootstrapping (N = 2048, k = 1, l = 4, Bgbit = 10,   */
+/* Torus64) and lvl2 -> lvl0 key switching (basebit 2, t 7): the          */
+/* *_lvl02 gates (src/cufhe_gates_gpu.cu:826-979), same templates at      */
+/* lvl02param / lvl20param.                                               */
+/* ===================================================================== */
+#define O2_N 2048
+#define O2_NBIT 11
+#define O2_HALF 1024
+#define O2_L 4
+#define O2_BGBIT 10
+#define O2_ROWS 8
+#define O2_TRLWE (2 * O2_N)
+#define O2_TRGSW (O2_ROWS * O2_TRLWE)
+#define O2_TLWE2 (O2_N + 1)
+
+static void rotate_poly64(uint64_t* out, const uint64_t* p, uint32_t a)
+{
+    const uint32_t am = a & (O2_N - 1), neg = a >> O2_NBIT;
+    for (uint32_t n = 0; n < O2_N; n++) {
+        const uint64_t v = p[(n - a) & (O2_N - 1)];
+        out[n] = ((n < am) ^ neg) ? 0ull - v : v;
+    }
+}
+
+/* l = 4 signed digits of 10 bits (include/gatebootstrapping_gpu.cuh:20-29) */
+void orc2_decompose(const uint64_t* poly, int32_t* digits)
+{
+    uint64_t off = 0;
+    for (int i = 1; i <= O2_L; i++) off += (uint64_t)512 << (64 - i * O2_BGBIT);
+    const uint64_t round = 1ull << (64 - O2_L * O2_BGBIT - 1);
+    for (int n = 0; n < O2_N; n++) {
+        const uint64_t t = poly[n] + off + round;
+        for (int d = 0; d < O2_L; d++)
+            digits[d * O2_N + n] = (int32_t)((t >> (64 - (d + 1) * O2_BGBIT)) & 1023u) - 512;
+    }
+}
+
+static void negacyclic_mac_exact64(uint64_t* restrict out, const int32_t* restrict d,
+                                   const uint64_t* restrict key)
+{
+    for (int m = 0; m < O2_N; m++) {
+        const uint64_t dm = (uint64_t)(int64_t)d[m];
+        if (!dm) continue;
+        const uint64_t* kw = key + O2_N - m;
+        for (int n = 0; n < m; n++) out[n] -= dm * kw[n];
+        const uint64_t* kp = key - m;
+        for (int n = m; n < O2_N; n++) out[n] += dm * kp[n];
+    }
+}
+
+void orc2_extprod_exact(const uint64_t* trgsw, const uint64_t* in, uint64_t* out)
+{
+    int32_t* dig = (int32_t*)malloc(sizeof(int32_t) * O2_L * O2_N);
+    memset(out, 0, sizeof(uint64_t) * O2_TRLWE);
+    for (int j = 0; j < 2; j++) {
+        orc2_decompose(in + j * O2_N, dig);
+        for (int d = 0; d < O2_L; d++) {
+            const int r = j * O2_L + d;
+            for (int oj = 0; oj < 2; oj++)
+                negacyclic_mac_exact64(out + oj * O2_N, dig + d * O2_N,
+                                       trgsw + ((size_t)r * 2 + oj) * O2_N);
+        }
+    }
+    free(dig);
+}
+
+void orc2_cmux_step_exact(uint64_t* acc, const uint64_t* bk_i, uint32_t abar)
+{
+    uint64_t* diff = (uint64_t*)malloc(sizeof(uint64_t) * 2 * O2_TRLWE);
+    uint64_t* prod = diff + O2_TRLWE;
+    for (int j = 0; j < 2; j++) {
+        rotate_poly64(diff + j * O2_N, acc + j * O2_N, abar);
+        for (int n = 0; n < O2_N; n++) diff[j * O2_N + n] -= acc[j * O2_N + n];
+    }
+    orc2_extprod_exact(bk_i, diff, prod);
+    for (int i = 0; i < O2_TRLWE; i++) acc[i] += prod[i];
+    free(diff);
+}
+
+void orc2_kb_step_exact(uint64_t* acc, const uint64_t* bk3, uint32_t a0, uint32_t a1)
+{
+    uint64_t* kb = (uint64_t*)calloc(O2_TRGSW, sizeof(uint64_t));
+    uint64_t* rot = (uint64_t*)malloc(sizeof(uint64_t) * (O2_N + O2_TRLWE));
+    uint64_t* out = rot + O2_N;
+    const uint32_t a01 = (a0 + a1) & (2 * O2_N - 1);
+    const uint32_t av[3] = {a01, a0, a1};
+    for (int r = 0; r < O2_ROWS; r++) {
+        const int j = r / O2_L, d = r % O2_L;
+        kb[((size_t)r * 2 + j) * O2_N] += 1ull << (64 - (d + 1) * O2_BGBIT);
+        for (int e = 0; e < 3; e++)
+            for (int oj = 0; oj < 2; oj++) {
+                const uint64_t* p = bk3 + (size_t)e * O2_TRGSW + ((size_t)r * 2 + oj) * O2_N;
+                uint64_t* q = kb + ((size_t)r * 2 + oj) * O2_N;
+                rotate_poly64(rot, p, av[e]);
+                for (int n = 0; n < O2_N; n++) q[n] += rot[n] - p[n];
+            }
+    }
+    orc2_extprod_exact(kb, acc, out);
+    memcpy(acc, out, sizeof(uint64_t) * O2_TRLWE);
+    free(rot);
+    free(kb);
+}
+
+/* ---- FP64 FFNT for N = 2048 (1024-point transform) ---- */
+typedef struct {
+    double complex twist[O2_HALF];
+    double complex untwist[O2_HALF];
+    double complex root[O2_HALF];   /* e^{2 pi i k / 1024} */
+    double complex psi[2 * O2_N];   /* e^{i pi t / 2048}: KeyBundle factors by evaluation */
+    uint16_t bitrev[O2_HALF];
+} orc_fft2_t;
+
+orc_fft2_t* orc_fft2_create(void)
+{
+    orc_fft2_t* c = (orc_fft2_t*)calloc(1, sizeof(orc_fft2_t));
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i < O2_HALF; i++) {
+        const long double tw = pi * i / O2_N;
+        c->twist[i] = (double)cosl(tw) + I * (double)sinl(tw);
+        c->untwist[i] = ((double)cosl(tw) - I * (double)sinl(tw)) / O2_HALF;
+        const long double ro = 2 * pi * i / O2_HALF;
+        c->root[i] = (double)cosl(ro) + I * (double)sinl(ro);
+        int r = 0;
+        for (int b = 0; b < 10; b++) r |= ((i >> b) & 1) << (9 - b);
+        c->bitrev[i] = (uint16_t)r;
+    }
+    for (int t = 0; t < 2 * O2_N; t++) {
+        const long double a = pi * t / O2_N;
+        c->psi[t] = (double)cosl(a) + I * (double)sinl(a);
+    }
+    return c;
+}
+
+void orc_fft2_destroy(orc_fft2_t* c) { free(c); }
+
+static void fft1024(const orc_fft2_t* c, double complex* x, int inverse)
+{
+    for (int i = 0; i < O2_HALF; i++) {
+        const int j = c->bitrev[i];
+        if (i < j) {
+            double complex t = x[i];
+            x[i] = x[j];
+            x[j] = t;
+        }
+    }
+    for (int len = 2; len <= O2_HALF; len <<= 1) {
+        const int half = len >> 1, step = O2_HALF / len;
+        for (int s = 0; s < O2_HALF; s += len)
+            for (int k = 0; k < half; k++) {
+                double complex w = c->root[k * step];
+                if (inverse) w = conj(w);
+                const double complex u = x[s + k], v = x[s + k + half] * w;
+                x[s + k] = u + v;
+                x[s + k + half] = u - v;
+            }
+    }
+}
+
+static void ffnt2_forward(const orc_fft2_t* c, const double* re, double complex* out)
+{
+    for (int i = 0; i < O2_HALF; i++) out[i] = (re[i] + I * re[i + O2_HALF]) * c->twist[i];
+    fft1024(c, out, 0);
+}
+
+/* FP64 -> Torus64 as include/utils_gpu.cuh:48-65 (mantissa shift, wraps mod 2^64) */
+uint64_t orc_double_to_torus64(double d)
+{
+    uint64_t i;
+    memcpy(&i, &d, 8);
+    const int expo = (int)(i >> 52) & 0x7FF;
+    if (expo == 0) return 0;
+    const uint64_t m = (i & 0x000FFFFFFFFFFFFFull) | 0x0010000000000000ull;
+    const int shift = expo - 1075;
+    uint64_t val;
+    if (shift >= 64)
+        val = 0;
+    else if (shift >= 0)
+        val = m << shift;
+    else if (shift > -64)
+        val = m >> (-shift);
+    else
+        val = 0;
+    return (i >> 63) ? 0ull - val : val;
+}
+
+void orc2_bk_to_fft(const orc_fft2_t* c, const uint64_t* bk, int ntrgsw, double complex* out)
+{
+#pragma omp parallel for schedule(static)
+    for (int p = 0; p < ntrgsw * O2_ROWS * 2; p++) {
+        double* re = (double*)malloc(sizeof(double) * O2_N);
+        for (int i = 0; i < O2_N; i++)
+            re[i] = (double)(int64_t)bk[(size_t)p * O2_N + i] * (1.0 / 18446744073709551616.0);
+        ffnt2_forward(c, re, out + (size_t)p * O2_HALF);
+        free(re);
+    }
+}
+
+static void ffnt2_inverse_round(const orc_fft2_t* c, double complex* acc, uint64_t* out, int add)
+{
+    fft1024(c, acc, 1);
+    for (int i = 0; i < O2_HALF; i++) {
+        const double complex v = acc[i] * c->untwist[i];
+        const uint64_t lo = orc_double_to_torus64(creal(v) * 18446744073709551616.0);
+        const uint64_t hi = orc_double_to_torus64(cimag(v) * 18446744073709551616.0);
+        if (add) {
+            out[i] += lo;
+            out[i + O2_HALF] += hi;
+        } else {
+            out[i] = lo;
+            out[i + O2_HALF] = hi;
+        }
+    }
+}
+
+static void digits2_fft(const orc_fft2_t* c, const uint64_t* in, double complex* spec /*[8][1024]*/)
+{
+    int32_t* dig = (int32_t*)malloc(sizeof(int32_t) * O2_L * O2_N);
+    double* re = (double*)malloc(sizeof(double) * O2_N);
+    for (int j = 0; j < 2; j++) {
+        orc2_decompose(in + j * O2_N, dig);
+        for (int d = 0; d < O2_L; d++) {
+            for (int i = 0; i < O2_N; i++) re[i] = (double)dig[d * O2_N + i];
+            ffnt2_forward(c, re, spec + (size_t)(j * O2_L + d) * O2_HALF);
+        }
+    }
+    free(re);
+    free(dig);
+}
+
+void orc2_cmux_step_fp64(const orc_fft2_t* c, uint64_t* acc, const double complex* bkf_i,
+                         uint32_t abar)
+{
+    uint64_t* diff = (uint64_t*)malloc(sizeof(uint64_t) * O2_TRLWE);
+    double complex* spec = (double complex*)malloc(sizeof(double complex) * (O2_ROWS + 2) * O2_HALF);
+    double complex* accf = spec + O2_ROWS * O2_HALF;
+    for (int j = 0; j < 2; j++) {
+        rotate_poly64(diff + j * O2_N, acc + j * O2_N, abar);
+        for (int n = 0; n < O2_N; n++) diff[j * O2_N + n] -= acc[j * O2_N + n];
+    }
+    digits2_fft(c, diff, spec);
+    memset(accf, 0, sizeof(double complex) * 2 * O2_HALF);
+    for (int r = 0; r < O2_ROWS; r++)
+        for (int oj = 0; oj < 2; oj++)
+            for (int f = 0; f < O2_HALF; f++)
+                accf[oj * O2_HALF + f] +=
+                    spec[r * O2_HALF + f] * bkf_i[((size_t)r * 2 + oj) * O2_HALF + f];
+    for (int oj = 0; oj < 2; oj++) ffnt2_inverse_round(c, accf + oj * O2_HALF, acc + oj * O2_N, 1);
+    free(spec);
+    free(diff);
+}
+
+void orc2_kb_step_fp64(const orc_fft2_t* c, uint64_t* acc, const double complex* bkf3, uint32_t a0,
+                       uint32_t a1)
+{
+    double complex* spec = (double complex*)malloc(sizeof(double complex) * (O2_ROWS + 2) * O2_HALF);
+    double complex* accf = spec + O2_ROWS * O2_HALF;
+    const uint32_t a01 = (a0 + a1) & (2 * O2_N - 1);
+    const size_t trgsw_f = (size_t)O2_ROWS * 2 * O2_HALF;
+    digits2_fft(c, acc, spec);
+    memset(accf, 0, sizeof(double complex) * 2 * O2_HALF);
+    for (int f = 0; f < O2_HALF; f++) {
+        const uint32_t e = 1u + 4u * (uint32_t)f;
+        const double complex x0 = c->psi[(e * a0) & (2 * O2_N - 1)] - 1.0;
+        const double complex x1 = c->psi[(e * a1) & (2 * O2_N - 1)] - 1.0;
+        const double complex x01 = c->psi[(e * a01) & (2 * O2_N - 1)] - 1.0;
+        for (int r = 0; r < O2_ROWS; r++) {
+            const int j = r / O2_L, d = r % O2_L;
+            const double h = ldexp(1.0, -(d + 1) * O2_BGBIT);
+            for (int oj = 0; oj < 2; oj++) {
+                const size_t o = ((size_t)r * 2 + oj) * O2_HALF + f;
+                double complex comb = (oj == j) ? h : 0.0;
+                comb += bkf3[2 * trgsw_f + o] * x1;
+                comb += bkf3[1 * trgsw_f + o] * x0;
+                comb += bkf3[0 * trgsw_f + o] * x01;
+                accf[oj * O2_HALF + f] += spec[r * O2_HALF + f] * comb;
+            }
+        }
+    }
+    for (int oj = 0; oj < 2; oj++) ffnt2_inverse_round(c, accf + oj * O2_HALF, acc + oj * O2_N, 0);
+    free(spec);
+}
+
+void orc2_test_vector(uint32_t bar, uint64_t mu, uint64_t* acc)
+{
+    for (uint32_t i = 0; i < O2_N; i++) {
+        acc[i] = 0;
+        if (bar == 2 * O2_N)
+            acc[O2_N + i] = mu;
+        else
+            acc[O2_N + i] = ((i < (bar & (O2_N - 1))) ^ (bar >> O2_NBIT)) ? 0ull - mu : mu;
+    }
+}
+
+/* lvl0 TLWE -> lvl2 TRLWE: bar = 2N - (b >> 20), abar = (a + 2^19) >> 20 */
+void orc2_blind_rotate(const uint32_t* x, uint64_t mu, const void* bk, int kb, int mode,
+                       const orc_fft2_t* c, int steps, uint64_t* acc)
+{
+    const uint32_t bar = 2 * O2_N - (x[O_N0] >> (32 - 1 - O2_NBIT));
+    orc2_test_vector(bar, mu, acc);
+    const uint32_t ro = 1u << (32 - 2 - O2_NBIT);
+    const size_t trgsw_f = (size_t)O2_ROWS * 2 * O2_HALF;
+    if (!kb) {
+        const int n = steps < 0 || steps > O_N0 ? O_N0 : steps;
+        for (int i = 0; i < n; i++) {
+            const uint32_t ab = (x[i] + ro) >> (32 - 1 - O2_NBIT);
+            if (mode == ORC_EXACT)
+                orc2_cmux_step_exact(acc, (const uint64_t*)bk + (size_t)i * O2_TRGSW, ab);
+            else
+                orc2_cmux_step_fp64(c, acc, (const double complex*)bk + (size_t)i * trgsw_f, ab);
+        }
+    } else {
+        const int n = steps < 0 || steps > O_N0 / 2 ? O_N0 / 2 : steps;
+        for (int p = 0; p < n; p++) {
+            const uint32_t a0 = (x[2 * p] + ro) >> (32 - 1 - O2_NBIT);
+            const uint32_t a1 = (x[2 * p + 1] + ro) >> (32 - 1 - O2_NBIT);
+            if (mode == ORC_EXACT)
+                orc2_kb_step_exact(acc, (const uint64_t*)bk + (size_t)p * 3 * O2_TRGSW, a0, a1);
+            else
+                orc2_kb_step_fp64(c, acc, (const double complex*)bk + (size_t)p * 3 * trgsw_f, a0, a1);
+        }
+    }
+}
+
+void orc2_sample_extract(const uint64_t* acc, uint64_t* tlwe2)
+{
+    tlwe2[0] = acc[0];
+    for (int n = 1; n < O2_N; n++) tlwe2[n] = 0ull - acc[O2_N - n];
+    tlwe2[O2_N] = acc[O2_N];
+}
+
+/* lvl2 -> lvl0 identity key switching (KeySwitchFromTLWE<lvl20param>,
+ * include/keyswitch_gpu.cuh:128-187; Torus64 -> Torus32 conversion of b with
+ * rounding, :33-50).  ksk: TLWE<lvl0>[2048][7][2]. */
+void orc20_iks(const uint64_t* in, const uint32_t* ksk, uint32_t* out)
+{
+    uint64_t decomp = 0;
+    for (int i = 1; i <= O_T; i++) decomp += 2ull << (64 - i * O_BASEBIT);
+    const uint64_t round = 1ull << (64 - (1 + O_BASEBIT * O_T));
+    uint32_t res[O_TLWE0];
+    memset(res, 0, sizeof(res));
+    res[O_N0] = (uint32_t)((in[O2_N] + (1ull << 31)) >> 32);
+    for (int i = 0; i < O2_N; i++) {
+        const uint64_t t = in[i] + decomp + round;
+        for (int j = 0; j < O_T; j++) {
+            const int32_t v = (int32_t)((t >> (64 - (j + 1) * O_BASEBIT)) & 3u) - 2;
+            if (v == 0) continue;
+            const uint32_t* row =
+                ksk + (((size_t)i * O_T + j) * 2 + (v > 0 ? v - 1 : -v - 1)) * O_TLWE0;
+            if (v > 0)
+                for (int o = 0; o < O_TLWE0; o++) res[o] -= row[o];
+            else
+                for (int o = 0; o < O_TLWE0; o++) res[o] += row[o];
+        }
+    }
+    memcpy(out, res, sizeof(res));
+}
+
+/* *_lvl02 gates: Ctxt<lvl0> I/O, lvl0 pre-add, blind rotation to lvl2, mux
+ * combination on the TRLWE (+mu2), SampleExtract, key switch lvl2 -> lvl0. */
+void orc2_gate(int gate, const uint32_t* in0, const uint32_t* in1, const uint32_t* in2,
+               uint32_t* out, const void* bk, const uint32_t* ksk, int kb, int mode,
+               const orc_fft2_t* c)
+{
+    const uint64_t mu2 = 1ull << 61;
+    if (gate == G_NOT || gate == G_COPY) {
+        for (int i = 0; i < O_TLWE0; i++) out[i] = gate == G_NOT ? 0u - in0[i] : in0[i];
+        return;
+    }
+    uint64_t* acc = (uint64_t*)malloc(sizeof(uint64_t) * (O2_TRLWE + 2 * O2_TLWE2));
+    uint64_t* t2 = acc + O2_TRLWE;
+    uint64_t* sum = t2 + O2_TLWE2;
+    uint32_t x0[O_TLWE0];
+    int32_t ca, cb;
+    uint32_t off;
+    const int mux = gate == G_MUX || gate == G_NMUX;
+    memset(sum, 0, sizeof(uint64_t) * O2_TLWE2);
+    for (int ln = 0; ln < (mux ? 2 : 1); ln++) {
+        const uint32_t* b;
+        if (mux) {
+            b = ln == 0 ? in1 : in2;
+            ca = ln == 0 ? 1 : -1;
+            cb = 1;
+            off = 0u - O_MU;
+        } else {
+            b = in1;
+            gate_table(gate, &ca, &cb, &off);
+        }
+        preadd0(in0, b, ca, cb, off, x0);
+        orc2_blind_rotate(x0, mu2, bk, kb, mode, c, -1, acc);
+        orc2_sample_extract(acc, t2);
+        for (int i = 0; i < O2_TLWE2; i++) sum[i] += t2[i];
+    }
+    if (gate == G_MUX) sum[O2_N] += mu2;
+    if (gate == G_NMUX) {
+        for (int i = 0; i < O2_TLWE2; i++) sum[i] = 0ull - sum[i];
+        sum[O2_N] -= mu2;
+    }
+    orc20_iks(sum, ksk, out);
+    free(acc);
+}
+
+void orc2_gate_batch(const int32_t* gates, const uint32_t* in0, const uint32_t* in1,
+                     const uint32_t* in2, uint32_t* out, int64_t count, const void* bk,
+                     const uint32_t* ksk, int kb, int mode, const orc_fft2_t* c)
+{
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t g = 0; g < count; g++)
+        orc2_gate(gates[g], in0 + g * O_TLWE0, in1 ? in1 + g * O_TLWE0 : NULL,
+                  in2 ? in2 + g * O_TLWE0 : NULL, out + g * O_TLWE0, bk, ksk, kb, mode, c);
+}
+
+void orc2_blind_rotate_batch(const uint32_t* x, uint64_t mu, int64_t count, const void* bk,
+                             int kb, int mode, const orc_fft2_t* c, int steps, uint64_t* acc_out)
+{
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t g = 0; g < count; g++)
+        orc2_blind_rotate(x + g * O_TLWE0, mu, bk, kb, mode, c, steps, acc_out + g * O2_TRLWE);
+}
+
+void orc20_iks_batch(const uint64_t* in, const uint32_t* ksk, int64_t count, uint32_t* out)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < count; g++) orc20_iks(in + g * O2_TLWE2, ksk, out + g * O_TLWE0);
+}
+
+void orc2_ffnt_roundtrip(const orc_fft2_t* c, const double* in, double* out)
+{
+    double complex z[O2_HALF];
+    ffnt2_forward(c, in, z);
+    fft1024(c, z, 1);
+    for (int i = 0; i < O2_HALF; i++) {
+        const double complex v = z[i] * c->untwist[i];
+        out[i] = creal(v);
+        out[i + O2_HALF] = cimag(v);
+    }
+}
+
+void orc2_ffnt_square(const orc_fft2_t* c, const double* in, double* out)
+{
+    double complex z[O2_HALF];
+    ffnt2_forward(c, in, z);
+    for (int i = 0; i < O2_HALF; i++) z[i] = z[i] * z[i];
+    fft1024(c, z, 1);
+    for (int i = 0; i < O2_HALF; i++) {
+        const double complex v = z[i] * c->untwist[i];
+        out[i] = creal(v);
+        out[i + O2_HALF] = cimag(v);
+    }
+}

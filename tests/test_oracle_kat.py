@@ -1,9 +1,9 @@
 """Pins the oracle on the reference's own known-answer tests.
 
-* test/test_accumulate_diag.cu:533-605  -- zero TRGSW, abar = 0: unchanged.
-* test/test_accumulate_diag.cu:405-531  -- noiseless TRGSW(1) (gadget rows
-  only, :369-403), abar = 1, (a = 0, b = vec(mu)) -> b = (-mu, mu, ..., mu),
-  tolerance 1 for Torus32 (:510-511).
+* test/test_accumulate_diag.cu:266-336  -- zero TRGSW, abar = 0: unchanged.
+* test/test_accumulate_diag.cu:137-262  -- noiseless TRGSW(1) (gadget rows
+  only, :101-134), abar = 1, (a = 0, b = vec(mu)) -> b = (-mu, mu, ..., mu),
+  tolerance 1 for Torus32 (:241-243).
 * test/test_fft_roundtrip.cu:141-184    -- mt19937(42) reals round-trip < 1e-6.
 * test/test_fft_roundtrip.cu:186-243    -- (1+X+X^2)^2 negacyclic < 1e-6.
 * test/test_fft_roundtrip.cu:245-295    -- mt19937(123) ints in [-5,5] squared < 0.5.
