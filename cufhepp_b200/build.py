@@ -32,6 +32,7 @@ ENGINE_SOURCES = [
     "gates_misc.cu",
     "peaks.cu",
     "noalloc.cu",
+    "br_fp64_lvl02.cu",
 ]
 
 

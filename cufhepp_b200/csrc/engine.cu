@@ -34,6 +34,13 @@ struct DeviceState {
     Int8Key i8;              // INT8 exact-path key (non-KeyBundle only)
     uint8_t* iks_key = nullptr;  // KSK as signed byte-limb tiles (tensor-core IKS)
     int* err = nullptr;          // set by a device wait that timed out
+    // lvl0 -> lvl2 path (Initialize_lvl02)
+    bool ready2 = false;
+    int kb2 = 0;
+    double2* bkf2 = nullptr;     // FP64 Fourier-domain BK<lvl2>
+    double2* psi2 = nullptr;     // psi2^s, s <= 512
+    uint8_t* iks2_key = nullptr; // lvl20 KSK byte-limb tiles
+    int* err2 = nullptr;
 };
 
 struct Workspace {
@@ -49,6 +56,9 @@ struct Workspace {
     cudaEvent_t stage_ev = nullptr;
     Int8Workspace i8;
     IksWorkspace iks;
+    size_t lane2_cap = 0;
+    uint64_t* lane_out2 = nullptr;  // lvl2 lane outputs [lanes][2049]
+    IksWorkspace iks2;
 };
 
 }  // namespace
@@ -143,6 +153,8 @@ void free_ws(Workspace& w)
     if (w.stage_ev) cudaEventDestroy(w.stage_ev);
     int8_workspace_free(w.i8);
     iks_tc_workspace_free(w.iks);
+    cudaFree(w.lane_out2);
+    iks_tc_workspace_free(w.iks2);
     w = Workspace();
 }
 
@@ -203,10 +215,26 @@ void host_tables(std::vector<double2>& psi, std::vector<double2>& tw)
         }
 }
 
+void release_device02(int d)
+{
+    DeviceState& D = g_dev[d];
+    cudaSetDevice(d);
+    cudaFree(D.bkf2);
+    cudaFree(D.psi2);
+    cudaFree(D.iks2_key);
+    cudaFree(D.err2);
+    D.bkf2 = D.psi2 = nullptr;
+    D.iks2_key = nullptr;
+    D.err2 = nullptr;
+    D.ready2 = false;
+    D.kb2 = 0;
+}
+
 void release_device(int d)
 {
     DeviceState& D = g_dev[d];
     cudaSetDevice(d);
+    release_device02(d);
     cudaFree(D.ksk);
     cudaFree(D.bkf);
     cudaFree(D.psi);
@@ -255,6 +283,44 @@ int init_device(int d, const cufhe_keyview* ek)
     cudaFree(raw);
     D.kb = ek->keybundle;
     D.ready = true;
+    return CUFHE_OK;
+}
+
+// Initialize_lvl02 on device d (src/cufhe_gates_gpu.cu:75-90): FFT tables of
+// N = 2048, Fourier BK<lvl2>, lvl20 key tiles
+int init_device02(int d, const cufhe_keyview02* ek)
+{
+    DeviceState& D = g_dev[d];
+    CK(cudaSetDevice(d));
+    CK(upload_fft2_constants());
+    std::vector<double2> tab(kPsi2Entries, make_double2(0.0, 0.0));
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int t = 0; t <= 512; t++) {
+        const long double a = pi * t / CUFHE_LVL2_N;
+        tab[t] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    CK(cudaMalloc(&D.psi2, tab.size() * sizeof(double2)));
+    CK(cudaMemcpy(D.psi2, tab.data(), tab.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&D.err2, sizeof(int)));
+    CK(cudaMemset(D.err2, 0, sizeof(int)));
+
+    uint32_t* ksk = nullptr;
+    CK(cudaMalloc(&ksk, ek->ksk_words * sizeof(uint32_t)));
+    CK(cudaMemcpy(ksk, ek->ksk, ek->ksk_words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&D.iks2_key, iks20_tc_key_bytes()));
+    CKL(iks20_tc_key_build(ksk, D.iks2_key, 0));
+
+    uint64_t* raw = nullptr;
+    CK(cudaMalloc(&raw, ek->bk_words * sizeof(uint64_t)));
+    CK(cudaMemcpy(raw, ek->bk, ek->bk_words * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    const int npolys = (int)(ek->bk_words / CUFHE_LVL2_N);
+    CK(cudaMalloc(&D.bkf2, (size_t)npolys * 1024 * sizeof(double2)));
+    CKL(launch_bk2_to_fft(raw, npolys, D.psi2, D.bkf2, 0));
+    CK(cudaDeviceSynchronize());
+    cudaFree(raw);
+    cudaFree(ksk);
+    D.kb2 = ek->keybundle;
+    D.ready2 = true;
     return CUFHE_OK;
 }
 
@@ -340,13 +406,55 @@ int run_iks(cufhe_stream_s* s, int mode, const Plan& plan, const uint32_t* in0, 
 int check_device_error(int d)
 {
     DeviceState& D = g_dev[d];
-    if (!D.ready || !D.err) return CUFHE_OK;
-    int h = 0;
-    CK(cudaMemcpy(&h, D.err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (h) {
-        cudaMemset(D.err, 0, sizeof(int));
-        return fail(CUFHE_ERR_CUDA, "a tensor-core kernel's bounded wait timed out (code %d)", h);
+    int* flags[2] = {D.ready ? D.err : nullptr, D.ready2 ? D.err2 : nullptr};
+    for (int* f : flags) {
+        if (!f) continue;
+        int h = 0;
+        CK(cudaMemcpy(&h, f, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) {
+            cudaMemset(f, 0, sizeof(int));
+            return fail(CUFHE_ERR_CUDA, "a tensor-core kernel's bounded wait timed out (code %d)", h);
+        }
     }
+    return CUFHE_OK;
+}
+
+// lvl2 -> lvl0 key switching of gates on the tensor cores
+int run_iks20(cufhe_stream_s* s, const Plan& plan, const uint64_t* lane_out, uint32_t* dst)
+{
+    DeviceState& D = g_dev[s->device];
+    int launches = 0;
+    ProfRec pr;
+    prof_begin(s->st, pr, CUFHE_K_IKS_LVL20);
+    cudaError_t e = launch_iks20_tc(plan, lane_out, D.iks2_key, dst, s->ws.iks2, D.err2, s->st,
+                                    &launches);
+    prof_end(s->st, pr);
+    g_launches.fetch_add(launches);
+    if (e != cudaSuccess) return fail(CUFHE_ERR_CUDA, "lvl20 key switching: %s", cudaGetErrorString(e));
+    return CUFHE_OK;
+}
+
+int run_br2(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint64_t mu, int steps,
+            uint64_t* acc_out, uint64_t* lane_out)
+{
+    DeviceState& D = g_dev[s->device];
+    LAUNCH(CUFHE_K_BR_FP64_LVL02, s->st,
+           launch_br2_fp64(D.kb2 != 0, lane_in, lanes, mu, D.bkf2, D.psi2, steps, acc_out, lane_out,
+                           s->st));
+    return CUFHE_OK;
+}
+
+int ensure_lane2(cufhe_stream_s* s, size_t lanes)
+{
+    Workspace& w = s->ws;
+    if (lanes <= w.lane2_cap) return CUFHE_OK;
+    CK(cudaStreamSynchronize(s->st));
+    cudaFree(w.lane_out2);
+    w.lane_out2 = nullptr;
+    const size_t cap = lanes < 256 ? 256 : lanes;
+    if (cudaMalloc(&w.lane_out2, cap * CUFHE_TLWE2_WORDS * sizeof(uint64_t)) != cudaSuccess)
+        return fail(CUFHE_ERR_NOMEM, "lvl2 lane buffer for %zu lanes", cap);
+    w.lane2_cap = cap;
     return CUFHE_OK;
 }
 
@@ -377,8 +485,11 @@ int run_br(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint32_t mu, i
 int run_batch(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count, int level,
               uint32_t* out, const uint32_t* in0, const uint32_t* in1, const uint32_t* in2)
 {
-    if (!g_dev[s->device].ready) return fail(CUFHE_ERR_STATE, "cufhe_initialize() not called");
-    if (level != CUFHE_LVL0 && level != CUFHE_LVL1) return fail(CUFHE_ERR_ARG, "bad level %d", level);
+    if (level != CUFHE_LVL0 && level != CUFHE_LVL1 && level != CUFHE_LVL02)
+        return fail(CUFHE_ERR_ARG, "bad level %d", level);
+    if (level == CUFHE_LVL02 ? !g_dev[s->device].ready2 : !g_dev[s->device].ready)
+        return fail(CUFHE_ERR_STATE, level == CUFHE_LVL02 ? "cufhe_initialize_lvl02() not called"
+                                                         : "cufhe_initialize() not called");
     if (count == 0) return CUFHE_OK;
     if (count > (1u << 24)) return fail(CUFHE_ERR_ARG, "batch of %zu gates too large", count);
     if (!out || !in0) return fail(CUFHE_ERR_ARG, "null ciphertext pointer");
@@ -397,9 +508,18 @@ int run_batch(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count
     Plan plan;
     int rc = build_plan(s, gates, uniform, count, plan);
     if (rc) return rc;
-    DeviceState& D = g_dev[s->device];
     Workspace& w = s->ws;
-    if (plan.lanes) {
+    if (plan.lanes && level == CUFHE_LVL02) {
+        // *_lvl02 gates: lvl0 pre-add, blind rotation to lvl2, combination +
+        // key switching lvl2 -> lvl0 (src/cufhe_gates_gpu.cu:826-979)
+        rc = ensure_lane2(s, plan.lanes);
+        if (rc) return rc;
+        LAUNCH(CUFHE_K_PREADD, s->st, launch_preadd_lvl0(plan, in0, in1, in2, w.lane_in, s->st));
+        rc = run_br2(s, w.lane_in, plan.lanes, CUFHE_MU64, -1, nullptr, w.lane_out2);
+        if (rc) return rc;
+        rc = run_iks20(s, plan, w.lane_out2, out);
+        if (rc) return rc;
+    } else if (plan.lanes) {
         if (level == CUFHE_LVL1) {
             rc = run_iks(s, 0, plan, in0, in1, in2, nullptr, w.lane_in);
             if (rc) return rc;
@@ -422,6 +542,7 @@ int run_batch(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count
         if (has)
             LAUNCH(CUFHE_K_FINALIZE, s->st,
                    launch_not_copy(plan, level == CUFHE_LVL1 ? kTlwe1 : kTlwe0, in0, out, s->st));
+    // (lvl02 gates keep Ctxt<lvl0> I/O, so Not/Copy work on TLWE<lvl0> there too)
     }
     return CUFHE_OK;
 }
@@ -494,6 +615,40 @@ int cufhe_cleanup(void)
 {
     for (int d = 0; d < kMaxDev; d++)
         if (g_dev[d].ready) release_device(d);
+    cudaSetDevice(0);
+    return CUFHE_OK;
+}
+
+int cufhe_initialize_lvl02(const cufhe_keyview02* ek)
+{
+    if (!ek || !ek->bk || !ek->ksk) return fail(CUFHE_ERR_ARG, "null key view");
+    const uint64_t want_bk = ek->keybundle ? CUFHE_BKKB2_WORDS : CUFHE_BK2_WORDS;
+    if (ek->bk_words != want_bk)
+        return fail(CUFHE_ERR_ARG, "lvl02 bootstrapping key has %zu words, expected %llu",
+                    ek->bk_words, (unsigned long long)want_bk);
+    if (ek->ksk_words != CUFHE_KSK20_WORDS)
+        return fail(CUFHE_ERR_ARG, "lvl20 key-switching key has %zu words, expected %llu",
+                    ek->ksk_words, (unsigned long long)CUFHE_KSK20_WORDS);
+    int avail = 0;
+    if (cudaGetDeviceCount(&avail) != cudaSuccess || avail == 0)
+        return fail(CUFHE_ERR_CUDA, "no CUDA device visible");
+    if (g_gpu_num > avail) return fail(CUFHE_ERR_ARG, "gpu num %d > %d visible", g_gpu_num, avail);
+    for (int d = 0; d < g_gpu_num; d++) {
+        if (g_dev[d].ready2) release_device02(d);
+        int rc = init_device02(d, ek);
+        if (rc) {
+            release_device02(d);
+            return rc;
+        }
+    }
+    cudaSetDevice(0);
+    return CUFHE_OK;
+}
+
+int cufhe_cleanup_lvl02(void)
+{
+    for (int d = 0; d < kMaxDev; d++)
+        if (g_dev[d].ready2) release_device02(d);
     cudaSetDevice(0);
     return CUFHE_OK;
 }
@@ -706,6 +861,33 @@ int cufhe_identity_keyswitch(const uint32_t* tlwe1, size_t count, uint32_t* tlwe
     // per input and the identity combination (1, 0, 0)
     plan.uniform_op = kAnd;
     return run_iks(s, 1, plan, nullptr, nullptr, nullptr, tlwe1, tlwe0_out);
+}
+
+int cufhe_blind_rotate_lvl02(const uint32_t* tlwe0, size_t count, uint64_t mu, int steps,
+                             uint64_t* acc_out, uint64_t* tlwe2_out, cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    if (!g_dev[s->device].ready2) return fail(CUFHE_ERR_STATE, "cufhe_initialize_lvl02() not called");
+    if (!tlwe0 || (!acc_out && !tlwe2_out)) return fail(CUFHE_ERR_ARG, "null pointer");
+    if (count == 0) return CUFHE_OK;
+    if (count > (1u << 24)) return fail(CUFHE_ERR_ARG, "too many inputs");
+    CK(cudaSetDevice(s->device));
+    return run_br2(s, tlwe0, (int)count, mu, steps, acc_out, tlwe2_out);
+}
+
+int cufhe_identity_keyswitch_lvl20(const uint64_t* tlwe2, size_t count, uint32_t* tlwe0_out,
+                                   cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    if (!g_dev[s->device].ready2) return fail(CUFHE_ERR_STATE, "cufhe_initialize_lvl02() not called");
+    if (!tlwe2 || !tlwe0_out) return fail(CUFHE_ERR_ARG, "null pointer");
+    if (count == 0) return CUFHE_OK;
+    if (count > (1u << 24)) return fail(CUFHE_ERR_ARG, "too many inputs");
+    CK(cudaSetDevice(s->device));
+    Plan plan = Plan();
+    plan.count = plan.lanes = (int)count;
+    plan.uniform_op = kAnd;  // one lane per input, identity combination
+    return run_iks20(s, plan, tlwe2, tlwe0_out);
 }
 
 int cufhe_profile_enable(int on)

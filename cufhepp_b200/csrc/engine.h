@@ -168,6 +168,7 @@ cudaError_t upload_fft_constants(void);
 // tiles.  A timed-out device wait sets *err (checked at synchronisation).
 struct IksWorkspace {
     size_t cap = 0;  // units
+    int chunks = 0;  // K chunks per unit the tiles were sized for
     uint8_t* atiles = nullptr;
     uint32_t* xb = nullptr;
     int* valid = nullptr;
@@ -179,6 +180,30 @@ cudaError_t launch_iks_tc(int mode, const Plan& plan, const uint32_t* in0, const
                           const uint32_t* in2, const uint32_t* lane_out, const uint8_t* key_tiles,
                           uint32_t* dst, IksWorkspace& w, int* err, cudaStream_t st,
                           int* launches);
+
+// ------------------------------------------------ lvl0 -> lvl2 path ----
+// psi2^s for s in [0, 512], psi2 = e^{i pi / 2048}: the root table of the
+// N = 2048 transforms (other powers by symmetry)
+constexpr int kPsi2Entries = 514;  // 513 used, padded to an even count
+
+// FP64 FFNT blind rotation to lvl2 + SampleExtract of `lanes` lvl0 TLWEs;
+// acc_out: TRLWE<lvl2> [lanes][4096], lane_out: TLWE<lvl2> [lanes][2049]
+// (both optional, uint64 words).  bkf: Fourier BK [step][(e)][8][2][1024].
+cudaError_t launch_br2_fp64(bool kb, const uint32_t* lane_in, int lanes, uint64_t mu,
+                            const double2* bkf, const double2* psi2, int steps, uint64_t* acc_out,
+                            uint64_t* lane_out, cudaStream_t st);
+cudaError_t launch_bk2_to_fft(const uint64_t* bk, int npolys, const double2* psi2, double2* out,
+                              cudaStream_t st);
+cudaError_t upload_fft2_constants(void);
+
+// Tensor-core key switching lvl2 -> lvl0 of gates (lane outputs at lvl2
+// combined per gate: Mux +mu2, NMux negated -mu2) or, with plan.uniform_op a
+// binary gate and no ops, of plain TLWE<lvl2> inputs.
+size_t iks20_tc_key_bytes();
+cudaError_t iks20_tc_key_build(const uint32_t* ksk_dev, uint8_t* key_tiles, cudaStream_t st);
+cudaError_t launch_iks20_tc(const Plan& plan, const uint64_t* lane_out, const uint8_t* key_tiles,
+                            uint32_t* dst, IksWorkspace& w, int* err, cudaStream_t st,
+                            int* launches);
 
 // Read-only view of the engine state that a gate call on stream `st` uses
 // (keys of the stream's device and the CUDA stream).  Returns 0 or a

@@ -25,9 +25,7 @@ namespace cufhe {
 namespace {
 
 constexpr int kT = CUFHE_LVL10_T;
-constexpr int kK = kN * kT * 2;             // 14336
 constexpr int kChunkK = 128;
-constexpr int kChunks = kK / kChunkK;       // 112
 constexpr int kMGates = 128;                // gates per tile (M)
 constexpr int kNCols = 256;                 // 64 outputs x 4 limbs per tile (N)
 constexpr int kOutPerTile = kNCols / 4;     // 64
@@ -40,6 +38,12 @@ constexpr size_t kSmem = 1024 + (size_t)kStages * kStageBytes + 256;
 constexpr uint32_t kIdescIks = idesc_i8(kMGates, kNCols);
 constexpr uint32_t kTmemColsIks = 256;
 
+// K = (i, j, e) of an input with NIN mask coefficients: NIN * 7 * 2
+template <int NIN>
+constexpr int iks_chunks() { return NIN * kT * 2 / kChunkK; }  // 112 (lvl1), 224 (lvl2)
+constexpr int kK = kN * kT * 2;             // 14336
+constexpr int kChunks = iks_chunks<kN>();
+
 __host__ __device__ constexpr uint32_t iks_offset_tc()
 {
     uint32_t off = 0;
@@ -47,16 +51,26 @@ __host__ __device__ constexpr uint32_t iks_offset_tc()
     return off + (1u << (32 - (1 + CUFHE_LVL10_BASEBIT * kT)));
 }
 
+// lvl20: the same decomposition of a Torus64 value (include/keyswitch_gpu.cuh
+// :128-187 at lvl20param)
+__host__ __device__ constexpr uint64_t iks20_offset_tc()
+{
+    uint64_t off = 0;
+    for (int i = 1; i <= (int)CUFHE_LVL20_T; i++) off += 2ull << (64 - i * CUFHE_LVL20_BASEBIT);
+    return off + (1ull << (64 - (1 + CUFHE_LVL20_BASEBIT * CUFHE_LVL20_T)));
+}
+
 // key tiles [nt][kc][32 KB]: row = o_local * 4 + c, K-major, 128B-swizzled
+template <int CH>
 __global__ void k_iks_key(const uint32_t* __restrict__ ksk, uint8_t* __restrict__ out)
 {
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t total = (size_t)kNTiles * kChunks * kBTile / 4;
+    const size_t total = (size_t)kNTiles * CH * kBTile / 4;
     if (q >= total) return;
     const size_t byte = q * 4;
     const int tile = (int)(byte / kBTile);
     const uint32_t w = (uint32_t)(byte % kBTile);
-    const int nt = tile / kChunks, kc = tile % kChunks;
+    const int nt = tile / CH, kc = tile % CH;
     const uint32_t row = (w / 1024) * 8 + (w % 1024) / 128;
     const uint32_t kl = ((((w % 128) / 16) ^ (row & 7)) << 4) + (w % 16);
     const int o = nt * kOutPerTile + (int)(row / 4);
@@ -68,6 +82,15 @@ __global__ void k_iks_key(const uint32_t* __restrict__ ksk, uint8_t* __restrict_
         packed |= (uint32_t)(uint8_t)v << (8 * e);
     }
     reinterpret_cast<uint32_t*>(out)[q] = packed;
+}
+
+// one-hot byte pair of digit code (v = code - 2): v = -1 -> +KSK[.][0],
+// v = +1 -> -KSK[.][0], v = -2 -> +KSK[.][1]
+__device__ __forceinline__ uint32_t onehot_pair(uint32_t code)
+{
+    const uint32_t b0 = code == 1 ? 0x01u : (code == 3 ? 0xFFu : 0u);
+    const uint32_t b1 = code == 0 ? 0x01u : 0u;
+    return b0 | (b1 << 8);
 }
 
 // one-hot digit tiles of unit u (a lane in mode 0, a gate in mode 1):
@@ -126,9 +149,7 @@ __global__ void __launch_bounds__(256) k_iks_prep(int mode, Plan plan, const uin
                 t = x + iks_offset_tc();
             }
             const uint32_t code = ok ? (t >> (30 - 2 * j)) & 3u : 2u;  // v = code - 2
-            const uint32_t b0 = code == 1 ? 0x01u : (code == 3 ? 0xFFu : 0u);
-            const uint32_t b1 = code == 0 ? 0x01u : 0u;
-            wv[e >> 1] |= (b0 | (b1 << 8)) << (16 * (e & 1));
+            wv[e >> 1] |= onehot_pair(code) << (16 * (e & 1));
         }
         const int k0 = 16 * q;
         *reinterpret_cast<uint4*>(tb + (size_t)(k0 / kChunkK) * kATile +
@@ -137,6 +158,62 @@ __global__ void __launch_bounds__(256) k_iks_prep(int mode, Plan plan, const uin
     }
 }
 
+// lvl02 gates: one-hot digit tiles of gate u from its lane outputs at lvl2
+// (uint64 TLWE<lvl2>), combined as binary -> lane0, Mux -> lane0 + lane1 +
+// mu2, NMux -> -(lane0 + lane1) - mu2 (src/cufhe_gates_gpu.cu:826-979);
+// xb[u] = the combined b rounded to Torus32 (include/keyswitch_gpu.cuh:33-50).
+__global__ void __launch_bounds__(256) k_iks20_prep(Plan plan, const uint64_t* __restrict__ lane_out,
+                                                    uint8_t* __restrict__ atiles,
+                                                    uint32_t* __restrict__ xb, int* __restrict__ valid)
+{
+    constexpr int kCh = iks_chunks<CUFHE_LVL2_N>();
+    constexpr int kTl2 = CUFHE_TLWE2_WORDS;
+    const int u = blockIdx.x;
+    const int l0 = plan_lane0(plan, u);
+    const bool ok = l0 >= 0;
+    const int op = plan_op(plan, u);
+    const uint64_t* A = ok ? lane_out + (size_t)l0 * kTl2 : nullptr;
+    const uint64_t* B = (ok && (op == kMux || op == kNMux)) ? A + kTl2 : nullptr;
+    const uint64_t neg = op == kNMux ? ~0ull : 0ull;  // x -> -x when set
+    if (threadIdx.x == 0) {
+        uint32_t b = 0;
+        if (ok) {
+            uint64_t x = A[CUFHE_LVL2_N] + (B ? B[CUFHE_LVL2_N] + CUFHE_MU64 : 0ull);
+            x = (x ^ neg) - neg;
+            b = (uint32_t)((x + (1ull << 31)) >> 32);
+        }
+        xb[u] = b;
+        valid[u] = ok;
+    }
+    const uint32_t row = (uint32_t)(u % kMGates);
+    uint8_t* tb = atiles + (size_t)(u / kMGates) * kCh * kATile;
+    for (int q = threadIdx.x; q < kCh * kChunkK / 16; q += blockDim.x) {
+        uint32_t wv[4] = {0, 0, 0, 0};
+        int ci = -1;
+        uint64_t t = 0;
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int pr = 8 * q + e, i = pr / kT, j = pr % kT;
+            if (i != ci) {
+                ci = i;
+                uint64_t x = 0;
+                if (ok) {
+                    x = A[i] + (B ? B[i] : 0ull);
+                    x = (x ^ neg) - neg;
+                }
+                t = x + iks20_offset_tc();
+            }
+            const uint32_t code = ok ? (uint32_t)(t >> (62 - 2 * j)) & 3u : 2u;
+            wv[e >> 1] |= onehot_pair(code) << (16 * (e & 1));
+        }
+        const int k0 = 16 * q;
+        *reinterpret_cast<uint4*>(tb + (size_t)(k0 / kChunkK) * kATile +
+                                  swz_offset(row, (uint32_t)(k0 % kChunkK))) =
+            make_uint4(wv[0], wv[1], wv[2], wv[3]);
+    }
+}
+
+template <int CH>
 __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__ atiles,
                                                      const uint8_t* __restrict__ btiles,
                                                      const uint32_t* __restrict__ xb,
@@ -153,8 +230,8 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int gt = blockIdx.x / kNTiles, nt = blockIdx.x % kNTiles;
-    const uint8_t* ga = atiles + (size_t)gt * kChunks * kATile;
-    const uint8_t* gb = btiles + (size_t)nt * kChunks * kBTile;
+    const uint8_t* ga = atiles + (size_t)gt * CH * kATile;
+    const uint8_t* gb = btiles + (size_t)nt * CH * kBTile;
     int pend[kStages] = {0, 0, 0, 0};  // thread 0: 1 + parity of an outstanding fill
     int last_commit = -1;
 
@@ -185,7 +262,7 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
             pend[s] = 1 + ((kc / kStages) & 1);
         };
         for (int s = 0; s < kStages; s++) fill(s, s);
-        for (int kc = 0; kc < kChunks; kc++) {
+        for (int kc = 0; kc < CH; kc++) {
             const int s = kc % kStages;
             if (!mbar_wait(&full[s], (kc / kStages) & 1)) {
                 s_fail = 1;
@@ -202,7 +279,7 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
             tc_commit(&empty[s]);
             last_commit = kc;
             // refill the stage of chunk kc-1 with chunk kc+3 once its MMAs are done
-            if (kc >= 1 && kc + kStages - 1 < kChunks) {
+            if (kc >= 1 && kc + kStages - 1 < CH) {
                 const int sp = (kc - 1) % kStages;
                 if (!mbar_wait(&empty[sp], ((kc - 1) / kStages) & 1)) {
                     s_fail = 1;
@@ -211,7 +288,7 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
                 fill(sp, kc + kStages - 1);
             }
         }
-        if (!s_fail && !mbar_wait(&empty[(kChunks - 1) % kStages], ((kChunks - 1) / kStages) & 1))
+        if (!s_fail && !mbar_wait(&empty[(CH - 1) % kStages], ((CH - 1) / kStages) & 1))
             s_fail = 1;
         if (s_fail) {
             atomicOr(err, 1);
@@ -254,25 +331,35 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
 }  // namespace
 
 size_t iks_tc_key_bytes() { return (size_t)kNTiles * kChunks * kBTile; }
+size_t iks20_tc_key_bytes() { return (size_t)kNTiles * iks_chunks<CUFHE_LVL2_N>() * kBTile; }
 
 cudaError_t iks_tc_key_build(const uint32_t* ksk_dev, uint8_t* key_tiles, cudaStream_t st)
 {
     const size_t units = iks_tc_key_bytes() / 4;
-    k_iks_key<<<(unsigned)((units + 255) / 256), 256, 0, st>>>(ksk_dev, key_tiles);
+    k_iks_key<kChunks><<<(unsigned)((units + 255) / 256), 256, 0, st>>>(ksk_dev, key_tiles);
     return cudaGetLastError();
 }
 
-cudaError_t iks_tc_workspace(IksWorkspace& w, int units)
+cudaError_t iks20_tc_key_build(const uint32_t* ksk_dev, uint8_t* key_tiles, cudaStream_t st)
 {
-    if ((size_t)units <= w.cap) return cudaSuccess;
+    const size_t units = iks20_tc_key_bytes() / 4;
+    k_iks_key<iks_chunks<CUFHE_LVL2_N>()><<<(unsigned)((units + 255) / 256), 256, 0, st>>>(
+        ksk_dev, key_tiles);
+    return cudaGetLastError();
+}
+
+static cudaError_t iks_tc_workspace(IksWorkspace& w, int units, int chunks)
+{
+    if ((size_t)units <= w.cap && chunks == w.chunks) return cudaSuccess;
     iks_tc_workspace_free(w);
     const size_t tiles = (size_t)(units + kMGates - 1) / kMGates;
     cudaError_t e;
-    if ((e = cudaMalloc(&w.atiles, tiles * kChunks * kATile)) != cudaSuccess) return e;
-    if ((e = cudaMemset(w.atiles, 0, tiles * kChunks * kATile)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&w.atiles, tiles * chunks * kATile)) != cudaSuccess) return e;
+    if ((e = cudaMemset(w.atiles, 0, tiles * chunks * kATile)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&w.xb, (size_t)units * 4)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&w.valid, (size_t)units * 4)) != cudaSuccess) return e;
     w.cap = (size_t)units;
+    w.chunks = chunks;
     return cudaSuccess;
 }
 
@@ -284,6 +371,21 @@ void iks_tc_workspace_free(IksWorkspace& w)
     w = IksWorkspace();
 }
 
+template <int CH>
+static cudaError_t gemm_attr()
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr[64] = {};
+    if (!attr[dev & 63]) {
+        cudaError_t e = cudaFuncSetAttribute(k_iks_gemm<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kSmem);
+        if (e != cudaSuccess) return e;
+        attr[dev & 63] = true;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t launch_iks_tc(int mode, const Plan& plan, const uint32_t* in0, const uint32_t* in1,
                           const uint32_t* in2, const uint32_t* lane_out, const uint8_t* key_tiles,
                           uint32_t* dst, IksWorkspace& w, int* err, cudaStream_t st,
@@ -292,20 +394,32 @@ cudaError_t launch_iks_tc(int mode, const Plan& plan, const uint32_t* in0, const
     *launches = 0;
     const int units = mode == 0 ? plan.lanes : plan.count;
     if (units <= 0) return cudaSuccess;
-    cudaError_t e = iks_tc_workspace(w, units);
+    cudaError_t e = iks_tc_workspace(w, units, kChunks);
+    if (e == cudaSuccess) e = gemm_attr<kChunks>();
     if (e != cudaSuccess) return e;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr[64] = {};
-    if (!attr[dev & 63]) {
-        e = cudaFuncSetAttribute(k_iks_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
-        if (e != cudaSuccess) return e;
-        attr[dev & 63] = true;
-    }
     k_iks_prep<<<units, 256, 0, st>>>(mode, plan, in0, in1, in2, lane_out, w.atiles, w.xb, w.valid);
     const int gtiles = (units + kMGates - 1) / kMGates;
-    k_iks_gemm<<<gtiles * kNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, w.xb, w.valid, units, dst,
-                                                     err);
+    k_iks_gemm<kChunks><<<gtiles * kNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, w.xb, w.valid,
+                                                              units, dst, err);
+    *launches = 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_iks20_tc(const Plan& plan, const uint64_t* lane_out, const uint8_t* key_tiles,
+                            uint32_t* dst, IksWorkspace& w, int* err, cudaStream_t st,
+                            int* launches)
+{
+    constexpr int kCh = iks_chunks<CUFHE_LVL2_N>();
+    *launches = 0;
+    const int units = plan.count;
+    if (units <= 0) return cudaSuccess;
+    cudaError_t e = iks_tc_workspace(w, units, kCh);
+    if (e == cudaSuccess) e = gemm_attr<kCh>();
+    if (e != cudaSuccess) return e;
+    k_iks20_prep<<<units, 256, 0, st>>>(plan, lane_out, w.atiles, w.xb, w.valid);
+    const int gtiles = (units + kMGates - 1) / kMGates;
+    k_iks_gemm<kCh><<<gtiles * kNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, w.xb, w.valid,
+                                                          units, dst, err);
     *launches = 2;
     return cudaGetLastError();
 }

@@ -58,3 +58,14 @@
 #define CUFHE_KSK10_WORDS                                                  \
     ((uint64_t)CUFHE_LVL1_N * CUFHE_LVL10_T * (1u << (CUFHE_LVL10_BASEBIT - 1u)) * \
      CUFHE_TLWE0_WORDS)
+
+/* lvl0 -> lvl2 path (uint64 words for lvl2 objects) */
+#define CUFHE_TLWE2_WORDS (CUFHE_LVL2_N + 1u)                  /* 2049 */
+#define CUFHE_TRLWE2_WORDS (2u * CUFHE_LVL2_N)                  /* 4096 */
+#define CUFHE_TRGSW2_ROWS (2u * CUFHE_LVL2_L)                   /* 8 */
+#define CUFHE_TRGSW2_WORDS (CUFHE_TRGSW2_ROWS * CUFHE_TRLWE2_WORDS) /* 32768 */
+#define CUFHE_BK2_WORDS ((uint64_t)CUFHE_LVL0_N * CUFHE_TRGSW2_WORDS)
+#define CUFHE_BKKB2_WORDS ((uint64_t)(CUFHE_LVL0_N / 2u) * 3u * CUFHE_TRGSW2_WORDS)
+#define CUFHE_KSK20_WORDS                                                  \
+    ((uint64_t)CUFHE_LVL2_N * CUFHE_LVL20_T * (1u << (CUFHE_LVL20_BASEBIT - 1u)) * \
+     CUFHE_TLWE0_WORDS)

@@ -17,7 +17,7 @@ OK = 0
 ERR = {-1: "CUFHE_ERR_ARG", -2: "CUFHE_ERR_STATE", -3: "CUFHE_ERR_CUDA", -4: "CUFHE_ERR_NOMEM",
        -5: "CUFHE_ERR_UNSUPPORTED"}
 
-LVL0, LVL1 = 0, 1
+LVL0, LVL1, LVL02 = 0, 1, 2
 
 # every symbol include/cufhe_b200.h declares: (argtypes, restype)
 _vp, _sz, _i, _u32, _u64 = C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_uint64
@@ -54,10 +54,14 @@ SIGNATURES = {
     "cufhe_profile_reset": ([], _i),
     "cufhe_profile_read": ([_i, _vp, _vp], _i),
     "cufhe_measure_fp64_peak": ([_vp], _i),
+    "cufhe_initialize_lvl02": ([_vp], _i),
+    "cufhe_cleanup_lvl02": ([], _i),
+    "cufhe_blind_rotate_lvl02": ([_vp, _sz, _u64, _i, _vp, _vp, _vp], _i),
+    "cufhe_identity_keyswitch_lvl20": ([_vp, _sz, _vp, _vp], _i),
 }
 
-K_IKS, K_PREADD, K_BR_FP64, K_BR_INT8, K_FINALIZE = range(5)
-K_NAMES = ["iks", "preadd", "br_fp64", "br_int8", "finalize"]
+K_IKS, K_PREADD, K_BR_FP64, K_BR_INT8, K_FINALIZE, K_BR_FP64_LVL02, K_IKS_LVL20 = range(7)
+K_NAMES = ["iks", "preadd", "br_fp64", "br_int8", "finalize", "br_fp64_lvl02", "iks_lvl20"]
 
 
 class KeyView(C.Structure):
@@ -188,6 +192,21 @@ def cleanup() -> None:
     check(load().cufhe_cleanup(), "cleanup")
 
 
+def initialize_lvl02(ek02, gpus: int | None = None) -> None:
+    """Initialize_lvl02: uploads a client.EvalKey02 (uint64 BK<lvl2>, lvl20 KSK)."""
+    L = load()
+    if gpus is not None:
+        check(L.cufhe_set_gpu_num(gpus), "set_gpu_num")
+    bk = np.ascontiguousarray(ek02.bk, np.uint64)
+    ksk = np.ascontiguousarray(ek02.ksk, np.uint32)
+    kv = KeyView(bk.ctypes.data, bk.size, ksk.ctypes.data, ksk.size, int(ek02.keybundle))
+    check(L.cufhe_initialize_lvl02(C.byref(kv)), "initialize_lvl02")
+
+
+def cleanup_lvl02() -> None:
+    check(load().cufhe_cleanup_lvl02(), "cleanup_lvl02")
+
+
 def synchronize() -> None:
     check(load().cufhe_synchronize(), "synchronize")
 
@@ -225,6 +244,17 @@ def blind_rotate(tlwe0, count: int, mu: int, steps: int, acc_out=None, tlwe_out=
                  stream=None) -> None:
     check(load().cufhe_blind_rotate(dptr(tlwe0), count, mu, steps, dptr(acc_out),
                                     dptr(tlwe_out), stream), "blind_rotate")
+
+
+def blind_rotate_lvl02(tlwe0, count: int, mu: int, steps: int, acc_out=None, tlwe_out=None,
+                       stream=None) -> None:
+    check(load().cufhe_blind_rotate_lvl02(dptr(tlwe0), count, mu, steps, dptr(acc_out),
+                                          dptr(tlwe_out), stream), "blind_rotate_lvl02")
+
+
+def identity_keyswitch_lvl20(tlwe2, count: int, out, stream=None) -> None:
+    check(load().cufhe_identity_keyswitch_lvl20(dptr(tlwe2), count, dptr(out), stream),
+          "identity_keyswitch_lvl20")
 
 
 def identity_keyswitch(tlwe1, count: int, out, stream=None) -> None:

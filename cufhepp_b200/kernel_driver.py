@@ -4,13 +4,17 @@
     python -m cufhepp_b200.kernel_driver br_int8 LANES [REPS] [STEPS]  # INT8 exact rotation
     python -m cufhepp_b200.kernel_driver iks LANES [REPS]       # identity key switching
     python -m cufhepp_b200.kernel_driver gates LANES [REPS]     # full mixed-gate batch (lvl1)
+    python -m cufhepp_b200.kernel_driver br2_fp64 LANES [REPS] [STEPS]  # lvl0 -> lvl2 rotation
+    python -m cufhepp_b200.kernel_driver gates02 LANES [REPS]   # mixed *_lvl02 gate batch
 
 Each stage is launched REPS times on LANES inputs, so a capture can skip the
-first (cold) launch.  Prints one line and exits 0.
+first (cold) launch.  Prints one line (with the wall time of the last REPS-1
+launches) and exits 0.
 """
 from __future__ import annotations
 
 import sys
+import time
 
 import numpy as np
 
@@ -22,11 +26,36 @@ def main(argv: list[str]) -> None:
     lanes = int(argv[1])
     reps = int(argv[2]) if len(argv) > 2 else 2
     sk = client.SecretKey.generate(5)
-    ek = client.EvalKey.generate(sk, keybundle=(stage != "br_int8"))
-    engine.initialize(ek)
+    lvl02 = stage in ("br2_fp64", "gates02")
+    if lvl02:
+        engine.initialize_lvl02(client.EvalKey02.generate(sk, keybundle=True))
+    else:
+        engine.initialize(client.EvalKey.generate(sk, keybundle=(stage != "br_int8")))
     rng = np.random.default_rng(1)
     bits = rng.integers(0, 2, lanes).astype(np.uint8)
-    if stage in ("br_fp64", "br_int8"):
+    t0 = None
+
+    def tick(i):
+        nonlocal t0
+        if i == 0:
+            engine.synchronize()
+            t0 = time.perf_counter()
+
+    if stage == "br2_fp64":
+        steps = int(argv[3]) if len(argv) > 3 else -1
+        d_in = engine.to_device(client.encrypt_bits(sk, bits, 0, seed=3))
+        d_out = engine.DeviceBuffer(lanes * P.TLWE2_WORDS * 8)
+        for i in range(reps):
+            engine.blind_rotate_lvl02(d_in, lanes, P.MU64, steps, tlwe_out=d_out)
+            tick(i)
+    elif stage == "gates02":
+        gates = rng.choice([P.NAND, P.AND, P.OR, P.XOR, P.XNOR, P.MUX], size=lanes).astype(np.int32)
+        cts = [engine.to_device(client.encrypt_bits(sk, bits, 0, seed=3 + i)) for i in range(3)]
+        d_out = engine.DeviceBuffer(lanes * P.TLWE0_WORDS * 4)
+        for i in range(reps):
+            engine.gate_batch(gates, lanes, engine.LVL02, d_out, *cts)
+            tick(i)
+    elif stage in ("br_fp64", "br_int8"):
         engine.set_precision(P.FP64_FFNT if stage == "br_fp64" else P.INT8_EXACT)
         steps = int(argv[3]) if len(argv) > 3 else -1
         x = client.encrypt_bits(sk, bits, 0, seed=3)
@@ -49,8 +78,9 @@ def main(argv: list[str]) -> None:
     else:
         raise SystemExit(f"unknown stage {stage}")
     engine.synchronize()
-    engine.cleanup()
-    print(f"ok {stage} lanes={lanes} reps={reps}")
+    ms = (time.perf_counter() - t0) * 1e3 / (reps - 1) if (t0 is not None and reps > 1) else 0.0
+    engine.cleanup_lvl02() if lvl02 else engine.cleanup()
+    print(f"ok {stage} lanes={lanes} reps={reps} wall_ms_per_rep={ms:.3f}")
 
 
 if __name__ == "__main__":

@@ -59,6 +59,12 @@ extern "C" {
  *             (src/cufhe_gates_gpu.cu:513-824) */
 #define CUFHE_LVL0 0
 #define CUFHE_LVL1 1
+/* CUFHE_LVL02: Ctxt<lvl0param> I/O through lvl02 bootstrapping: blind
+ *              rotation to lvl2 (N = 2048, Torus64), then key switching
+ *              lvl2 -> lvl0 -- the *_lvl02 gates (include/cufhe_gpu.cuh:332-358,
+ *              src/cufhe_gates_gpu.cu:826-979).  Needs cufhe_initialize_lvl02();
+ *              always the FP64 FFNT form. */
+#define CUFHE_LVL02 2
 
 /* ---- external-product precision form -------------------------------- */
 #define CUFHE_FP64_FFNT 0  /* the reference's FP64 negacyclic FFNT */
@@ -77,6 +83,19 @@ typedef struct cufhe_keyview {
     int keybundle;
 } cufhe_keyview;
 
+/* lvl02 evaluation key (stands in for the EvalKey members that
+ * Initialize_lvl02 reads, src/cufhe_gates_gpu.cu:75-90):
+ *   bk : keybundle == 0 -> TRGSW<lvl2>[636]     (20,840,448 uint64 words)
+ *        keybundle == 1 -> TRGSW<lvl2>[318][3]  (31,260,672 uint64 words)
+ *   ksk: TLWE<lvl0>[2048][7][2] (lvl20 key switching, 18,264,064 words) */
+typedef struct cufhe_keyview02 {
+    const uint64_t* bk;
+    size_t bk_words;
+    const uint32_t* ksk;
+    size_t ksk_words;
+    int keybundle;
+} cufhe_keyview02;
+
 typedef struct cufhe_stream_s* cufhe_stream_t; /* NULL = legacy default stream */
 
 /* ---- setup / teardown ----------------------------------------------- */
@@ -91,6 +110,13 @@ int cufhe_initialize(const cufhe_keyview* ek);
 
 /* CleanUp() -- src/cufhe_gates_gpu.cu:63-73 */
 int cufhe_cleanup(void);
+
+/* Initialize_lvl02(const TFHEpp::EvalKey&, const TFHEpp::SecretKey&) --
+ * include/cufhe_gpu.cuh:59, src/cufhe_gates_gpu.cu:75-90: uploads the lvl02
+ * keys to every GPU (independent of cufhe_initialize).  CleanUp_lvl02() --
+ * include/cufhe_gpu.cuh:64. */
+int cufhe_initialize_lvl02(const cufhe_keyview02* ek);
+int cufhe_cleanup_lvl02(void);
 
 /* Synchronize() -- include/cufhe_gpu.cuh:70-76 */
 int cufhe_synchronize(void);
@@ -186,6 +212,18 @@ int cufhe_blind_rotate(const uint32_t* tlwe0, size_t count, uint32_t mu, int ste
 int cufhe_identity_keyswitch(const uint32_t* tlwe1, size_t count, uint32_t* tlwe0_out,
                              cufhe_stream_t st);
 
+/* lvl02 counterparts: blind rotation of count lvl0 TLWEs to lvl2 with test
+ * polynomial mu (Torus64, 2^61 for the gates), first `steps` steps when
+ * steps >= 0; acc_out: TRLWE<lvl2> [count][2][2048], tlwe2_out: TLWE<lvl2>
+ * [count][2049] (uint64 words, device memory, either may be NULL). */
+int cufhe_blind_rotate_lvl02(const uint32_t* tlwe0, size_t count, uint64_t mu, int steps,
+                             uint64_t* acc_out, uint64_t* tlwe2_out, cufhe_stream_t st);
+
+/* Key switching lvl2 -> lvl0 of count TLWE<lvl2> (uint64 [count][2049]) into
+ * TLWE<lvl0> (KeySwitchFromTLWE<lvl20param>, include/keyswitch_gpu.cuh:128-187). */
+int cufhe_identity_keyswitch_lvl20(const uint64_t* tlwe2, size_t count, uint32_t* tlwe0_out,
+                                   cufhe_stream_t st);
+
 /* ---- diagnostics ----------------------------------------------------- */
 /* Per-kernel timing: when enabled, every engine kernel launch is bracketed
  * by CUDA events on its stream; cufhe_profile_read() sums the durations of
@@ -195,7 +233,9 @@ int cufhe_identity_keyswitch(const uint32_t* tlwe1, size_t count, uint32_t* tlwe
 #define CUFHE_K_BR_FP64 2    /* FP64 FFNT blind rotation + SampleExtract */
 #define CUFHE_K_BR_INT8 3    /* INT8 exact blind rotation step kernels */
 #define CUFHE_K_FINALIZE 4   /* lane combination (Mux) and Not/Copy */
-#define CUFHE_K_CLASSES 5
+#define CUFHE_K_BR_FP64_LVL02 5 /* FP64 FFNT blind rotation to lvl2 + SampleExtract */
+#define CUFHE_K_IKS_LVL20 6  /* key switching lvl2 -> lvl0 */
+#define CUFHE_K_CLASSES 7
 int cufhe_profile_enable(int on);
 int cufhe_profile_reset(void);
 int cufhe_profile_read(int kernel_class, double* total_ms, uint64_t* launches);

@@ -66,3 +66,22 @@ def test_gate_before_initialize_is_state_error():
 def test_bad_gate_id_rejected():
     lib = engine.load()
     assert lib.cufhe_gate(99, 1, None, None, None, None, None) == -1
+
+
+def test_lvl02_entry_points_check_state_and_sizes():
+    import numpy as np
+    lib = engine.load()
+    assert lib.cufhe_initialize_lvl02(None) == -1
+    bk = np.zeros(10, np.uint64)
+    ksk = np.zeros(10, np.uint32)
+    kv = engine.KeyView(bk.ctypes.data, bk.size, ksk.ctypes.data, ksk.size, 1)
+    assert lib.cufhe_initialize_lvl02(C.byref(kv)) == -1
+    assert b"lvl02 bootstrapping key" in lib.cufhe_last_error()
+    x = np.zeros(2049, np.uint64)
+    p = x.ctypes.data_as(C.c_void_p)
+    # lvl02 gates and path pieces refuse to run before cufhe_initialize_lvl02
+    assert lib.cufhe_gate(0, 2, p, p, p, None, None) in (-2, -3)
+    assert lib.cufhe_blind_rotate_lvl02(p, 1, 1 << 61, -1, p, None, None) == -2
+    assert b"initialize_lvl02" in lib.cufhe_last_error()
+    assert lib.cufhe_identity_keyswitch_lvl20(p, 1, p, None) == -2
+    assert lib.cufhe_gate(0, 3, p, p, p, None, None) == -1  # no level 3
