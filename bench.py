@@ -42,6 +42,10 @@ A100_PUBLISHED = 1.0 / 0.12e-3   # reference README: 0.12 ms/gate, lvl1 NAND FP6
 # algorithmic work per bootstrap (lvl1): FP64 FFNT flops, INT8 tensor ops
 FLOP_FP64 = {True: 287_744 * 318, False: 189_440 * 636}
 OPS_INT8 = {False: 2 * 636 * 4096 * 8192}
+# lvl2 (N = 2048, 1024-point transforms, 8 digit rows): per KeyBundle step
+# 10 transforms x 5*1024*10 + twist/untwist 10*1024*6 + combine/MAC 8*2*1024*32
+FLOP_FP64_LVL2_KB = (10 * 51_200 + 61_440 + 524_288) * 318
+LVL02_BATCHES = (512, 2048, 8192)
 WORKLOAD = ("lvl1 mixed-gate batch: 4096 independent gates uniform over "
             "NAND/AND/OR/XOR/XNOR/MUX, Ctxt<lvl1> I/O (IKS->BR->SampleExtract), "
             "n0=636 N=1024 l=2 Bgbit=8 IKS basebit=2 t=7, Torus32")
@@ -58,6 +62,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-lvl02", action="store_true",
+                    help="skip the lvl0->lvl2 NAND batches reported under the 'lvl02' key")
     return ap.parse_args()
 
 
@@ -167,6 +173,33 @@ def cpu_gate_rate(seconds, seed, sample_gates=None):
         if el >= seconds:
             break
     return done / el, cores, f"{n}-gate batches of the same mix, repeated for {el:.1f} s"
+
+
+def cpu_gate2_rate(seconds, seed):
+    """Oracle port of the lvl02 CPU gate (FP64 FFNT restatement at N = 2048,
+    KeyBundle), OpenMP over gates on all host cores; bounded sample."""
+    from cufhepp_b200 import client
+    from oracle import oracle as O
+    sk = client.SecretKey.generate(seed)
+    ek = client.EvalKey02.generate(sk, keybundle=True)
+    fft = O.FFT2()
+    bkf = O.bk2_to_fft(fft, ek.bk)
+    cores = os.cpu_count() or 1
+    n = max(8, cores)
+    rng = np.random.default_rng(seed)
+    a, b = (rng.integers(0, 2, n).astype(np.uint8) for _ in range(2))
+    cts = [client.encrypt_bits(sk, x, 0, seed=seed + i) for i, x in enumerate((a, b))]
+    gates = np.zeros(n, np.int32)
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        O.gate2_batch(gates, cts[0], cts[1], None, bkf, ek.ksk, True, O.FP64, fft)
+        done += n
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return {"value": done / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n}-NAND batches repeated for {el:.1f} s"}
 
 
 def run_reference(args):
@@ -347,6 +380,83 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
     return res
 
 
+def run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush):
+    """configs: lvl0 -> lvl2 NAND gate bootstrapping (Ctxt<lvl0> I/O: pre-add,
+    blind rotation to N = 2048, lvl2 -> lvl0 key switching), KeyBundle,
+    batches of 512 / 2048 / 8192 gates; device-resident inputs, CUDA events,
+    L2 flushed between steps."""
+    ek = client.EvalKey02.generate(sk, keybundle=True)
+    engine.initialize_lvl02(ek)
+    rng = np.random.default_rng(args.seed + 7 + rank)
+    out = {}
+    kern_share = None
+    for B in LVL02_BATCHES:
+        a, b = (rng.integers(0, 2, B).astype(np.uint8) for _ in range(2))
+        cts = [client.encrypt_bits(sk, x, 0, seed=args.seed + 500 + i) for i, x in enumerate((a, b))]
+        din = [engine.to_device(x) for x in cts]
+        dout = engine.DeviceBuffer(B * P.TLWE0_WORDS * 4)
+        for _ in range(max(args.warmup, 3)):
+            engine.gate_batch(None, B, engine.LVL02, dout, *din, uniform=P.NAND)
+        torch.cuda.synchronize()
+        res = engine.from_device(dout, (B, P.TLWE0_WORDS))
+        fails = int(np.count_nonzero(client.decrypt_bits(sk, res, 0) != (1 - (a & b))))
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        engine.profile_reset()
+        engine.profile_enable(True)
+        for k in range(args.steps):
+            ev[k][0].record()
+            engine.gate_batch(None, B, engine.LVL02, dout, *din, uniform=P.NAND)
+            ev[k][1].record()
+            flush.zero_()
+        torch.cuda.synchronize()
+        engine.profile_enable(False)
+        kern = {}
+        for cls, name in enumerate(engine.K_NAMES):
+            ms, n = engine.profile_read(cls)
+            if n:
+                kern[name] = ms / args.steps
+        step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+        total = max_over_ranks(torch, sum(step_ms), "cuda")
+        out[str(B)] = {"value": whole_job_rate(B, ws, args.steps, total),
+                       "ms_per_step": total / args.steps, "decrypt_failures": fails,
+                       "kernel_ms_per_step": kern}
+        kern_share = kern
+    # single NAND on an idle GPU
+    lat = []
+    L = engine.load()
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        engine.check(L.cufhe_gate(P.NAND, engine.LVL02, engine.dptr(dout), engine.dptr(din[0]),
+                                  engine.dptr(din[1]), None, None), "gate")
+        e1.record()
+        torch.cuda.synchronize()
+        lat.append(e0.elapsed_time(e1))
+    engine.cleanup_lvl02()
+    big = str(LVL02_BATCHES[-1])
+    br_ms = kern_share.get("br_fp64_lvl02") if kern_share else None
+    rl = None
+    if br_ms:
+        work = FLOP_FP64_LVL2_KB * LVL02_BATCHES[-1]
+        peak = engine_peak_fp64(engine)
+        ach = work / (br_ms * 1e-3) / 1e12
+        rl = {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+              "frac": ach / peak, "traffic": ncu_traffic("br_fp64_lvl02"),
+              "kernel": "k_br2_fp64 (FP64 FFNT blind rotation to lvl2 + SampleExtract)",
+              "work_per_launch": work,
+              "peak_source": "measured FP64 FMA probe on this GPU"}
+    return {"metric": "lvl0->lvl2->lvl0 NAND bootstraps/s", "unit": UNIT,
+            "workload": ("NAND gates, Ctxt<lvl0> I/O, lvl2 N=2048 l=4 Bgbit=10 Torus64, "
+                         "KeyBundle, lvl20 key switch basebit=2 t=7"),
+            "batches": out, "value": out[big]["value"],
+            "single_gate_latency_ms": statistics.median(lat), "roofline": rl,
+            "dtype": "f64"}
+
+
 _PEAK = {}
 
 
@@ -395,10 +505,15 @@ def run_ours(args):
         ek = client.EvalKey.generate(sk, keybundle=(p == "fp64"))
         results[p] = run_path(args, p, torch, engine, client, P, sk, ek, workload, rank, ws, flush)
     primary = results[paths[0]]
+    lvl02 = None
+    if not args.no_lvl02:
+        lvl02 = run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, cores, sample = cpu_gate_rate(args.cpu_seconds, args.seed)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        if lvl02 is not None:
+            lvl02["cpu_baseline"] = cpu_gate2_rate(min(args.cpu_seconds, 8.0), args.seed)
     if rank == 0:
         line = {
             "metric": METRIC, "value": primary["value"], "unit": UNIT, "n_gpus": ws,
@@ -421,6 +536,8 @@ def run_ours(args):
             "kernel_ms_per_step": primary["kernel_ms_per_step"],
             "vs_reference_a100_published": primary["value"] / A100_PUBLISHED,
         }
+        if lvl02 is not None:
+            line["lvl02"] = lvl02
         if len(paths) > 1:
             line["paths"] = {p: {k: results[p][k] for k in
                                  ("value", "ms_per_step", "p50_gate_latency_ms",

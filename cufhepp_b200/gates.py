@@ -2,7 +2,9 @@
 over the engine's C-ABI: SetGPUNum, Initialize, CleanUp, Synchronize,
 Stream, StreamQuery, Ctxt, and the 14 gates in copying (Nand, ...) and
 device-resident (gNand, ...) forms.  Ctxt level 1 is Ctxt<lvl1param>
-(key switching, then blind rotation), level 0 is Ctxt<lvl0param>.
+(key switching, then blind rotation), level 0 is Ctxt<lvl0param>.  The lvl02
+path: Initialize_lvl02 / CleanUp_lvl02 and Nand_lvl02 ... NMux_lvl02 on level-0
+Ctxts (include/cufhe_gpu.cuh:59-64, :332-358).
 """
 from __future__ import annotations
 
@@ -21,6 +23,15 @@ def Initialize(ek) -> None:
 
 def CleanUp() -> None:
     engine.cleanup()
+
+
+def Initialize_lvl02(ek02, sk=None) -> None:
+    """Initialize_lvl02(ek, sk): the secret key is unused, as in the reference."""
+    engine.initialize_lvl02(ek02)
+
+
+def CleanUp_lvl02() -> None:
+    engine.cleanup_lvl02()
 
 
 def Synchronize() -> None:
@@ -70,11 +81,12 @@ class Ctxt:
         self.tlwedevices = [engine.DeviceBuffer(words * 4, d) for d in range(n)]
 
 
-def _copy(gate, out, a, b=None, c=None, st: Stream | None = None):
+def _copy(gate, out, a, b=None, c=None, st: Stream | None = None, level: int | None = None):
     d = st.device_id() if st else 0
     h = lambda x: None if x is None else engine._p(x.tlwehost)  # noqa: E731
     v = lambda x: None if x is None else engine.dptr(x.tlwedevices[d])  # noqa: E731
-    engine.check(engine.load().cufhe_gate_copy(gate, out.level, h(out), v(out), h(a), v(a), h(b),
+    lv = out.level if level is None else level
+    engine.check(engine.load().cufhe_gate_copy(gate, lv, h(out), v(out), h(a), v(a), h(b),
                                                v(b), h(c), v(c), st.st() if st else None),
                  P.GATE_NAMES[gate])
 
@@ -105,6 +117,33 @@ AndNY, gAndNY = _binary(P.ANDNY)
 Nor, gNor = _binary(P.NOR)
 Xor, gXor = _binary(P.XOR)
 Xnor, gXnor = _binary(P.XNOR)
+
+
+def _binary02(gid):
+    def f(out, in0, in1, st=None):
+        assert out.level == 0, "the lvl02 gates take Ctxt<lvl0param>"
+        _copy(gid, out, in0, in1, None, st, level=engine.LVL02)
+    return f
+
+
+Nand_lvl02 = _binary02(P.NAND)
+Or_lvl02 = _binary02(P.OR)
+OrYN_lvl02 = _binary02(P.ORYN)
+OrNY_lvl02 = _binary02(P.ORNY)
+And_lvl02 = _binary02(P.AND)
+AndYN_lvl02 = _binary02(P.ANDYN)
+AndNY_lvl02 = _binary02(P.ANDNY)
+Nor_lvl02 = _binary02(P.NOR)
+Xor_lvl02 = _binary02(P.XOR)
+Xnor_lvl02 = _binary02(P.XNOR)
+
+
+def Mux_lvl02(out, inc, in1, in0, st=None):
+    _copy(P.MUX, out, inc, in1, in0, st, level=engine.LVL02)
+
+
+def NMux_lvl02(out, inc, in1, in0, st=None):
+    _copy(P.NMUX, out, inc, in1, in0, st, level=engine.LVL02)
 
 
 def Mux(out, inc, in1, in0, st=None):

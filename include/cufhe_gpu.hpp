@@ -6,7 +6,9 @@
 // Create/Destroy), StreamQuery, Ctxt<P> (pinned host TLWE + one device
 // buffer per GPU, non-copyable), the 14 gates in copying (Nand, ...) and
 // device-resident (gNand, ...) forms, for P = lvl0param (blind rotation then
-// key switching) and P = lvl1param (key switching then blind rotation).
+// key switching) and P = lvl1param (key switching then blind rotation), and
+// the lvl02 path: Initialize_lvl02 / CleanUp_lvl02 and Nand_lvl02 ...
+// NMux_lvl02 on Ctxt<lvl0param> (include/cufhe_gpu.cuh:59-64, :332-358).
 // Differences: TFHEpp types are replaced by the plain-array EvalKey below,
 // and errors throw cufhe::Error instead of printing and exiting.
 #pragma once
@@ -58,6 +60,14 @@ struct EvalKey {
     bool keybundle = true;
 };
 
+// The EvalKey members Initialize_lvl02 reads (getbk<lvl02param>,
+// getiksk<lvl20param>): BK<lvl2> in uint64 words, lvl2->lvl0 KSK
+struct EvalKey02 {
+    std::vector<uint64_t> bk;
+    std::vector<uint32_t> ksk;
+    bool keybundle = true;
+};
+
 inline void SetGPUNum(int n) { check(cufhe_set_gpu_num(n), "SetGPUNum"); }
 
 inline void Initialize(const EvalKey& ek)
@@ -68,6 +78,21 @@ inline void Initialize(const EvalKey& ek)
 }
 
 inline void CleanUp() { check(cufhe_cleanup(), "CleanUp"); }
+
+// Initialize_lvl02(ek, sk) -- src/cufhe_gates_gpu.cu:75-90 (the secret key
+// argument is unused there too)
+inline void Initialize_lvl02(const EvalKey02& ek)
+{
+    cufhe_keyview02 kv{ek.bk.data(), ek.bk.size(), ek.ksk.data(), ek.ksk.size(),
+                       ek.keybundle ? 1 : 0};
+    check(cufhe_initialize_lvl02(&kv), "Initialize_lvl02");
+}
+template <class SecretKey>
+inline void Initialize_lvl02(const EvalKey02& ek, const SecretKey&)
+{
+    Initialize_lvl02(ek);
+}
+inline void CleanUp_lvl02() { check(cufhe_cleanup_lvl02(), "CleanUp_lvl02"); }
 inline void Synchronize() { check(cufhe_synchronize(), "Synchronize"); }
 
 namespace detail {
@@ -147,6 +172,16 @@ inline void gate_copy(int g, const char* name, Ctxt<P>& out, Ctxt<P>& a, Ctxt<P>
                           c ? c->tlwedevices[d] : nullptr, st.st()),
           name);
 }
+inline void gate_copy02(int g, const char* name, Ctxt<lvl0param>& out, Ctxt<lvl0param>& a,
+                        Ctxt<lvl0param>* b, Ctxt<lvl0param>* c, Stream st)
+{
+    const int d = st.device_id();
+    check(cufhe_gate_copy(g, CUFHE_LVL02, out.tlwehost.data(), out.tlwedevices[d],
+                          a.tlwehost.data(), a.tlwedevices[d], b ? b->tlwehost.data() : nullptr,
+                          b ? b->tlwedevices[d] : nullptr, c ? c->tlwehost.data() : nullptr,
+                          c ? c->tlwedevices[d] : nullptr, st.st()),
+          name);
+}
 template <class P>
 inline void gate_dev(int g, const char* name, Ctxt<P>& out, Ctxt<P>& a, Ctxt<P>* b, Ctxt<P>* c,
                      Stream st)
@@ -168,6 +203,11 @@ inline void gate_dev(int g, const char* name, Ctxt<P>& out, Ctxt<P>& a, Ctxt<P>*
     inline void g##Name(Ctxt<P>& out, Ctxt<P>& in0, Ctxt<P>& in1, Stream st)           \
     {                                                                                  \
         detail::gate_dev<P>(ID, "g" #Name, out, in0, &in1, nullptr, st);               \
+    }                                                                                  \
+    inline void Name##_lvl02(Ctxt<lvl0param>& out, Ctxt<lvl0param>& in0,               \
+                             Ctxt<lvl0param>& in1, Stream st)                          \
+    {                                                                                  \
+        detail::gate_copy02(ID, #Name "_lvl02", out, in0, &in1, nullptr, st);          \
     }
 
 CUFHE_BINARY_GATE(Nand, CUFHE_NAND)
@@ -202,6 +242,16 @@ template <class P>
 inline void gNMux(Ctxt<P>& out, Ctxt<P>& inc, Ctxt<P>& in1, Ctxt<P>& in0, Stream st)
 {
     detail::gate_dev<P>(CUFHE_NMUX, "gNMux", out, inc, &in1, &in0, st);
+}
+inline void Mux_lvl02(Ctxt<lvl0param>& out, Ctxt<lvl0param>& inc, Ctxt<lvl0param>& in1,
+                      Ctxt<lvl0param>& in0, Stream st)
+{
+    detail::gate_copy02(CUFHE_MUX, "Mux_lvl02", out, inc, &in1, &in0, st);
+}
+inline void NMux_lvl02(Ctxt<lvl0param>& out, Ctxt<lvl0param>& inc, Ctxt<lvl0param>& in1,
+                       Ctxt<lvl0param>& in0, Stream st)
+{
+    detail::gate_copy02(CUFHE_NMUX, "NMux_lvl02", out, inc, &in1, &in0, st);
 }
 template <class P>
 inline void Not(Ctxt<P>& out, Ctxt<P>& in, Stream st)

@@ -37,6 +37,13 @@ void tfhe_bk32_gen(uint64_t seed, const int32_t* key0, uint32_t n0, const int32_
 /* key-switching key TLWE<lvl0>[n_src][t][2^(basebit-1)] */
 void tfhe_ksk32_gen(uint64_t seed, const int32_t* key_src, uint32_t n_src, const int32_t* key0,
                     uint32_t n0, uint32_t basebit, uint32_t t, double alpha, uint32_t* out);
+/* lvl0 -> lvl2 bootstrapping key (Torus64 TRGSW<lvl2>, N = 2048, l = 4,
+ * Bgbit = 10): kb = 0 -> TRGSW[n0], kb = 1 -> TRGSW[n0/2][3]; the lvl2 -> lvl0
+ * key-switching key is tfhe_ksk32_gen with the lvl2 key as key_src. */
+void tfhe_bk64_gen(uint64_t seed, const int32_t* key0, uint32_t n0, const int32_t* key2,
+                   uint32_t N, uint32_t l, uint32_t bgbit, double alpha, int kb, uint64_t* out);
+void tfhe_trlwe64_phase(const int32_t* key, uint32_t N, const uint64_t* c, uint64_t* phase);
+uint64_t tfhe_tlwe64_phase(const int32_t* key, uint32_t n, const uint64_t* c);
 
 #ifdef __cplusplus
 }

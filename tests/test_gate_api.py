@@ -69,3 +69,39 @@ def test_python_mirror_of_the_gate_api(keys):
             s.Destroy()
     finally:
         G.CleanUp()
+
+
+@pytest.mark.gpu
+def test_python_mirror_lvl02_gates():
+    """Nand_lvl02 ... NMux_lvl02 on Ctxt<lvl0param> (test/test_gate_gpu_lvl02.cc)."""
+    sk = client.SecretKey.generate(0xA11)
+    G.Initialize_lvl02(client.EvalKey02.generate(sk, keybundle=True), sk)
+    try:
+        rng = np.random.default_rng(78)
+        st = [G.Stream() for _ in range(3)]
+        for s in st:
+            s.Create()
+        n = 12
+        pt = rng.integers(0, 2, 4 * n).astype(np.uint8)
+        ct = [G.Ctxt(0) for _ in range(4 * n)]
+        enc = client.encrypt_bits(sk, pt, 0, seed=15)
+        for i in range(4 * n):
+            ct[i].tlwehost[:] = enc[i]
+        ops = [(G.Nand_lvl02, lambda a, b, c: 1 - (a & b)), (G.Or_lvl02, lambda a, b, c: a | b),
+               (G.AndYN_lvl02, lambda a, b, c: a & (1 - b)), (G.Xnor_lvl02, lambda a, b, c: 1 - (a ^ b)),
+               (G.Mux_lvl02, lambda a, b, c: b if a else c), (G.NMux_lvl02, lambda a, b, c: 1 - (b if a else c))]
+        for i in range(n):
+            f = ops[i % len(ops)][0]
+            if f in (G.Mux_lvl02, G.NMux_lvl02):
+                f(ct[i], ct[i + n], ct[i + 2 * n], ct[i + 3 * n], st[i % 3])
+            else:
+                f(ct[i], ct[i + n], ct[i + 2 * n], st[i % 3])
+        G.Synchronize()
+        for i in range(n):
+            a, b, c = int(pt[i + n]), int(pt[i + 2 * n]), int(pt[i + 3 * n])
+            want = ops[i % len(ops)][1](a, b, c)
+            assert client.decrypt_bits(sk, ct[i].tlwehost, 0)[0] == want, i
+        for s in st:
+            s.Destroy()
+    finally:
+        G.CleanUp_lvl02()
