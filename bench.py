@@ -64,6 +64,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-lvl02", action="store_true",
                     help="skip the lvl0->lvl2 NAND batches reported under the 'lvl02' key")
+    ap.add_argument("--no-uneven", action="store_true",
+                    help="skip the uneven-circuit workload reported under the 'uneven' key")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the built-in lanes-per-CTA rule instead of the autotuner's table")
     return ap.parse_args()
 
 
@@ -457,6 +461,63 @@ def run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush):
             "dtype": "f64"}
 
 
+def run_uneven(args, torch, engine, client, P, sk, ek, rank, ws, flush, ref_rate):
+    """Uneven circuits: 256 seeded levelised random DAGs of 50-2000 gates
+    (fan-in 2, gate types uniform over the ten binary gates, level widths
+    log-uniform 1-64) plus 64 ripple-carry adders of width 8-64 on random
+    operands, merged into one wire table of Ctxt<lvl1>; the engine levelises
+    it into waves (cufhe_circuit_create) and runs the waves as one CUDA graph.
+    Timed with CUDA events per full run, L2 flushed between runs."""
+    from cufhepp_b200 import circuits as CI
+    net = CI.uneven_workload(args.seed + 31 * rank)
+    engine.initialize(ek)
+    engine.set_precision(P.FP64_FFNT)
+    rng = np.random.default_rng(args.seed + 3 + rank)
+    bits = rng.integers(0, 2, net.inputs.size).astype(np.uint8)
+    host = np.zeros((net.num_wires, P.TLWE1_WORDS), np.uint32)
+    host[net.inputs] = client.encrypt_bits(sk, bits, 1, seed=args.seed + 900 + rank)
+    wires = torch.from_numpy(host.view(np.int32)).cuda()
+    c = engine.Circuit(1, net.num_wires, net.ops, net.in0, net.in1, net.in2, net.out)
+    waves, max_gates, max_lanes = c.info()
+    wg, wl = c.wave_sizes()
+    res = {}
+    for mode in ("graph", "direct"):
+        for _ in range(max(args.warmup, 3) if mode == "graph" else 1):
+            c.run(wires.data_ptr(), graph=(mode == "graph"))
+        torch.cuda.synchronize()
+        n = max(2, min(args.steps, 3))
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(n)]
+        if ws > 1:
+            torch.distributed.barrier()
+        l0 = engine.kernel_launches()
+        for k in range(n):
+            ev[k][0].record()
+            c.run(wires.data_ptr(), graph=(mode == "graph"))
+            ev[k][1].record()
+            flush.zero_()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(torch, sum(e0.elapsed_time(e1) for e0, e1 in ev), "cuda") / n
+        res[mode] = {"ms_per_run": ms, "value": net.bootstraps() * ws / (ms * 1e-3),
+                     "gates_per_s": net.gates * ws / (ms * 1e-3),
+                     "gpu_launches_per_run": (engine.kernel_launches() - l0) / n}
+    out = wires.cpu().numpy().view(np.uint32)
+    plain = CI.evaluate(net, bits)
+    fails = int(np.count_nonzero(client.decrypt_bits(sk, out[net.out], 1) != plain[net.out]))
+    c.destroy()
+    engine.cleanup()
+    return {"metric": "uneven-circuit bootstraps/s (whole workload per run)", "unit": UNIT,
+            "workload": ("256 levelised random DAGs (50-2000 gates, fan-in 2, widths log-uniform "
+                         "1-64) + 64 ripple-carry adders (width 8-64, carry by Mux), Ctxt<lvl1>"),
+            "gates": net.gates, "bootstraps": net.bootstraps(), "waves": waves,
+            "max_wave_gates": max_gates, "max_wave_lanes": max_lanes,
+            "median_wave_lanes": float(np.median(wl)),
+            "value": res["graph"]["value"], "graph": res["graph"], "direct": res["direct"],
+            "decrypt_failures": fails, "gates_checked": net.gates,
+            "vs_full_batch_rate": res["graph"]["value"] / ref_rate if ref_rate else None,
+            "dtype": "f64"}
+
+
 _PEAK = {}
 
 
@@ -500,11 +561,22 @@ def run_ours(args):
     workload = make_workload(rng, args.batch)
     sk = client.SecretKey.generate(args.seed)
     paths = ["fp64", "int8"] if args.path == "both" else [args.path]
+    tuned = None
+    if not args.no_autotune:
+        ek_t = client.EvalKey.generate(sk, keybundle=True)
+        engine.initialize(ek_t)
+        tuned = engine.autotune()
+        engine.cleanup()
     results = {}
     for p in paths:
         ek = client.EvalKey.generate(sk, keybundle=(p == "fp64"))
         results[p] = run_path(args, p, torch, engine, client, P, sk, ek, workload, rank, ws, flush)
     primary = results[paths[0]]
+    uneven = None
+    if not args.no_uneven:
+        ek_u = client.EvalKey.generate(sk, keybundle=True)
+        uneven = run_uneven(args, torch, engine, client, P, sk, ek_u, rank, ws, flush,
+                            results["fp64"]["value"] if "fp64" in results else None)
     lvl02 = None
     if not args.no_lvl02:
         lvl02 = run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush)
@@ -538,6 +610,11 @@ def run_ours(args):
         }
         if lvl02 is not None:
             line["lvl02"] = lvl02
+        if uneven is not None:
+            line["uneven"] = uneven
+        line["config"]["br_lanes_per_cta"] = (
+            {"source": "autotuner (cufhe_autotune)", "table": tuned} if tuned
+            else {"source": "built-in rule"})
         if len(paths) > 1:
             line["paths"] = {p: {k: results[p][k] for k in
                                  ("value", "ms_per_step", "p50_gate_latency_ms",

@@ -304,18 +304,64 @@ static int br_lanes_per_cta()
     return g;
 }
 
+namespace {
+struct BrTuning {
+    int n = 0;
+    int bound[32];
+    int g[32];
+};
+BrTuning g_br_tuning[64];
+}  // namespace
+
+void br_fp64_set_tuning(int dev, int n, const int* bound, const int* g)
+{
+    BrTuning& t = g_br_tuning[dev & 63];
+    t.n = n < 0 ? 0 : (n > 32 ? 32 : n);
+    for (int i = 0; i < t.n; i++) {
+        t.bound[i] = bound[i];
+        t.g[i] = g[i];
+    }
+}
+
+int br_fp64_get_tuning(int dev, int* bound, int* g, int cap)
+{
+    const BrTuning& t = g_br_tuning[dev & 63];
+    for (int i = 0; i < t.n && i < cap; i++) {
+        bound[i] = t.bound[i];
+        g[i] = t.g[i];
+    }
+    return t.n;
+}
+
 cudaError_t launch_br_fp64(bool kb, const uint32_t* lane_in, int lanes, uint32_t mu,
                            const double2* bkf, const Fp64Tables& t, int steps, uint32_t* acc_out,
                            uint32_t* lane_out, cudaStream_t st)
 {
     if (lanes <= 0) return cudaSuccess;
-    // small batches: one lane per CTA (3 CTAs per SM) while they fit one wave,
-    // which minimises latency; larger ones: two lanes per CTA for throughput
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int g = getenv("CUFHE_BR_LANES_PER_CTA") ? br_lanes_per_cta()
-                                                   : (lanes <= 3 * sms ? 1 : kDefaultBrGates);
+    int g;
+    const BrTuning& tun = g_br_tuning[dev & 63];
+    if (getenv("CUFHE_BR_LANES_PER_CTA")) {
+        g = br_lanes_per_cta();
+    } else if (tun.n > 0) {
+        int i = 0;
+        while (i + 1 < tun.n && lanes > tun.bound[i]) i++;
+        g = tun.g[i];
+    } else {
+        // untuned: one lane per CTA (3 CTAs per SM) while the batch fits one
+        // wave, which minimises latency; larger ones: two lanes per CTA
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g = lanes <= 3 * sms ? 1 : kDefaultBrGates;
+    }
+    return launch_br_fp64_g(g, kb, lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st);
+}
+
+cudaError_t launch_br_fp64_g(int g, bool kb, const uint32_t* lane_in, int lanes, uint32_t mu,
+                             const double2* bkf, const Fp64Tables& t, int steps,
+                             uint32_t* acc_out, uint32_t* lane_out, cudaStream_t st)
+{
+    if (lanes <= 0) return cudaSuccess;
     if (g == 1)
         return kb ? launch_g<true, 1>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st)
                   : launch_g<false, 1>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st);

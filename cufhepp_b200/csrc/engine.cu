@@ -70,6 +70,27 @@ struct cufhe_stream_s {
     cufhe::Workspace ws;
 };
 
+// A levelised gate circuit (cufhe_circuit_create): one Plan per wave of
+// independent gates, all plan and index arrays in one device buffer, and a
+// private workspace sized for the widest wave, so that running the circuit
+// allocates nothing and can be captured into a CUDA graph.
+struct cufhe_circuit_s {
+    int device = 0;
+    int level = 0;
+    size_t wires = 0, gates = 0;
+    int max_lanes = 0, max_gates = 0;
+    std::vector<cufhe::Plan> waves;
+    std::vector<char> wave_nc;  // wave holds Not/Copy gates
+    void* dbuf = nullptr;
+    cufhe_stream_s exec;        // workspace of the circuit; exec.st = the stream of a run
+    cudaStream_t cap = nullptr; // private stream the graph is captured on
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    uint32_t* graph_wires = nullptr;
+    int graph_precision = -1;
+    uint64_t graph_launches = 0;
+};
+
 namespace cufhe {
 namespace {
 
@@ -487,9 +508,6 @@ int run_batch(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count
 {
     if (level != CUFHE_LVL0 && level != CUFHE_LVL1 && level != CUFHE_LVL02)
         return fail(CUFHE_ERR_ARG, "bad level %d", level);
-    if (level == CUFHE_LVL02 ? !g_dev[s->device].ready2 : !g_dev[s->device].ready)
-        return fail(CUFHE_ERR_STATE, level == CUFHE_LVL02 ? "cufhe_initialize_lvl02() not called"
-                                                         : "cufhe_initialize() not called");
     if (count == 0) return CUFHE_OK;
     if (count > (1u << 24)) return fail(CUFHE_ERR_ARG, "batch of %zu gates too large", count);
     if (!out || !in0) return fail(CUFHE_ERR_ARG, "null ciphertext pointer");
@@ -504,6 +522,11 @@ int run_batch(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count
         need2 = uniform == kMux || uniform == kNMux;
     }
     if ((need1 && !in1) || (need2 && !in2)) return fail(CUFHE_ERR_ARG, "missing input operand");
+    // keys are needed by gates that bootstrap; Not/Copy alone run without them
+    // (the reference's lvl02 test runs Not/Copy<lvl0param> after Initialize_lvl02 only)
+    if (need1 && (level == CUFHE_LVL02 ? !g_dev[s->device].ready2 : !g_dev[s->device].ready))
+        return fail(CUFHE_ERR_STATE, level == CUFHE_LVL02 ? "cufhe_initialize_lvl02() not called"
+                                                         : "cufhe_initialize() not called");
     CK(cudaSetDevice(s->device));
     Plan plan;
     int rc = build_plan(s, gates, uniform, count, plan);
@@ -545,6 +568,148 @@ int run_batch(cufhe_stream_s* s, const int32_t* gates, int uniform, size_t count
     // (lvl02 gates keep Ctxt<lvl0> I/O, so Not/Copy work on TLWE<lvl0> there too)
     }
     return CUFHE_OK;
+}
+
+// ------------------------------------------------------------ circuits ----
+// Runs wave w of circuit c on the wire table `wires` on stream c->exec.st.
+int run_wave(cufhe_circuit_s* c, size_t w, uint32_t* wires)
+{
+    const Plan& plan = c->waves[w];
+    cufhe_stream_s* s = &c->exec;
+    Workspace& ws = s->ws;
+    int rc = CUFHE_OK;
+    if (plan.lanes) {
+        if (c->level == CUFHE_LVL1) {
+            if ((rc = run_iks(s, 0, plan, wires, wires, wires, nullptr, ws.lane_in))) return rc;
+            if ((rc = run_br(s, ws.lane_in, plan.lanes, kMu, -1, nullptr, ws.lane_out))) return rc;
+            LAUNCH(CUFHE_K_FINALIZE, s->st, launch_finalize_lvl1(plan, ws.lane_out, wires, s->st));
+        } else if (c->level == CUFHE_LVL0) {
+            LAUNCH(CUFHE_K_PREADD, s->st,
+                   launch_preadd_lvl0(plan, wires, wires, wires, ws.lane_in, s->st));
+            if ((rc = run_br(s, ws.lane_in, plan.lanes, kMu, -1, nullptr, ws.lane_out))) return rc;
+            if ((rc = run_iks(s, 1, plan, nullptr, nullptr, nullptr, ws.lane_out, wires))) return rc;
+        } else {
+            LAUNCH(CUFHE_K_PREADD, s->st,
+                   launch_preadd_lvl0(plan, wires, wires, wires, ws.lane_in, s->st));
+            if ((rc = run_br2(s, ws.lane_in, plan.lanes, CUFHE_MU64, -1, nullptr, ws.lane_out2)))
+                return rc;
+            if ((rc = run_iks20(s, plan, ws.lane_out2, wires))) return rc;
+        }
+    }
+    if (c->wave_nc[w])
+        LAUNCH(CUFHE_K_FINALIZE, s->st,
+               launch_not_copy(plan, c->level == CUFHE_LVL1 ? kTlwe1 : kTlwe0, wires, wires, s->st));
+    return CUFHE_OK;
+}
+
+void circuit_drop_graph(cufhe_circuit_s* c)
+{
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->gexec = nullptr;
+    c->graph = nullptr;
+    c->graph_wires = nullptr;
+}
+
+// Captures every wave into a CUDA graph (on the circuit's private stream)
+int circuit_capture(cufhe_circuit_s* c, uint32_t* wires)
+{
+    circuit_drop_graph(c);
+    const bool prof = g_prof;
+    g_prof = false;  // per-kernel event timing is not recorded inside graphs
+    const uint64_t l0 = g_launches.load();
+    CK(cudaStreamBeginCapture(c->cap, cudaStreamCaptureModeRelaxed));
+    c->exec.st = c->cap;
+    int rc = CUFHE_OK;
+    for (size_t w = 0; w < c->waves.size() && !rc; w++) rc = run_wave(c, w, wires);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->cap, &g);
+    g_prof = prof;
+    c->graph_launches = g_launches.load() - l0;
+    g_launches.fetch_sub(c->graph_launches);  // counted when the graph runs
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(CUFHE_ERR_CUDA, "circuit capture: %s", cudaGetErrorString(e));
+    c->graph = g;
+    CK(cudaGraphInstantiate(&c->gexec, g, 0));
+    c->graph_wires = wires;
+    c->graph_precision = g_precision;
+    return CUFHE_OK;
+}
+
+void circuit_free(cufhe_circuit_s* c)
+{
+    cudaSetDevice(c->device);
+    circuit_drop_graph(c);
+    cudaFree(c->dbuf);
+    free_ws(c->exec.ws);
+    if (c->cap) cudaStreamDestroy(c->cap);
+    delete c;
+}
+
+// lanes per CTA of the FP64 blind rotation measured on the current device for a
+// ladder of batch sizes (the autotuner behind cufhe_autotune)
+int autotune_br(int d)
+{
+    DeviceState& D = g_dev[d];
+    if (!D.ready) return fail(CUFHE_ERR_STATE, "cufhe_initialize() not called");
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d));
+    const int ladder[] = {1, sms / 2, sms, 2 * sms, 3 * sms, 4 * sms, 6 * sms, 8 * sms,
+                          12 * sms, 16 * sms, 24 * sms, 32 * sms};
+    const int n = (int)(sizeof(ladder) / sizeof(ladder[0]));
+    const int maxl = ladder[n - 1];
+    uint32_t *lin = nullptr, *lout = nullptr;
+    CK(cudaMalloc(&lin, (size_t)maxl * kTlwe0 * 4));
+    if (cudaMalloc(&lout, (size_t)maxl * kTlwe1 * 4) != cudaSuccess) {
+        cudaFree(lin);
+        return fail(CUFHE_ERR_NOMEM, "autotune buffers");
+    }
+    cudaMemset(lin, 0, (size_t)maxl * kTlwe0 * 4);  // valid (noiseless zero) inputs
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const Fp64Tables t = {D.psi, D.tw512};
+    int bound[32], best[32];
+    int rc = CUFHE_OK;
+    for (int i = 0; i < n && !rc; i++) {
+        const int L = ladder[i];
+        float best_ms = 1e30f;
+        best[i] = 1;
+        bound[i] = L;
+        const int cands[] = {1, 2, 4};
+        for (int g : cands) {
+            float ms_min = 1e30f;
+            for (int rep = 0; rep < 3; rep++) {
+                cudaEventRecord(e0, 0);
+                cudaError_t e = launch_br_fp64_g(g, D.kb != 0, lin, L, kMu, D.bkf, t, -1, nullptr,
+                                                 lout, 0);
+                cudaEventRecord(e1, 0);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                if (e != cudaSuccess) {
+                    rc = fail(CUFHE_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+                    break;
+                }
+                g_launches.fetch_add(1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0 && ms < ms_min) ms_min = ms;  // first run warms up
+            }
+            if (rc) break;
+            if (ms_min < best_ms * 0.98f) {  // prefer fewer lanes per CTA on a tie
+                best_ms = ms_min;
+                best[i] = g;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(lin);
+    cudaFree(lout);
+    if (!rc) br_fp64_set_tuning(d, n, bound, best);
+    return rc;
 }
 
 }  // namespace
@@ -888,6 +1053,264 @@ int cufhe_identity_keyswitch_lvl20(const uint64_t* tlwe2, size_t count, uint32_t
     plan.count = plan.lanes = (int)count;
     plan.uniform_op = kAnd;  // one lane per input, identity combination
     return run_iks20(s, plan, tlwe2, tlwe0_out);
+}
+
+int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, size_t num_gates,
+                         const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
+                         const int32_t* in2, const int32_t* out, int device)
+{
+    if (!out_c) return fail(CUFHE_ERR_ARG, "null circuit handle");
+    *out_c = nullptr;
+    if (level != CUFHE_LVL0 && level != CUFHE_LVL1 && level != CUFHE_LVL02)
+        return fail(CUFHE_ERR_ARG, "bad level %d", level);
+    if (device < 0) device = 0;
+    if (device >= g_gpu_num) return fail(CUFHE_ERR_ARG, "device %d >= gpu num", device);
+    if (num_gates == 0 || num_wires == 0) return fail(CUFHE_ERR_ARG, "empty circuit");
+    if (num_gates > (1u << 26) || num_wires > (1u << 30))
+        return fail(CUFHE_ERR_ARG, "circuit too large");
+    if (!gate_ops || !in0 || !out) return fail(CUFHE_ERR_ARG, "null circuit array");
+
+    // ---- validation: gate ids, operand and result wires, single assignment
+    std::vector<int32_t> producer(num_wires, -1);
+    for (size_t g = 0; g < num_gates; g++) {
+        const int op = gate_ops[g];
+        if (op < 0 || op >= kNumGates) return fail(CUFHE_ERR_ARG, "bad gate id %d at gate %zu", op, g);
+        const int nin = (op == kNot || op == kCopy) ? 1 : ((op == kMux || op == kNMux) ? 3 : 2);
+        const int32_t* ins[3] = {in0, in1, in2};
+        for (int k = 0; k < nin; k++) {
+            if (!ins[k]) return fail(CUFHE_ERR_ARG, "gate %zu needs operand %d", g, k);
+            if (ins[k][g] < 0 || (size_t)ins[k][g] >= num_wires)
+                return fail(CUFHE_ERR_ARG, "gate %zu operand %d: wire %d out of range", g, k, ins[k][g]);
+        }
+        if (out[g] < 0 || (size_t)out[g] >= num_wires)
+            return fail(CUFHE_ERR_ARG, "gate %zu result wire %d out of range", g, out[g]);
+        if (producer[out[g]] >= 0)
+            return fail(CUFHE_ERR_ARG, "wire %d is written by gates %d and %zu", out[g],
+                        producer[out[g]], g);
+        producer[out[g]] = (int32_t)g;
+    }
+    // ---- levelisation (Kahn): wave of a gate = 1 + latest wave of its producers
+    std::vector<int32_t> indeg(num_gates, 0), wave(num_gates, 0), head(num_gates, -1),
+        nxt, to;
+    for (size_t g = 0; g < num_gates; g++) {
+        const int op = gate_ops[g];
+        const int nin = (op == kNot || op == kCopy) ? 1 : ((op == kMux || op == kNMux) ? 3 : 2);
+        const int32_t* ins[3] = {in0, in1, in2};
+        for (int k = 0; k < nin; k++) {
+            const int32_t p = producer[ins[k][g]];
+            if (p < 0) continue;
+            indeg[g]++;
+            nxt.push_back(head[p]);
+            to.push_back((int32_t)g);
+            head[p] = (int32_t)(to.size() - 1);
+        }
+    }
+    std::vector<int32_t> queue;
+    queue.reserve(num_gates);
+    for (size_t g = 0; g < num_gates; g++)
+        if (!indeg[g]) queue.push_back((int32_t)g);
+    for (size_t qi = 0; qi < queue.size(); qi++) {
+        const int32_t g = queue[qi];
+        for (int32_t e = head[g]; e >= 0; e = nxt[e]) {
+            const int32_t h = to[e];
+            if (wave[g] + 1 > wave[h]) wave[h] = wave[g] + 1;
+            if (--indeg[h] == 0) queue.push_back(h);
+        }
+    }
+    if (queue.size() != num_gates) return fail(CUFHE_ERR_ARG, "the circuit has a cycle");
+    int nwaves = 0;
+    for (size_t g = 0; g < num_gates; g++) nwaves = wave[g] + 1 > nwaves ? wave[g] + 1 : nwaves;
+    std::vector<std::vector<int32_t>> members(nwaves);
+    for (size_t g = 0; g < num_gates; g++) members[wave[g]].push_back((int32_t)g);
+    const DeviceState& D = g_dev[device];
+    if (level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
+        return fail(CUFHE_ERR_STATE, level == CUFHE_LVL02 ? "cufhe_initialize_lvl02() not called"
+                                                         : "cufhe_initialize() not called");
+
+    // ---- per-wave plan arrays, packed into one buffer (16-byte aligned)
+    auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    std::vector<size_t> off(nwaves);
+    size_t total = 0;
+    int max_lanes = 0, max_gates = 0;
+    for (int w = 0; w < nwaves; w++) {
+        const size_t n = members[w].size();
+        size_t lanes = 0;
+        for (int32_t g : members[w]) lanes += lanes_of_gate(gate_ops[g]);
+        off[w] = total;
+        total += al(n) + al(4 * n) + al(4 * lanes) + al(lanes) + 4 * al(4 * n);
+        max_lanes = (int)lanes > max_lanes ? (int)lanes : max_lanes;
+        max_gates = (int)n > max_gates ? (int)n : max_gates;
+    }
+    std::vector<unsigned char> host(total, 0);
+    cufhe_circuit_s* c = new cufhe_circuit_s();
+    c->device = device;
+    c->level = level;
+    c->wires = num_wires;
+    c->gates = num_gates;
+    c->max_lanes = max_lanes;
+    c->max_gates = max_gates;
+    c->exec.device = device;
+    int rc = CUFHE_OK;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaMalloc(&c->dbuf, total);
+    if (e != cudaSuccess) {
+        circuit_free(c);
+        return fail(CUFHE_ERR_NOMEM, "circuit plan buffer: %s", cudaGetErrorString(e));
+    }
+    unsigned char* dbase = static_cast<unsigned char*>(c->dbuf);
+    for (int w = 0; w < nwaves; w++) {
+        const std::vector<int32_t>& m = members[w];
+        const size_t n = m.size();
+        size_t lanes = 0;
+        for (int32_t g : m) lanes += lanes_of_gate(gate_ops[g]);
+        size_t o = off[w];
+        const size_t o_ops = o; o += al(n);
+        const size_t o_l0 = o; o += al(4 * n);
+        const size_t o_lg = o; o += al(4 * lanes);
+        const size_t o_ls = o; o += al(lanes);
+        size_t o_idx[4];
+        for (int k = 0; k < 4; k++) { o_idx[k] = o; o += al(4 * n); }
+        int8_t* ops = (int8_t*)&host[o_ops];
+        int32_t* l0 = (int32_t*)&host[o_l0];
+        int32_t* lg = (int32_t*)&host[o_lg];
+        int8_t* ls = (int8_t*)&host[o_ls];
+        int32_t* idx[4];
+        for (int k = 0; k < 4; k++) idx[k] = (int32_t*)&host[o_idx[k]];
+        size_t l = 0;
+        bool nc = false;
+        for (size_t b = 0; b < n; b++) {
+            const int32_t g = m[b];
+            const int op = gate_ops[g];
+            const int nl = lanes_of_gate(op);
+            ops[b] = (int8_t)op;
+            l0[b] = nl ? (int32_t)l : -1;
+            for (int k = 0; k < nl; k++, l++) {
+                lg[l] = (int32_t)b;
+                ls[l] = (int8_t)k;
+            }
+            nc |= nl == 0;
+            const int nin = (op == kNot || op == kCopy) ? 1 : ((op == kMux || op == kNMux) ? 3 : 2);
+            const int32_t* ins[3] = {in0, in1, in2};
+            for (int k = 0; k < 3; k++) idx[k][b] = k < nin ? ins[k][g] : 0;  // unused -> row 0
+            idx[3][b] = out[g];
+        }
+        Plan p = Plan();
+        p.count = (int)n;
+        p.lanes = (int)lanes;
+        p.uniform_op = 0;
+        p.ops = (const int8_t*)(dbase + o_ops);
+        p.gate_lane0 = (const int32_t*)(dbase + o_l0);
+        p.lane_gate = (const int32_t*)(dbase + o_lg);
+        p.lane_sub = (const int8_t*)(dbase + o_ls);
+        for (int k = 0; k < 3; k++) p.in_idx[k] = (const int32_t*)(dbase + o_idx[k]);
+        p.out_idx = (const int32_t*)(dbase + o_idx[3]);
+        c->waves.push_back(p);
+        c->wave_nc.push_back(nc ? 1 : 0);
+    }
+    e = cudaMemcpy(c->dbuf, host.data(), total, cudaMemcpyHostToDevice);
+    // workspace for the widest wave
+    Workspace& ws = c->exec.ws;
+    const size_t cap = max_lanes < 1 ? 1 : (size_t)max_lanes;
+    if (e == cudaSuccess) e = cudaMalloc(&ws.lane_in, cap * kTlwe0 * 4);
+    if (e == cudaSuccess) {
+        if (level == CUFHE_LVL02) {
+            e = cudaMalloc(&ws.lane_out2, cap * CUFHE_TLWE2_WORDS * 8);
+            ws.lane2_cap = cap;
+        } else {
+            e = cudaMalloc(&ws.lane_out, cap * kTlwe1 * 4);
+        }
+        ws.lane_cap = cap;
+    }
+    if (e == cudaSuccess) {
+        const int units = level == CUFHE_LVL1 ? max_lanes : max_gates;
+        if (units > 0) e = iks_tc_reserve(level == CUFHE_LVL02 ? ws.iks2 : ws.iks, units,
+                                          level == CUFHE_LVL02);
+    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        circuit_free(c);
+        return fail(CUFHE_ERR_NOMEM, "circuit buffers: %s", cudaGetErrorString(e));
+    }
+    (void)rc;
+    *out_c = c;
+    return CUFHE_OK;
+}
+
+int cufhe_circuit_info(cufhe_circuit_t c, int* waves, int* max_wave_gates, int* max_wave_lanes)
+{
+    if (!c) return fail(CUFHE_ERR_ARG, "null circuit");
+    if (waves) *waves = (int)c->waves.size();
+    if (max_wave_gates) *max_wave_gates = c->max_gates;
+    if (max_wave_lanes) *max_wave_lanes = c->max_lanes;
+    return CUFHE_OK;
+}
+
+int cufhe_circuit_wave_sizes(cufhe_circuit_t c, int32_t* gates, int32_t* lanes, size_t cap)
+{
+    if (!c) return fail(CUFHE_ERR_ARG, "null circuit");
+    for (size_t w = 0; w < c->waves.size() && w < cap; w++) {
+        if (gates) gates[w] = c->waves[w].count;
+        if (lanes) lanes[w] = c->waves[w].lanes;
+    }
+    return (int)c->waves.size();
+}
+
+int cufhe_circuit_run(cufhe_circuit_t c, uint32_t* wires, cufhe_stream_t st, int use_graph)
+{
+    if (!c || !wires) return fail(CUFHE_ERR_ARG, "null circuit or wire table");
+    cufhe_stream_s* s = resolve(st);
+    if (s->device != c->device)
+        return fail(CUFHE_ERR_ARG, "circuit lives on device %d, stream on %d", c->device, s->device);
+    const DeviceState& D = g_dev[c->device];
+    if (c->level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
+        return fail(CUFHE_ERR_STATE, "keys of the circuit's level are not initialised");
+    CK(cudaSetDevice(c->device));
+    // the INT8 form synchronises inside its launcher, so it always runs directly
+    const bool graph = use_graph && !(c->level != CUFHE_LVL02 && g_precision == CUFHE_INT8_EXACT);
+    if (!graph) {
+        c->exec.st = s->st;
+        for (size_t w = 0; w < c->waves.size(); w++) {
+            const int rc = run_wave(c, w, wires);
+            if (rc) return rc;
+        }
+        return CUFHE_OK;
+    }
+    if (!c->gexec || c->graph_wires != wires || c->graph_precision != g_precision) {
+        const int rc = circuit_capture(c, wires);
+        if (rc) return rc;
+    }
+    CK(cudaGraphLaunch(c->gexec, s->st));
+    g_launches.fetch_add(c->graph_launches);
+    return CUFHE_OK;
+}
+
+int cufhe_circuit_destroy(cufhe_circuit_t c)
+{
+    if (!c) return CUFHE_OK;
+    cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
+    circuit_free(c);
+    return CUFHE_OK;
+}
+
+int cufhe_autotune(void)
+{
+    int d = 0;
+    CK(cudaGetDevice(&d));
+    return autotune_br(d);
+}
+
+int cufhe_autotune_table(int32_t* lanes, int32_t* lanes_per_cta, int cap)
+{
+    int d = 0;
+    CK(cudaGetDevice(&d));
+    int b[32], g[32];
+    const int n = br_fp64_get_tuning(d, b, g, 32);
+    for (int i = 0; i < n && i < cap; i++) {
+        if (lanes) lanes[i] = b[i];
+        if (lanes_per_cta) lanes_per_cta[i] = g[i];
+    }
+    return n;
 }
 
 int cufhe_profile_enable(int on)

@@ -65,7 +65,9 @@ __host__ __device__ inline int lanes_of_gate(int g)
 // Lane plan of a batch.  With ops == nullptr every gate is `uniform_op` and
 // lanes map arithmetically; otherwise lane_gate[l] is the gate of lane l,
 // lane_sub[l] its index within the gate (0/1), gate_lane0[b] the first lane
-// of gate b (-1 for Not/Copy).
+// of gate b (-1 for Not/Copy).  Gate b reads operand k from row in_idx[k][b]
+// of its input array and writes its result to row out_idx[b] of the output
+// array (a circuit's wire table); a null index array means row b.
 struct Plan {
     int count;       // gates
     int lanes;       // lanes
@@ -74,6 +76,8 @@ struct Plan {
     const int32_t* lane_gate;
     const int8_t* lane_sub;
     const int32_t* gate_lane0;
+    const int32_t* in_idx[3];
+    const int32_t* out_idx;
 };
 
 __device__ inline int plan_op(const Plan& p, int b) { return p.ops ? p.ops[b] : p.uniform_op; }
@@ -90,6 +94,16 @@ __device__ inline void plan_lane(const Plan& p, int l, int& b, int& sub)
         b = l;
         sub = 0;
     }
+}
+
+__host__ __device__ inline size_t plan_in_row(const Plan& p, int k, int b)
+{
+    return p.in_idx[k] ? (size_t)p.in_idx[k][b] : (size_t)b;
+}
+
+__host__ __device__ inline size_t plan_out_row(const Plan& p, int b)
+{
+    return p.out_idx ? (size_t)p.out_idx[b] : (size_t)b;
 }
 
 __device__ inline int plan_lane0(const Plan& p, int b)
@@ -119,6 +133,17 @@ __device__ inline LanePreadd lane_preadd(int op, int sub, const uint32_t* in0,
     }
     const GateCoef c = gate_coef(op);
     return {in0, in1, c.ca, c.cb, c.off};
+}
+
+// Pre-add of lane l of the plan from gate inputs of `words` words each
+__device__ inline LanePreadd plan_lane_preadd(const Plan& p, int l, const uint32_t* in0,
+                                              const uint32_t* in1, const uint32_t* in2, int words)
+{
+    int b, sub;
+    plan_lane(p, l, b, sub);
+    return lane_preadd(plan_op(p, b), sub, in0 + plan_in_row(p, 0, b) * words,
+                       in1 ? in1 + plan_in_row(p, 1, b) * words : nullptr,
+                       in2 ? in2 + plan_in_row(p, 2, b) * words : nullptr);
 }
 
 // Combination of a gate's lane outputs (lvl1 TLWEs) into the gate's lvl1
@@ -161,6 +186,16 @@ cudaError_t launch_br_fp64(bool kb, const uint32_t* lane_in, int lanes, uint32_t
 
 cudaError_t launch_bk_to_fft(const uint32_t* bk, int npolys, const Fp64Tables& t, double2* out,
                              cudaStream_t st);
+// The same rotation with a fixed number of lanes per CTA (1, 2 or 4), for the
+// autotuner; launch_br_fp64 picks it from the tuned table of the device
+// (br_fp64_set_tuning) or, without one, from the batch size.
+cudaError_t launch_br_fp64_g(int g, bool kb, const uint32_t* lane_in, int lanes, uint32_t mu,
+                             const double2* bkf, const Fp64Tables& t, int steps,
+                             uint32_t* acc_out, uint32_t* lane_out, cudaStream_t st);
+// tuned choice for device dev: lanes <= bound[i] (ascending) -> g[i]; the last
+// entry covers larger batches.  n = 0 clears the table.
+void br_fp64_set_tuning(int dev, int n, const int* bound, const int* g);
+int br_fp64_get_tuning(int dev, int* bound, int* g, int cap);
 cudaError_t upload_fft_constants(void);
 
 // Tensor-core identity key switching (iks_tc.cu).  Key tiles are built once
@@ -176,6 +211,9 @@ struct IksWorkspace {
 size_t iks_tc_key_bytes();
 cudaError_t iks_tc_key_build(const uint32_t* ksk_dev, uint8_t* key_tiles, cudaStream_t st);
 void iks_tc_workspace_free(IksWorkspace& w);
+// sizes the workspace for `units` key switches up front (lvl1 or lvl2 inputs),
+// so that later launches allocate nothing
+cudaError_t iks_tc_reserve(IksWorkspace& w, int units, bool lvl2);
 cudaError_t launch_iks_tc(int mode, const Plan& plan, const uint32_t* in0, const uint32_t* in1,
                           const uint32_t* in2, const uint32_t* lane_out, const uint8_t* key_tiles,
                           uint32_t* dst, IksWorkspace& w, int* err, cudaStream_t st,

@@ -17,11 +17,7 @@ __global__ void k_preadd_lvl0(Plan plan, const uint32_t* __restrict__ in0,
 {
     const int l = blockIdx.x;
     if (l >= plan.lanes) return;
-    int b, sub;
-    plan_lane(plan, l, b, sub);
-    const size_t o = (size_t)b * kTlwe0;
-    const LanePreadd p = lane_preadd(plan_op(plan, b), sub, in0 + o, in1 ? in1 + o : nullptr,
-                                     in2 ? in2 + o : nullptr);
+    const LanePreadd p = plan_lane_preadd(plan, l, in0, in1, in2, kTlwe0);
     uint32_t* dst = lane_in + (size_t)l * kTlwe0;
     for (int i = threadIdx.x; i < kTlwe0; i += blockDim.x) {
         uint32_t x = (uint32_t)p.ca * p.a[i];
@@ -41,7 +37,7 @@ __global__ void k_finalize_lvl1(Plan plan, const uint32_t* __restrict__ lane_out
     if (l0 < 0) return;
     const LanePreadd p = gate_combine(op, lane_out + (size_t)l0 * kTlwe1,
                                       lane_out + (size_t)(l0 + 1) * kTlwe1);
-    uint32_t* dst = out + (size_t)b * kTlwe1;
+    uint32_t* dst = out + plan_out_row(plan, b) * kTlwe1;
     for (int i = threadIdx.x; i < kTlwe1; i += blockDim.x) {
         uint32_t x = (uint32_t)p.ca * p.a[i];
         if (p.cb) x += (uint32_t)p.cb * p.b[i];
@@ -57,8 +53,8 @@ __global__ void k_not_copy(Plan plan, int words, const uint32_t* __restrict__ in
     if (b >= plan.count) return;
     const int op = plan_op(plan, b);
     if (op != kNot && op != kCopy) return;
-    const uint32_t* s = in0 + (size_t)b * words;
-    uint32_t* d = out + (size_t)b * words;
+    const uint32_t* s = in0 + plan_in_row(plan, 0, b) * words;
+    uint32_t* d = out + plan_out_row(plan, b) * words;
     for (int i = threadIdx.x; i < words; i += blockDim.x) d[i] = op == kNot ? 0u - s[i] : s[i];
 }
 

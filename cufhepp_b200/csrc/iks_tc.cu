@@ -106,11 +106,7 @@ __global__ void __launch_bounds__(256) k_iks_prep(int mode, Plan plan, const uin
     LanePreadd p = {nullptr, nullptr, 0, 0, 0};
     int ok = 0;
     if (mode == 0) {
-        int b, sub;
-        plan_lane(plan, u, b, sub);
-        const size_t o = (size_t)b * kTlwe1;
-        p = lane_preadd(plan_op(plan, b), sub, in0 + o, in1 ? in1 + o : nullptr,
-                        in2 ? in2 + o : nullptr);
+        p = plan_lane_preadd(plan, u, in0, in1, in2, kTlwe1);
         ok = 1;
     } else {
         const int l0 = plan_lane0(plan, u);
@@ -218,7 +214,9 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
                                                      const uint8_t* __restrict__ btiles,
                                                      const uint32_t* __restrict__ xb,
                                                      const int* __restrict__ valid, int units,
-                                                     uint32_t* __restrict__ dst, int* __restrict__ err)
+                                                     uint32_t* __restrict__ dst,
+                                                     const int32_t* __restrict__ dst_idx,
+                                                     int* __restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t raw_addr = smem_u32(smem_raw);
@@ -303,6 +301,7 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
     if (!s_fail) {
         const int u = gt * kMGates + warp * 32 + lane;  // this thread's TMEM lane = gate row
         const bool live = u < units && valid[u];
+        const size_t row = live ? (dst_idx ? (size_t)dst_idx[u] : (size_t)u) : 0;
         const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
 #pragma unroll 1
         for (int cc = 0; cc < kNCols / 32; cc++) {
@@ -316,7 +315,7 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
                     uint32_t r = v[4 * oo] + (v[4 * oo + 1] << 8) + (v[4 * oo + 2] << 16) +
                                  (v[4 * oo + 3] << 24);
                     if (o == kN0) r += xb[u];
-                    if (o < kTlwe0) dst[(size_t)u * kTlwe0 + o] = r;
+                    if (o < kTlwe0) dst[row * kTlwe0 + o] = r;
                 }
             }
         }
@@ -363,6 +362,11 @@ static cudaError_t iks_tc_workspace(IksWorkspace& w, int units, int chunks)
     return cudaSuccess;
 }
 
+cudaError_t iks_tc_reserve(IksWorkspace& w, int units, bool lvl2)
+{
+    return iks_tc_workspace(w, units, lvl2 ? iks_chunks<CUFHE_LVL2_N>() : kChunks);
+}
+
 void iks_tc_workspace_free(IksWorkspace& w)
 {
     cudaFree(w.atiles);
@@ -399,8 +403,8 @@ cudaError_t launch_iks_tc(int mode, const Plan& plan, const uint32_t* in0, const
     if (e != cudaSuccess) return e;
     k_iks_prep<<<units, 256, 0, st>>>(mode, plan, in0, in1, in2, lane_out, w.atiles, w.xb, w.valid);
     const int gtiles = (units + kMGates - 1) / kMGates;
-    k_iks_gemm<kChunks><<<gtiles * kNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, w.xb, w.valid,
-                                                              units, dst, err);
+    k_iks_gemm<kChunks><<<gtiles * kNTiles, 128, kSmem, st>>>(
+        w.atiles, key_tiles, w.xb, w.valid, units, dst, mode == 1 ? plan.out_idx : nullptr, err);
     *launches = 2;
     return cudaGetLastError();
 }
@@ -419,7 +423,7 @@ cudaError_t launch_iks20_tc(const Plan& plan, const uint64_t* lane_out, const ui
     k_iks20_prep<<<units, 256, 0, st>>>(plan, lane_out, w.atiles, w.xb, w.valid);
     const int gtiles = (units + kMGates - 1) / kMGates;
     k_iks_gemm<kCh><<<gtiles * kNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, w.xb, w.valid,
-                                                          units, dst, err);
+                                                          units, dst, plan.out_idx, err);
     *launches = 2;
     return cudaGetLastError();
 }

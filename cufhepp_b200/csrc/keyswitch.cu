@@ -55,11 +55,7 @@ __global__ void __launch_bounds__(kIksThreads) k_iks(int mode, Plan plan, const 
         int ok = 0;
         if (u < total) {
             if (mode == 0) {
-                int b, sub;
-                plan_lane(plan, u, b, sub);
-                const size_t o = (size_t)b * kTlwe1;
-                p = lane_preadd(plan_op(plan, b), sub, in0 + o, in1 ? in1 + o : nullptr,
-                                in2 ? in2 + o : nullptr);
+                p = plan_lane_preadd(plan, u, in0, in1, in2, kTlwe1);
                 ok = 1;
             } else {
                 const int op = plan_op(plan, u);
@@ -135,7 +131,10 @@ __global__ void __launch_bounds__(kIksThreads) k_iks(int mode, Plan plan, const 
     if (tid < kTlwe0) {
 #pragma unroll
         for (int g = 0; g < G; g++)
-            if (first + g < total && valid[g]) dst[(size_t)(first + g) * kTlwe0 + tid] = acc[g];
+            if (first + g < total && valid[g]) {
+                const size_t row = mode == 0 ? (size_t)(first + g) : plan_out_row(plan, first + g);
+                dst[row * kTlwe0 + tid] = acc[g];
+            }
     }
 }
 

@@ -58,6 +58,13 @@ SIGNATURES = {
     "cufhe_cleanup_lvl02": ([], _i),
     "cufhe_blind_rotate_lvl02": ([_vp, _sz, _u64, _i, _vp, _vp, _vp], _i),
     "cufhe_identity_keyswitch_lvl20": ([_vp, _sz, _vp, _vp], _i),
+    "cufhe_circuit_create": ([_vp, _i, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i], _i),
+    "cufhe_circuit_info": ([_vp, _vp, _vp, _vp], _i),
+    "cufhe_circuit_wave_sizes": ([_vp, _vp, _vp, _sz], _i),
+    "cufhe_circuit_run": ([_vp, _vp, _vp, _i], _i),
+    "cufhe_circuit_destroy": ([_vp], _i),
+    "cufhe_autotune": ([], _i),
+    "cufhe_autotune_table": ([_vp, _vp, _i], _i),
 }
 
 K_IKS, K_PREADD, K_BR_FP64, K_BR_INT8, K_FINALIZE, K_BR_FP64_LVL02, K_IKS_LVL20 = range(7)
@@ -260,6 +267,68 @@ def identity_keyswitch_lvl20(tlwe2, count: int, out, stream=None) -> None:
 def identity_keyswitch(tlwe1, count: int, out, stream=None) -> None:
     check(load().cufhe_identity_keyswitch(dptr(tlwe1), count, dptr(out), stream),
           "identity_keyswitch")
+
+
+class Circuit:
+    """A DAG of gates over a wire table, levelised into waves by the engine
+    (cufhe_circuit_create).  ops/in0/in1/in2/out are per-gate arrays of gate
+    ids and wire indices (-1 for an operand the gate does not take)."""
+
+    def __init__(self, level: int, num_wires: int, ops, in0, in1, in2, out, device: int = 0):
+        arr = lambda a: np.ascontiguousarray(a, np.int32)  # noqa: E731
+        self.ops, self.in0, self.in1, self.in2, self.out = (arr(x) for x in (ops, in0, in1, in2,
+                                                                            out))
+        self.level = level
+        self.num_wires = int(num_wires)
+        self.words = P.TLWE1_WORDS if level == LVL1 else P.TLWE0_WORDS
+        h = C.c_void_p()
+        check(load().cufhe_circuit_create(C.byref(h), level, self.num_wires, self.ops.size,
+                                          _p(self.ops), _p(self.in0), _p(self.in1),
+                                          _p(self.in2), _p(self.out), device), "circuit_create")
+        self.h = h
+
+    def info(self) -> tuple[int, int, int]:
+        w, g, l = C.c_int(), C.c_int(), C.c_int()
+        check(load().cufhe_circuit_info(self.h, C.byref(w), C.byref(g), C.byref(l)), "circuit_info")
+        return w.value, g.value, l.value
+
+    def wave_sizes(self) -> tuple[np.ndarray, np.ndarray]:
+        n = self.info()[0]
+        g = np.zeros(n, np.int32)
+        lanes = np.zeros(n, np.int32)
+        load().cufhe_circuit_wave_sizes(self.h, _p(g), _p(lanes), n)
+        return g, lanes
+
+    def run(self, wires, stream=None, graph: bool = True) -> None:
+        check(load().cufhe_circuit_run(self.h, dptr(wires), stream, int(graph)), "circuit_run")
+
+    def destroy(self) -> None:
+        if getattr(self, "h", None):
+            load().cufhe_circuit_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def autotune() -> list[tuple[int, int]]:
+    """Measures the blind rotation's lanes per CTA for a ladder of batch
+    sizes on the current device; returns [(max lanes, lanes per CTA)]."""
+    L = load()
+    check(L.cufhe_autotune(), "autotune")
+    return autotune_table()
+
+
+def autotune_table() -> list[tuple[int, int]]:
+    b = np.zeros(32, np.int32)
+    g = np.zeros(32, np.int32)
+    n = load().cufhe_autotune_table(_p(b), _p(g), 32)
+    if n < 0:
+        check(n, "autotune_table")
+    return [(int(b[i]), int(g[i])) for i in range(n)]
 
 
 def profile_enable(on: bool = True) -> None:

@@ -224,6 +224,49 @@ int cufhe_blind_rotate_lvl02(const uint32_t* tlwe0, size_t count, uint64_t mu, i
 int cufhe_identity_keyswitch_lvl20(const uint64_t* tlwe2, size_t count, uint32_t* tlwe0_out,
                                    cufhe_stream_t st);
 
+/* ---- circuits of dependent gates -------------------------------------- */
+/* No counterpart in the reference, whose callers track dependencies
+ * themselves (polling StreamQuery per gate, test/test_intensive.cc:23-56).
+ *
+ * A circuit is a DAG of gates over a table of num_wires ciphertexts of one
+ * level (CUFHE_LVL0, CUFHE_LVL1 or CUFHE_LVL02): gate g computes
+ * gate_ops[g] on wires in0[g] (, in1[g], in2[g] as the gate needs; Mux takes
+ * in0 = selector, in1 = selected when 1, in2 = selected when 0) and writes wire
+ * out[g].  Every wire is written by at most one gate; wires no gate writes are
+ * the circuit's inputs.  Gates may be listed in any order.
+ *
+ * cufhe_circuit_create checks the DAG (ranges, single assignment, no cycle),
+ * levelises it into waves of independent gates (a gate's wave is one more than
+ * the latest wave among the gates it reads from), uploads every wave's plan
+ * and wire indices once and sizes a private workspace for the widest wave.
+ * cufhe_circuit_run runs all waves in order on `st` over the device wire
+ * table `wires` ([num_wires][words of the level]); with use_graph = 1 the
+ * waves are captured into one CUDA graph the first time (and again when
+ * `wires` or the precision form changes) and replayed afterwards.  Runs of
+ * one circuit share its workspace: do not overlap them on the GPU.  The INT8
+ * form always launches directly.  Per-kernel profiling does not see graph
+ * replays. */
+typedef struct cufhe_circuit_s* cufhe_circuit_t;
+int cufhe_circuit_create(cufhe_circuit_t* c, int level, size_t num_wires, size_t num_gates,
+                         const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
+                         const int32_t* in2, const int32_t* out, int device);
+int cufhe_circuit_info(cufhe_circuit_t c, int* waves, int* max_wave_gates, int* max_wave_lanes);
+/* gates and blind rotations of each wave; returns the number of waves */
+int cufhe_circuit_wave_sizes(cufhe_circuit_t c, int32_t* gates, int32_t* lanes, size_t cap);
+int cufhe_circuit_run(cufhe_circuit_t c, uint32_t* wires, cufhe_stream_t st, int use_graph);
+int cufhe_circuit_destroy(cufhe_circuit_t c);
+
+/* ---- autotuner -------------------------------------------------------- */
+/* Measures, on the current device with its keys, how many lanes (blind
+ * rotations) per CTA the FP64 blind rotation should carry for a ladder of
+ * batch sizes, and makes every later launch on that device use the
+ * measured choice (takes about a second; CUFHE_BR_LANES_PER_CTA still
+ * overrides).  cufhe_autotune_table reads the table back: batches of up to
+ * lanes[i] blind rotations use lanes_per_cta[i]; returns its length (0 when
+ * the device is untuned and a built-in rule applies). */
+int cufhe_autotune(void);
+int cufhe_autotune_table(int32_t* lanes, int32_t* lanes_per_cta, int cap);
+
 /* ---- diagnostics ----------------------------------------------------- */
 /* Per-kernel timing: when enabled, every engine kernel launch is bracketed
  * by CUDA events on its stream; cufhe_profile_read() sums the durations of

@@ -1,0 +1,152 @@
+"""GPU checks of the circuit executor (cufhe_circuit_*) and the autotuner.
+
+* a merged uneven workload (random levelised DAGs + ripple-carry adders) at
+  each ciphertext level decrypts to its plaintext evaluation on every wire;
+* the CUDA-graph run, its replay and the direct run give identical wires;
+* the result is bit-identical to evaluating the same waves one by one
+  through cufhe_gate_batch (the circuit adds scheduling, not arithmetic);
+* the INT8 form runs circuits (directly) and decrypts correctly;
+* cufhe_autotune yields a table of lanes-per-CTA choices and gates stay
+  correct under it.
+"""
+import numpy as np
+import pytest
+
+from cufhepp_b200 import circuits as CI, client, engine, params as P
+
+pytestmark = pytest.mark.gpu
+
+
+def words_of(level):
+    return P.TLWE1_WORDS if level == engine.LVL1 else P.TLWE0_WORDS
+
+
+def prepare(sk, net, level, seed):
+    rng = np.random.default_rng(seed)
+    bits = rng.integers(0, 2, net.inputs.size).astype(np.uint8)
+    host = np.zeros((net.num_wires, words_of(level)), np.uint32)
+    host[net.inputs] = client.encrypt_bits(sk, bits, 0 if level == engine.LVL02 else level,
+                                           seed=seed)
+    return bits, host
+
+
+def check_decrypts(sk, net, level, bits, wires):
+    plain = CI.evaluate(net, bits)
+    got = client.decrypt_bits(sk, wires[net.out], 0 if level == engine.LVL02 else level)
+    assert int(np.count_nonzero(got != plain[net.out])) == 0
+
+
+def run_circuit(net, level, host):
+    d = engine.to_device(host)
+    c = engine.Circuit(level, net.num_wires, net.ops, net.in0, net.in1, net.in2, net.out)
+    c.run(d, graph=False)
+    direct = engine.from_device(d, host.shape)
+    c.run(d, graph=True)
+    g1 = engine.from_device(d, host.shape)
+    c.run(d, graph=True)
+    g2 = engine.from_device(d, host.shape)
+    info = c.info()
+    c.destroy()
+    return direct, g1, g2, info
+
+
+def wave_by_wave(net, level, host):
+    """The same circuit evaluated level by level through cufhe_gate_batch_host."""
+    ref = host.copy()
+    lv = CI.levels(net)
+    for w in range(int(lv.max()) + 1):
+        gs = np.nonzero(lv == w)[0]
+        rows = lambda idx: ref[np.where(idx[gs] >= 0, idx[gs], 0)]  # noqa: E731
+        out = engine.gate_batch_host(net.ops[gs], level, rows(net.in0), rows(net.in1),
+                                     rows(net.in2))
+        engine.synchronize()
+        ref[net.out[gs]] = out
+    return ref
+
+
+@pytest.fixture(scope="module")
+def lvl1_ctx(keys):
+    sk, ek_kb, _ = keys
+    engine.initialize(ek_kb)
+    engine.set_precision(P.FP64_FFNT)
+    yield sk
+    engine.cleanup()
+
+
+@pytest.mark.parametrize("level", [engine.LVL1, engine.LVL0], ids=["lvl1", "lvl0"])
+def test_uneven_circuit_matches_plaintext_and_batches(lvl1_ctx, level):
+    sk = lvl1_ctx
+    net = CI.uneven_workload(11 + level, dags=12, adders=4, dag_gates=(50, 400),
+                             adder_width=(8, 24))
+    bits, host = prepare(sk, net, level, 40 + level)
+    direct, g1, g2, (waves, max_gates, max_lanes) = run_circuit(net, level, host)
+    assert waves == int(CI.levels(net).max()) + 1
+    assert np.array_equal(direct, g1) and np.array_equal(g1, g2)
+    check_decrypts(sk, net, level, bits, direct)
+    assert np.array_equal(direct, wave_by_wave(net, level, host))
+
+
+def test_circuit_with_not_copy_and_nmux(lvl1_ctx):
+    sk = lvl1_ctx
+    # hand-written: wires 0..3 inputs
+    ops = [P.NOT, P.COPY, P.NMUX, P.XNOR, P.MUX, P.NOT]
+    i0 = [0, 1, 2, 4, 6, 8]
+    i1 = [-1, -1, 3, 5, 4, -1]
+    i2 = [-1, -1, 0, -1, 5, -1]
+    out = [4, 5, 6, 7, 8, 9]
+    net = CI.Netlist(10, np.arange(4, dtype=np.int32), *(np.asarray(x, np.int32)
+                     for x in (ops, i0, i1, i2, out)), np.asarray(out, np.int32))
+    for trial in range(3):
+        bits, host = prepare(sk, net, engine.LVL1, 90 + trial)
+        direct, g1, _, (waves, _, _) = run_circuit(net, engine.LVL1, host)
+        assert waves == 3 and np.array_equal(direct, g1)
+        check_decrypts(sk, net, engine.LVL1, bits, direct)
+
+
+def test_circuit_int8_form(keys):
+    sk, _, ek = keys
+    engine.initialize(ek)
+    engine.set_precision(P.INT8_EXACT)
+    try:
+        net = CI.uneven_workload(5, dags=2, adders=1, dag_gates=(50, 80), adder_width=(8, 8))
+        bits, host = prepare(sk, net, engine.LVL1, 55)
+        d = engine.to_device(host)
+        c = engine.Circuit(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1, net.in2, net.out)
+        c.run(d, graph=True)  # the INT8 form launches directly
+        wires = engine.from_device(d, host.shape)
+        c.destroy()
+        check_decrypts(sk, net, engine.LVL1, bits, wires)
+    finally:
+        engine.set_precision(P.FP64_FFNT)
+        engine.initialize(keys[1])  # the KeyBundle key of the module's other tests
+
+
+def test_circuit_lvl02():
+    sk = client.SecretKey.generate(0xC1C)
+    engine.initialize_lvl02(client.EvalKey02.generate(sk, keybundle=True))
+    try:
+        net = CI.uneven_workload(9, dags=4, adders=2, dag_gates=(50, 150), adder_width=(8, 12))
+        bits, host = prepare(sk, net, engine.LVL02, 77)
+        direct, g1, g2, _ = run_circuit(net, engine.LVL02, host)
+        assert np.array_equal(direct, g1) and np.array_equal(g1, g2)
+        check_decrypts(sk, net, engine.LVL02, bits, direct)
+    finally:
+        engine.cleanup_lvl02()
+
+
+def test_autotune_table_and_gates(lvl1_ctx):
+    sk = lvl1_ctx
+    table = engine.autotune()
+    assert len(table) >= 4
+    bounds = [b for b, _ in table]
+    assert bounds == sorted(bounds)
+    assert all(g in (1, 2, 4) for _, g in table)
+    assert engine.autotune_table() == table
+    gates = np.array([P.NAND, P.MUX, P.XOR, P.AND] * 300, np.int32)
+    rng = np.random.default_rng(4)
+    a, b, c = (rng.integers(0, 2, gates.size).astype(np.uint8) for _ in range(3))
+    cts = [client.encrypt_bits(sk, x, 1, seed=140 + i) for i, x in enumerate((a, b, c))]
+    out = engine.gate_batch_host(gates, engine.LVL1, *cts)
+    engine.synchronize()
+    exp = np.array([P.TRUTH[g](int(x), int(y), int(z)) for g, x, y, z in zip(gates, a, b, c)])
+    assert np.array_equal(client.decrypt_bits(sk, out, 1), exp)
