@@ -33,6 +33,7 @@ ENGINE_SOURCES = [
     "peaks.cu",
     "noalloc.cu",
     "br_fp64_lvl02.cu",
+    "cb.cu",
 ]
 
 

@@ -39,6 +39,7 @@ def _load():
             "tfhe_ksk32_gen": [u64, vp, u32, vp, u32, u32, u32, dbl, vp],
             "tfhe_bk64_gen": [u64, vp, u32, vp, u32, u32, u32, dbl, i, vp],
             "tfhe_trlwe64_phase": [vp, u32, vp, vp],
+            "tfhe_privks_gen": [u64, vp, u32, vp, u32, u32, u32, dbl, i, vp],
         }
         for name, argt in sigs.items():
             fn = getattr(lib, name)
@@ -117,6 +118,47 @@ class EvalKey02:
         lib.tfhe_ksk32_gen(seed + 1, _p(sk.lvl2), P.LVL2_N, _p(sk.lvl0), P.LVL0_N,
                            P.LVL20_BASEBIT, P.LVL20_T, P.LVL0_ALPHA, _p(ksk))
         return cls(bk, ksk, keybundle)
+
+
+def privks_key(key_src: np.ndarray, key1: np.ndarray, func: int, seed: int,
+               basebit: int = 4, t: int = 10, alpha: float = P.LVL1_ALPHA) -> np.ndarray:
+    """Private key-switching key TLWE<src> -> TRLWE<lvl1> for circuit
+    bootstrapping: [n_src+1][t][2^basebit-1][2][N] uint32 encrypting
+    f(k_i (u+1) 2^-(j+1)basebit), f(x) = -x s1 (func 0) or x (func 1)."""
+    lib = _load()
+    n_src = int(key_src.size)
+    out = np.empty((n_src + 1) * t * ((1 << basebit) - 1) * 2 * P.LVL1_N, np.uint32)
+    lib.tfhe_privks_gen(seed, _p(np.ascontiguousarray(key_src, np.int32)), n_src,
+                        _p(np.ascontiguousarray(key1, np.int32)), P.LVL1_N, basebit, t, alpha,
+                        func, _p(out))
+    return out
+
+
+@dataclass
+class CBKey:
+    """Keys of circuit bootstrapping lvl0 -> TRGSW<lvl1> (l = 3, Bgbit = 6): the
+    lvl02 bootstrapping key (EvalKey02) and the two private key-switching keys
+    lvl2 -> lvl1 (basebit 4, t 10) for the a-rows (f = -x s1) and b-rows (f = x)."""
+    ek02: EvalKey02
+    privks0: np.ndarray
+    privks1: np.ndarray
+
+    @classmethod
+    def generate(cls, sk: SecretKey, seed: int | None = None, keybundle: bool = True,
+                 ek02: EvalKey02 | None = None) -> "CBKey":
+        seed = sk.seed + 0xCB if seed is None else seed
+        ek02 = ek02 or EvalKey02.generate(sk, keybundle=keybundle)
+        return cls(ek02, privks_key(sk.lvl2, sk.lvl1, 0, seed),
+                   privks_key(sk.lvl2, sk.lvl1, 1, seed))
+
+
+def trgsw_encrypt_g(sk: SecretKey, m: int, seed: int, stream: int, l: int, bgbit: int,
+                    alpha: float = P.LVL1_ALPHA) -> np.ndarray:
+    """TRGSW<lvl1>(m) with l digits of bgbit bits: [2l][2][N] uint32."""
+    lib = _load()
+    out = np.empty(2 * l * P.TRLWE1_WORDS, np.uint32)
+    lib.tfhe_trgsw32_encrypt(seed, stream, _p(sk.lvl1), P.LVL1_N, l, bgbit, m, alpha, _p(out))
+    return out
 
 
 def trlwe64_phase(sk: SecretKey, c: np.ndarray) -> np.ndarray:

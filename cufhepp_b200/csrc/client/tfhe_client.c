@@ -351,3 +351,44 @@ uint64_t tfhe_tlwe64_phase(const int32_t* key, uint32_t n, const uint64_t* c)
     for (uint32_t i = 0; i < n; i++) p -= c[i] * (uint64_t)(uint32_t)key[i];
     return p;
 }
+
+/* ------------------------------------------ private key switching key ---- */
+/* Key of the private functional key switching TLWE<src> (Torus64, n_src
+ * mask coefficients) -> TRLWE<lvl1> that circuit bootstrapping uses
+ * (CGGI17, the privKS lvl2 -> lvl1 of the circuit-bootstrapping workload):
+ *   out[i][j][u] = TRLWE_s1( f(c) ),  i in [0, n_src], j < t, u < 2^basebit - 1,
+ *   c = k_i * v_{j,u},  k_i = key_src[i] (i < n_src), k_{n_src} = -1,
+ *   v_{j,u} = (u + 1) 2^(64 - (j+1) basebit) rounded to Torus32,
+ *   f(x) = -x * s1(X) for func 0 (the rows that carry the message in the
+ *   mask polynomial) and f(x) = x for func 1 (rows carrying it in b).
+ * Layout [n_src + 1][t][2^basebit - 1][2][N] uint32; row (i, j, u) uses RNG
+ * stream 0x400000000 + ((func (n_src+1) + i) t + j) (2^basebit - 1) + u. */
+void tfhe_privks_gen(uint64_t seed, const int32_t* key_src, uint32_t n_src, const int32_t* key1,
+                     uint32_t N, uint32_t basebit, uint32_t t, double alpha, int func,
+                     uint32_t* out)
+{
+    const uint32_t nu = (1u << basebit) - 1;
+    const int64_t rows = (int64_t)(n_src + 1) * t * nu;
+#pragma omp parallel
+    {
+        uint32_t* msg = (uint32_t*)malloc(sizeof(uint32_t) * N);
+#pragma omp for schedule(static)
+        for (int64_t q = 0; q < rows; q++) {
+            const uint32_t u = (uint32_t)(q % nu);
+            const uint32_t j = (uint32_t)((q / nu) % t);
+            const uint32_t i = (uint32_t)(q / ((int64_t)nu * t));
+            const int shift = 64 - (int)((j + 1) * basebit);
+            const uint64_t v64 = (uint64_t)(u + 1) << shift;
+            const uint32_t v = (uint32_t)((v64 + (1ull << 31)) >> 32);
+            const uint32_t k = i < n_src ? (uint32_t)key_src[i] : 0xFFFFFFFFu;
+            const uint32_t c = k * v;
+            for (uint32_t m = 0; m < N; m++)
+                msg[m] = func == 0 ? (uint32_t)(0u - c * (uint32_t)key1[m]) : (m == 0 ? c : 0u);
+            crng_t r;
+            crng_seed(&r, seed, 0x400000000ull + ((uint64_t)func * (n_src + 1) + i) * t * nu +
+                                   (uint64_t)j * nu + u);
+            trlwe32_encrypt_rng(&r, key1, N, msg, alpha, out + (uint64_t)q * 2 * N);
+        }
+        free(msg);
+    }
+}

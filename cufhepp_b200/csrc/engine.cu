@@ -41,6 +41,11 @@ struct DeviceState {
     double2* psi2 = nullptr;     // psi2^s, s <= 512
     uint8_t* iks2_key = nullptr; // lvl20 KSK byte-limb tiles
     int* err2 = nullptr;
+    // circuit bootstrapping (cufhe_initialize_cb)
+    bool ready_cb = false;
+    uint32_t* pks[2] = {nullptr, nullptr};  // private key-switching keys lvl2 -> lvl1
+    double2* cb_psi = nullptr;               // lvl1 FFT tables for CMUX
+    double2* cb_tw512 = nullptr;
 };
 
 struct Workspace {
@@ -59,6 +64,10 @@ struct Workspace {
     size_t lane2_cap = 0;
     uint64_t* lane_out2 = nullptr;  // lvl2 lane outputs [lanes][2049]
     IksWorkspace iks2;
+    size_t lut_cap = 0;             // lookup tables the node buffers hold
+    uint32_t* lut_a = nullptr;      // CMUX-tree node buffers [q][256] / [q][128] TRLWEs
+    uint32_t* lut_b = nullptr;
+    uint8_t* lut_tab = nullptr;     // the tables, [q][256] bytes
 };
 
 }  // namespace
@@ -176,6 +185,9 @@ void free_ws(Workspace& w)
     iks_tc_workspace_free(w.iks);
     cudaFree(w.lane_out2);
     iks_tc_workspace_free(w.iks2);
+    cudaFree(w.lut_a);
+    cudaFree(w.lut_b);
+    cudaFree(w.lut_tab);
     w = Workspace();
 }
 
@@ -236,10 +248,13 @@ void host_tables(std::vector<double2>& psi, std::vector<double2>& tw)
         }
 }
 
+void release_cb(int d);
+
 void release_device02(int d)
 {
     DeviceState& D = g_dev[d];
     cudaSetDevice(d);
+    release_cb(d);
     cudaFree(D.bkf2);
     cudaFree(D.psi2);
     cudaFree(D.iks2_key);
@@ -251,10 +266,24 @@ void release_device02(int d)
     D.kb2 = 0;
 }
 
+void release_cb(int d)
+{
+    DeviceState& D = g_dev[d];
+    cudaSetDevice(d);
+    cudaFree(D.pks[0]);
+    cudaFree(D.pks[1]);
+    cudaFree(D.cb_psi);
+    cudaFree(D.cb_tw512);
+    D.pks[0] = D.pks[1] = nullptr;
+    D.cb_psi = D.cb_tw512 = nullptr;
+    D.ready_cb = false;
+}
+
 void release_device(int d)
 {
     DeviceState& D = g_dev[d];
     cudaSetDevice(d);
+    release_cb(d);
     release_device02(d);
     cudaFree(D.ksk);
     cudaFree(D.bkf);
@@ -342,6 +371,30 @@ int init_device02(int d, const cufhe_keyview02* ek)
     cudaFree(ksk);
     D.kb2 = ek->keybundle;
     D.ready2 = true;
+    return CUFHE_OK;
+}
+
+// cufhe_initialize_cb on device d: private key-switching keys and the lvl1
+// FFT tables of the CMUX kernels
+int init_cb(int d, const cufhe_cbkeyview* kv)
+{
+    DeviceState& D = g_dev[d];
+    CK(cudaSetDevice(d));
+    CK(upload_cb_constants());
+    CK(upload_fft_constants());  // k_bk_to_fft (TRGSW -> Fourier) lives in br_fp64.cu
+    std::vector<double2> psi, tw;
+    host_tables(psi, tw);
+    CK(cudaMalloc(&D.cb_psi, psi.size() * sizeof(double2)));
+    CK(cudaMalloc(&D.cb_tw512, tw.size() * sizeof(double2)));
+    CK(cudaMemcpy(D.cb_psi, psi.data(), psi.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(D.cb_tw512, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    const uint32_t* src[2] = {kv->privks0, kv->privks1};
+    for (int f = 0; f < 2; f++) {
+        if (cudaMalloc(&D.pks[f], kv->words * sizeof(uint32_t)) != cudaSuccess)
+            return fail(CUFHE_ERR_NOMEM, "private key-switching key (%zu words)", kv->words);
+        CK(cudaMemcpy(D.pks[f], src[f], kv->words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    }
+    D.ready_cb = true;
     return CUFHE_OK;
 }
 
@@ -1290,6 +1343,191 @@ int cufhe_circuit_destroy(cufhe_circuit_t c)
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
     circuit_free(c);
+    return CUFHE_OK;
+}
+
+int cufhe_initialize_cb(const cufhe_cbkeyview* kv)
+{
+    if (!kv || !kv->privks0 || !kv->privks1) return fail(CUFHE_ERR_ARG, "null key view");
+    const uint64_t want = (uint64_t)(CUFHE_LVL2_N + 1) * 10 * 15 * CUFHE_TRLWE1_WORDS;
+    if (kv->words != want)
+        return fail(CUFHE_ERR_ARG, "private key-switching key has %zu words, expected %llu",
+                    kv->words, (unsigned long long)want);
+    int avail = 0;
+    if (cudaGetDeviceCount(&avail) != cudaSuccess || avail == 0)
+        return fail(CUFHE_ERR_CUDA, "no CUDA device visible");
+    for (int d = 0; d < g_gpu_num; d++) {
+        if (g_dev[d].ready_cb) release_cb(d);
+        const int rc = init_cb(d, kv);
+        if (rc) {
+            release_cb(d);
+            return rc;
+        }
+    }
+    cudaSetDevice(0);
+    return CUFHE_OK;
+}
+
+int cufhe_cleanup_cb(void)
+{
+    for (int d = 0; d < kMaxDev; d++)
+        if (g_dev[d].ready_cb) release_cb(d);
+    cudaSetDevice(0);
+    return CUFHE_OK;
+}
+
+int cufhe_private_keyswitch(const uint64_t* tlwe2, size_t count, int func, uint32_t* trlwe_out,
+                            cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    const DeviceState& D = g_dev[s->device];
+    if (!D.ready_cb) return fail(CUFHE_ERR_STATE, "cufhe_initialize_cb() not called");
+    if (!tlwe2 || !trlwe_out) return fail(CUFHE_ERR_ARG, "null pointer");
+    if (func != 0 && func != 1) return fail(CUFHE_ERR_ARG, "bad key-switching function %d", func);
+    if (count == 0) return CUFHE_OK;
+    if (count > (1u << 24)) return fail(CUFHE_ERR_ARG, "too many inputs");
+    CK(cudaSetDevice(s->device));
+    PksMap map = {};
+    map.per = (int)count;
+    map.stride_lo = CUFHE_TRLWE1_WORDS;
+    LAUNCH(CUFHE_K_PRIVKS, s->st, launch_privks(tlwe2, (int)count, D.pks[func], map, trlwe_out, s->st));
+    return CUFHE_OK;
+}
+
+int cufhe_circuit_bootstrap(const uint32_t* tlwe0, size_t count, uint32_t* trgsw_out,
+                            cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    const DeviceState& D = g_dev[s->device];
+    if (!D.ready_cb) return fail(CUFHE_ERR_STATE, "cufhe_initialize_cb() not called");
+    if (!D.ready2) return fail(CUFHE_ERR_STATE, "cufhe_initialize_lvl02() not called");
+    if (!tlwe0 || !trgsw_out) return fail(CUFHE_ERR_ARG, "null pointer");
+    if (count == 0) return CUFHE_OK;
+    if (count > (1u << 22)) return fail(CUFHE_ERR_ARG, "too many inputs");
+    CK(cudaSetDevice(s->device));
+    int rc = ensure_lane2(s, 3 * count);
+    if (rc) return rc;
+    uint64_t* t2 = s->ws.lane_out2;
+    constexpr int kL = 3, kBgbit = 6;
+    PksMap map = {};
+    map.per = (int)count;  // unit u = i * count + bit
+    map.stride_lo = (size_t)2 * kL * CUFHE_TRLWE1_WORDS;
+    map.stride_hi = CUFHE_TRLWE1_WORDS;
+    for (int i = 0; i < kL; i++) {
+        const uint64_t mu = 1ull << (64 - (i + 1) * kBgbit - 1);
+        map.badd[i] = mu;
+        rc = run_br2(s, tlwe0, (int)count, mu, -1, nullptr, t2 + (size_t)i * count * CUFHE_TLWE2_WORDS);
+        if (rc) return rc;
+    }
+    for (int f = 0; f < 2; f++)
+        LAUNCH(CUFHE_K_PRIVKS, s->st,
+               launch_privks(t2, (int)(3 * count), D.pks[f], map,
+                             trgsw_out + (size_t)f * kL * CUFHE_TRLWE1_WORDS, s->st));
+    return CUFHE_OK;
+}
+
+static int gadget_rows(int gadget) { return gadget == CUFHE_GADGET_CB ? 6 : 4; }
+
+int cufhe_trgsw_to_fft(int gadget, const uint32_t* trgsw, size_t count, double* fft_out,
+                       cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    const DeviceState& D = g_dev[s->device];
+    if (gadget != CUFHE_GADGET_LVL1 && gadget != CUFHE_GADGET_CB)
+        return fail(CUFHE_ERR_ARG, "bad gadget %d", gadget);
+    if (!trgsw || !fft_out) return fail(CUFHE_ERR_ARG, "null pointer");
+    const double2* psi = D.ready_cb ? D.cb_psi : D.psi;
+    const double2* tw = D.ready_cb ? D.cb_tw512 : D.tw512;
+    if (!psi) return fail(CUFHE_ERR_STATE, "cufhe_initialize() or cufhe_initialize_cb() not called");
+    if (count == 0) return CUFHE_OK;
+    if (count > (1u << 22)) return fail(CUFHE_ERR_ARG, "too many TRGSWs");
+    CK(cudaSetDevice(s->device));
+    const Fp64Tables t = {psi, tw};
+    LAUNCH(CUFHE_K_CMUX, s->st,
+           launch_bk_to_fft(trgsw, (int)(count * 2 * gadget_rows(gadget)), t,
+                            reinterpret_cast<double2*>(fft_out), s->st));
+    return CUFHE_OK;
+}
+
+int cufhe_cmux(int gadget, const double* trgsw_fft, const uint32_t* d1, const uint32_t* d0,
+               uint32_t* out, size_t count, cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    const DeviceState& D = g_dev[s->device];
+    if (gadget != CUFHE_GADGET_LVL1 && gadget != CUFHE_GADGET_CB)
+        return fail(CUFHE_ERR_ARG, "bad gadget %d", gadget);
+    if (!trgsw_fft || !d1 || !d0 || !out) return fail(CUFHE_ERR_ARG, "null pointer");
+    const double2* psi = D.ready_cb ? D.cb_psi : D.psi;
+    const double2* tw = D.ready_cb ? D.cb_tw512 : D.tw512;
+    if (!psi) return fail(CUFHE_ERR_STATE, "cufhe_initialize() or cufhe_initialize_cb() not called");
+    if (count == 0) return CUFHE_OK;
+    if (count > (1u << 24)) return fail(CUFHE_ERR_ARG, "too many CMUXes");
+    CK(cudaSetDevice(s->device));
+    CmuxPlan p = {};
+    p.count = (int)count;
+    p.per = 1;
+    p.node_stride_g = 1;
+    p.d0 = d0;
+    p.d1 = d1;
+    p.trgsw = reinterpret_cast<const double2*>(trgsw_fft);
+    p.trgsw_stride = (size_t)2 * gadget_rows(gadget) * 512;
+    p.out = out;
+    const Fp64Tables t = {psi, tw};
+    LAUNCH(CUFHE_K_CMUX, s->st, launch_cmux(gadget, p, t, s->st));
+    return CUFHE_OK;
+}
+
+int cufhe_lut_eval(const uint8_t* luts_host, size_t num_luts, const double* trgsw_fft,
+                   uint32_t mu, uint32_t* tlwe1_out, cufhe_stream_t st)
+{
+    cufhe_stream_s* s = resolve(st);
+    const DeviceState& D = g_dev[s->device];
+    if (!luts_host || !trgsw_fft || !tlwe1_out) return fail(CUFHE_ERR_ARG, "null pointer");
+    const double2* psi = D.ready_cb ? D.cb_psi : D.psi;
+    const double2* tw = D.ready_cb ? D.cb_tw512 : D.tw512;
+    if (!psi) return fail(CUFHE_ERR_STATE, "cufhe_initialize() or cufhe_initialize_cb() not called");
+    if (num_luts == 0) return CUFHE_OK;
+    if (num_luts > (1u << 16)) return fail(CUFHE_ERR_ARG, "too many lookup tables");
+    CK(cudaSetDevice(s->device));
+    Workspace& w = s->ws;
+    const int q = (int)num_luts;
+    if (num_luts > w.lut_cap) {
+        CK(cudaStreamSynchronize(s->st));
+        cudaFree(w.lut_a);
+        cudaFree(w.lut_b);
+        cudaFree(w.lut_tab);
+        w.lut_a = w.lut_b = nullptr;
+        w.lut_tab = nullptr;
+        w.lut_cap = 0;
+        if (cudaMalloc(&w.lut_a, num_luts * 256 * kTrlwe * 4) != cudaSuccess ||
+            cudaMalloc(&w.lut_b, num_luts * 128 * kTrlwe * 4) != cudaSuccess ||
+            cudaMalloc(&w.lut_tab, num_luts * 256) != cudaSuccess)
+            return fail(CUFHE_ERR_NOMEM, "lookup-table buffers for %zu tables", num_luts);
+        w.lut_cap = num_luts;
+    }
+    CK(cudaMemcpyAsync(w.lut_tab, luts_host, num_luts * 256, cudaMemcpyHostToDevice, s->st));
+    LAUNCH(CUFHE_K_CMUX, s->st, launch_lut_leaves(w.lut_tab, q, mu, w.lut_a, s->st));
+    const Fp64Tables t = {psi, tw};
+    const size_t trgsw_words = (size_t)2 * gadget_rows(CUFHE_GADGET_CB) * 512;  // double2
+    uint32_t* in = w.lut_a;
+    uint32_t* outb = w.lut_b;
+    for (int k = 0, width = 128; k < 8; k++, width >>= 1) {
+        CmuxPlan p = {};
+        p.per = width;  // CMUXes per table at this level
+        p.count = q * width;
+        p.node_stride_g = (size_t)2 * width;
+        p.node_stride_m = 2;
+        p.d0 = in;
+        p.d1 = in + kTrlwe;
+        p.trgsw = reinterpret_cast<const double2*>(trgsw_fft) + (size_t)k * trgsw_words;
+        p.trgsw_stride = 8 * trgsw_words;
+        p.out = outb;
+        LAUNCH(CUFHE_K_CMUX, s->st, launch_cmux(CUFHE_GADGET_CB, p, t, s->st));
+        uint32_t* tmp = in;
+        in = outb;
+        outb = tmp;
+    }
+    LAUNCH(CUFHE_K_CMUX, s->st, launch_extract8(in, q, tlwe1_out, s->st));
     return CUFHE_OK;
 }
 

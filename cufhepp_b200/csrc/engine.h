@@ -243,6 +243,36 @@ cudaError_t launch_iks20_tc(const Plan& plan, const uint64_t* lane_out, const ui
                             uint32_t* dst, IksWorkspace& w, int* err, cudaStream_t st,
                             int* launches);
 
+// ------------------------------- circuit bootstrapping, CMUX, lookup tables ----
+// Private key switching TLWE<lvl2> -> TRLWE<lvl1>: unit u reads TLWE u (with
+// badd[u / per] added to its b) and writes its TRLWE at
+// out + (u % per) * stride_lo + (u / per) * stride_hi (words).
+struct PksMap {
+    int per;
+    size_t stride_lo, stride_hi;
+    uint64_t badd[4];
+};
+cudaError_t launch_privks(const uint64_t* tlwe, int units, const uint32_t* key, const PksMap& map,
+                          uint32_t* out, cudaStream_t st);
+
+// Batched CMUX: CMUX c = (g, m) with g = c / per, m = c % per reads d0/d1 at
+// node g * node_stride_g + m * node_stride_m (TRLWE units), the Fourier TRGSW at
+// trgsw + g * trgsw_stride (double2 units) and writes out[g * per + m].
+struct CmuxPlan {
+    int count, per;
+    size_t node_stride_g, node_stride_m;
+    const uint32_t* d0;
+    const uint32_t* d1;
+    const double2* trgsw;
+    size_t trgsw_stride;
+    uint32_t* out;
+};
+cudaError_t launch_cmux(int gadget, const CmuxPlan& p, const Fp64Tables& t, cudaStream_t st);
+cudaError_t launch_lut_leaves(const uint8_t* luts, int q, uint32_t mu, uint32_t* nodes,
+                              cudaStream_t st);
+cudaError_t launch_extract8(const uint32_t* roots, int q, uint32_t* out, cudaStream_t st);
+cudaError_t upload_cb_constants(void);
+
 // Read-only view of the engine state that a gate call on stream `st` uses
 // (keys of the stream's device and the CUDA stream).  Returns 0 or a
 // CUFHE_ERR_* code (and sets the last error).

@@ -64,16 +64,30 @@ SIGNATURES = {
     "cufhe_circuit_run": ([_vp, _vp, _vp, _i], _i),
     "cufhe_circuit_destroy": ([_vp], _i),
     "cufhe_autotune": ([], _i),
+    "cufhe_initialize_cb": ([_vp], _i),
+    "cufhe_cleanup_cb": ([], _i),
+    "cufhe_private_keyswitch": ([_vp, _sz, _i, _vp, _vp], _i),
+    "cufhe_circuit_bootstrap": ([_vp, _sz, _vp, _vp], _i),
+    "cufhe_trgsw_to_fft": ([_i, _vp, _sz, _vp, _vp], _i),
+    "cufhe_cmux": ([_i, _vp, _vp, _vp, _vp, _sz, _vp], _i),
+    "cufhe_lut_eval": ([_vp, _sz, _vp, _u32, _vp, _vp], _i),
     "cufhe_autotune_table": ([_vp, _vp, _i], _i),
 }
 
-K_IKS, K_PREADD, K_BR_FP64, K_BR_INT8, K_FINALIZE, K_BR_FP64_LVL02, K_IKS_LVL20 = range(7)
-K_NAMES = ["iks", "preadd", "br_fp64", "br_int8", "finalize", "br_fp64_lvl02", "iks_lvl20"]
+(K_IKS, K_PREADD, K_BR_FP64, K_BR_INT8, K_FINALIZE, K_BR_FP64_LVL02, K_IKS_LVL20, K_PRIVKS,
+ K_CMUX) = range(9)
+K_NAMES = ["iks", "preadd", "br_fp64", "br_int8", "finalize", "br_fp64_lvl02", "iks_lvl20",
+           "privks", "cmux"]
+GADGET_LVL1, GADGET_CB = 0, 1
 
 
 class KeyView(C.Structure):
     _fields_ = [("bk", _vp), ("bk_words", _sz), ("ksk", _vp), ("ksk_words", _sz),
                 ("keybundle", _i)]
+
+
+class CBKeyView(C.Structure):
+    _fields_ = [("privks0", _vp), ("privks1", _vp), ("words", _sz)]
 
 
 class CufheError(RuntimeError):
@@ -212,6 +226,46 @@ def initialize_lvl02(ek02, gpus: int | None = None) -> None:
 
 def cleanup_lvl02() -> None:
     check(load().cufhe_cleanup_lvl02(), "cleanup_lvl02")
+
+
+def initialize_cb(cbkey) -> None:
+    """Circuit bootstrapping: lvl02 keys (if not yet initialised by the caller
+    use initialize_lvl02(cbkey.ek02) first) and the private key-switching keys."""
+    k0 = np.ascontiguousarray(cbkey.privks0, np.uint32)
+    k1 = np.ascontiguousarray(cbkey.privks1, np.uint32)
+    assert k0.size == k1.size
+    kv = CBKeyView(k0.ctypes.data, k1.ctypes.data, k0.size)
+    check(load().cufhe_initialize_cb(C.byref(kv)), "initialize_cb")
+
+
+def cleanup_cb() -> None:
+    check(load().cufhe_cleanup_cb(), "cleanup_cb")
+
+
+def private_keyswitch(tlwe2, count: int, func: int, out, stream=None) -> None:
+    check(load().cufhe_private_keyswitch(dptr(tlwe2), count, func, dptr(out), stream),
+          "private_keyswitch")
+
+
+def circuit_bootstrap(tlwe0, count: int, trgsw_out, stream=None) -> None:
+    check(load().cufhe_circuit_bootstrap(dptr(tlwe0), count, dptr(trgsw_out), stream),
+          "circuit_bootstrap")
+
+
+def trgsw_to_fft(gadget: int, trgsw, count: int, out, stream=None) -> None:
+    check(load().cufhe_trgsw_to_fft(gadget, dptr(trgsw), count, dptr(out), stream),
+          "trgsw_to_fft")
+
+
+def cmux(gadget: int, trgsw_fft, d1, d0, out, count: int, stream=None) -> None:
+    check(load().cufhe_cmux(gadget, dptr(trgsw_fft), dptr(d1), dptr(d0), dptr(out), count,
+                            stream), "cmux")
+
+
+def lut_eval(luts: np.ndarray, trgsw_fft, mu: int, out, stream=None) -> None:
+    luts = np.ascontiguousarray(luts, np.uint8).reshape(-1, 256)
+    check(load().cufhe_lut_eval(_p(luts), luts.shape[0], dptr(trgsw_fft), mu, dptr(out), stream),
+          "lut_eval")
 
 
 def synchronize() -> None:

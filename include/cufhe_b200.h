@@ -256,6 +256,62 @@ int cufhe_circuit_wave_sizes(cufhe_circuit_t c, int32_t* gates, int32_t* lanes, 
 int cufhe_circuit_run(cufhe_circuit_t c, uint32_t* wires, cufhe_stream_t st, int use_graph);
 int cufhe_circuit_destroy(cufhe_circuit_t c);
 
+/* ---- circuit bootstrapping, CMUX, lookup tables ----------------------- */
+/* Gadgets of TRGSW<lvl1> (N = 1024, Torus32): */
+#define CUFHE_GADGET_LVL1 0 /* l = 2, Bgbit = 8: the bootstrapping gadget (lvl1param) */
+#define CUFHE_GADGET_CB 1   /* l = 3, Bgbit = 6: circuit-bootstrapping output */
+
+/* Keys of circuit bootstrapping (CGGI17 form): the two private key-switching
+ * keys lvl2 -> lvl1 (basebit 4, t 10), each TRLWE<lvl1>[2049][10][15] =
+ * 629,452,800 uint32 words, encrypting f(k_i (u+1) 2^-4(j+1)) with
+ * f(x) = -x s1 (privks0, rows carrying the message in the mask) and f(x) = x
+ * (privks1).  Circuit bootstrapping also needs cufhe_initialize_lvl02 (its
+ * blind rotations go to lvl2).  No counterpart in the reference, whose circuit
+ * bootstrapping is annihilation-based (include/circuitbootstrapping_gpu.cuh:
+ * 1-69) and takes different keys. */
+typedef struct cufhe_cbkeyview {
+    const uint32_t* privks0;
+    const uint32_t* privks1;
+    size_t words; /* of each key */
+} cufhe_cbkeyview;
+int cufhe_initialize_cb(const cufhe_cbkeyview* kv);
+int cufhe_cleanup_cb(void);
+
+/* Private key switching of count TLWE<lvl2> (uint64 [count][2049], device)
+ * with key func (0 or 1) into TRLWE<lvl1> [count][2][1024] (device). */
+int cufhe_private_keyswitch(const uint64_t* tlwe2, size_t count, int func, uint32_t* trlwe_out,
+                            cufhe_stream_t st);
+
+/* Circuit bootstrapping of count lvl0 TLWEs (device [count][637], bits
+ * encrypted as +-1/8) into TRGSW<lvl1> with the CB gadget, raw Torus32
+ * [count][6 rows][2][1024] (row r = j*3 + i): per bit three blind rotations
+ * to lvl2 with test polynomial 2^-(6(i+1)+1), plus that value on b, then
+ * private key switching with privks0 (rows j = 0) and privks1 (rows j = 1). */
+int cufhe_circuit_bootstrap(const uint32_t* tlwe0, size_t count, uint32_t* trgsw_out,
+                            cufhe_stream_t st);
+
+/* Raw TRGSW<lvl1> ([count][2l][2][1024]) -> Fourier form ([count][2l][2][512]
+ * complex doubles, interleaved re/im) for cufhe_cmux / cufhe_lut_eval
+ * (the reference's TRGSW NTT form, src/bootstrap_gpu.cu:59-112). */
+int cufhe_trgsw_to_fft(int gadget, const uint32_t* trgsw, size_t count, double* fft_out,
+                       cufhe_stream_t st);
+
+/* Batched CMUX: out[i] = d0[i] + ExtProd(C_i, d1[i] - d0[i]) over TRLWE<lvl1>
+ * (device [count][2][1024]) with Fourier TRGSWs C_i -- CMUXNTT
+ * (src/cufhe_gates_gpu.cu:116-133) for count selections at once. */
+int cufhe_cmux(int gadget, const double* trgsw_fft, const uint32_t* d1, const uint32_t* d0,
+               uint32_t* out, size_t count, cufhe_stream_t st);
+
+/* 8-bit -> 8-bit lookup tables: luts_host [num_luts][256] bytes (entry x
+ * holds the 8 output bits of input x); trgsw_fft [num_luts][8] Fourier
+ * TRGSWs with the CB gadget (TRGSW k of a table selects on input bit k,
+ * least significant first: e.g. circuit-bootstrapped bits); out
+ * [num_luts][8][1025] TLWE<lvl1> (device) encrypting output bit b as +-mu.
+ * Each table is a CMUX tree of 255 CMUXes over leaves packing the 8 output
+ * bits in coefficients 0..7; the trees of all tables advance level by level. */
+int cufhe_lut_eval(const uint8_t* luts_host, size_t num_luts, const double* trgsw_fft,
+                   uint32_t mu, uint32_t* tlwe1_out, cufhe_stream_t st);
+
 /* ---- autotuner -------------------------------------------------------- */
 /* Measures, on the current device with its keys, how many lanes (blind
  * rotations) per CTA the FP64 blind rotation should carry for a ladder of
@@ -278,7 +334,9 @@ int cufhe_autotune_table(int32_t* lanes, int32_t* lanes_per_cta, int cap);
 #define CUFHE_K_FINALIZE 4   /* lane combination (Mux) and Not/Copy */
 #define CUFHE_K_BR_FP64_LVL02 5 /* FP64 FFNT blind rotation to lvl2 + SampleExtract */
 #define CUFHE_K_IKS_LVL20 6  /* key switching lvl2 -> lvl0 */
-#define CUFHE_K_CLASSES 7
+#define CUFHE_K_PRIVKS 7     /* private key switching lvl2 -> lvl1 */
+#define CUFHE_K_CMUX 8       /* CMUX (lookup tables, cufhe_cmux) */
+#define CUFHE_K_CLASSES 9
 int cufhe_profile_enable(int on);
 int cufhe_profile_reset(void);
 int cufhe_profile_read(int kernel_class, double* total_ms, uint64_t* launches);

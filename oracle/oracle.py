@@ -72,6 +72,15 @@ def lib():
             "orc2_ffnt_roundtrip": ([vp, vp, vp], None),
             "orc2_ffnt_square": ([vp, vp, vp], None),
             "orc_double_to_torus64": ([C.c_double], C.c_uint64),
+            "orc_privks": ([vp, u32, vp, vp], None),
+            "orc_privks_batch": ([vp, i64, u32, vp, vp], None),
+            "orc_extprod_exact_g": ([vp, vp, i, i, vp], None),
+            "orc_extprod_fp64_g": ([vp, vp, vp, i, i, vp], None),
+            "orc_polys_to_fft": ([vp, vp, i64, vp], None),
+            "orc_cmux_g": ([vp, vp, vp, i, i, i, vp, vp], None),
+            "orc_cmux_batch_g": ([vp, vp, vp, i64, i, i, i, vp, vp], None),
+            "orc_circuit_bootstrap_batch": ([vp, i64, vp, i, i, vp, vp, vp, vp], None),
+            "orc_lut_eval_batch": ([vp, vp, i64, u32, i, i, i, vp, vp], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -326,3 +335,69 @@ def ffnt2_square(fft: FFT2, x) -> np.ndarray:
 
 def double_to_torus64(d: float) -> int:
     return int(lib().orc_double_to_torus64(d))
+
+
+# ------------------------------- circuit bootstrapping and CMUX lookup tables ---
+CB_L, CB_BGBIT = 3, 6
+PKS_BASEBIT, PKS_T, PKS_NU = 4, 10, 15
+
+
+def privks(tlwe2, key, n_src: int = N2) -> np.ndarray:
+    """Exact private key switching of Torus64 TLWEs [count][n_src+1] -> TRLWE<lvl1>."""
+    t = u64(tlwe2).reshape(-1, n_src + 1)
+    out = np.empty((t.shape[0], TRLWE), np.uint32)
+    lib().orc_privks_batch(_p(t), t.shape[0], n_src, _p(u32(key)), _p(out))
+    return out
+
+
+def extprod_g(trgsw, trlwe, L: int, bgbit: int, mode: int, fft: FFT | None = None) -> np.ndarray:
+    out = np.empty(TRLWE, np.uint32)
+    if mode == EXACT:
+        lib().orc_extprod_exact_g(_p(u32(trgsw)), _p(u32(trlwe)), L, bgbit, _p(out))
+    else:
+        lib().orc_extprod_fp64_g(fft.h, _p(np.ascontiguousarray(trgsw, np.complex128)),
+                                 _p(u32(trlwe)), L, bgbit, _p(out))
+    return out
+
+
+def polys_to_fft(fft: FFT, polys) -> np.ndarray:
+    polys = u32(polys)
+    n = polys.size // N
+    out = np.empty(n * HALF, np.complex128)
+    lib().orc_polys_to_fft(fft.h, _p(polys), n, _p(out))
+    return out
+
+
+def cmux_batch(trgsw, d1, d0, L: int, bgbit: int, mode: int, fft: FFT | None = None) -> np.ndarray:
+    """out[i] = d0[i] + ExtProd(trgsw[i], d1[i] - d0[i]); trgsw raw (EXACT) or Fourier (FP64)."""
+    d1 = u32(d1).reshape(-1, TRLWE)
+    d0 = u32(d0).reshape(-1, TRLWE)
+    t = u32(trgsw) if mode == EXACT else np.ascontiguousarray(trgsw, np.complex128)
+    out = np.empty_like(d1)
+    lib().orc_cmux_batch_g(_p(t), _p(d1), _p(d0), d1.shape[0], L, bgbit, mode,
+                           fft.h if fft else None, _p(out))
+    return out
+
+
+def circuit_bootstrap(x, bk2, kb: bool, mode: int, fft2: FFT2 | None, privks0, privks1) -> np.ndarray:
+    """lvl0 TLWEs [count][637] -> TRGSW<lvl1> (l = 3, Bgbit = 6) [count][6][2048]."""
+    x = u32(x).reshape(-1, TLWE0)
+    bkp = u64(bk2) if mode == EXACT else np.ascontiguousarray(bk2, np.complex128)
+    out = np.empty((x.shape[0], 2 * CB_L, TRLWE), np.uint32)
+    lib().orc_circuit_bootstrap_batch(_p(x), x.shape[0], _p(bkp), int(kb), mode,
+                                      fft2.h if fft2 else None, _p(u32(privks0)),
+                                      _p(u32(privks1)), _p(out))
+    return out
+
+
+def lut_eval(trgsw, luts, mu: int, mode: int, fft: FFT | None = None, L: int = CB_L,
+             bgbit: int = CB_BGBIT) -> np.ndarray:
+    """CMUX-tree lookup tables: luts uint8 [count][256]; trgsw [count][8] TRGSWs
+    (raw for EXACT, Fourier for FP64) -> TLWE<lvl1> [count][8][1025]."""
+    luts = np.ascontiguousarray(luts, np.uint8).reshape(-1, 256)
+    t = u32(trgsw) if mode == EXACT else np.ascontiguousarray(trgsw, np.complex128)
+    out = np.empty((luts.shape[0], 8, TLWE1), np.uint32)
+    lib().orc_lut_eval_batch(_p(t), _p(luts), luts.shape[0], mu, L, bgbit, mode,
+                             fft.h if fft else None, _p(out))
+    return out
+

@@ -1062,3 +1062,213 @@ void orc2_ffnt_square(const orc_fft2_t* c, const double* in, double* out)
         out[i + O2_HALF] = cimag(v);
     }
 }
+
+/* ===================================================================== */
+/* Circuit bootstrapping (CGGI17 form) and CMUX lookup tables.           */
+/*   lvl0 TLWE -> 3 blind rotations to lvl2 (test polynomial mu_i =      */
+/*   2^(64 - 6(i+1) - 1), then b += mu_i: message m 2^(64 - 6(i+1)))     */
+/*   -> private functional key switching lvl2 -> lvl1 (basebit 4, t 10) */
+/*   with f(x) = -x s1 (rows j = 0) and f(x) = x (rows j = 1)            */
+/*   -> TRGSW<lvl1> with l = 3, Bgbit = 6, row r = j l + i.              */
+/* The reference's circuit bootstrapping is annihilation-based            */
+/* (src/circuitbootstrapping_gpu.cu) and has no private key switching,   */
+/* so these functions restate the published CGGI17 procedure; their      */
+/* parity is unpinned against the reference.  The CMUX is the reference's */
+/* CMUX (src/bootstrap_gpu.cu:704-813): d0 + ExtProd(C, d1 - d0).         */
+/* ===================================================================== */
+#define PKS_BASEBIT 4
+#define PKS_T 10
+#define PKS_NU 15
+
+/* exact private key switching: out[2][N] = -sum_i sum_j key[i][j][d_ij - 1]
+ * over the n_src + 1 words of the Torus64 input (TFHEpp PrivKeySwitch) */
+void orc_privks(const uint64_t* tlwe, uint32_t n_src, const uint32_t* key, uint32_t* out)
+{
+    memset(out, 0, sizeof(uint32_t) * O_TRLWE);
+    const uint64_t off = 1ull << (64 - (1 + PKS_BASEBIT * PKS_T));
+    for (uint32_t i = 0; i <= n_src; i++) {
+        const uint64_t abar = tlwe[i] + off;
+        for (int j = 0; j < PKS_T; j++) {
+            const uint32_t d = (uint32_t)(abar >> (64 - (j + 1) * PKS_BASEBIT)) & 15u;
+            if (!d) continue;
+            const uint32_t* row = key + (((size_t)i * PKS_T + j) * PKS_NU + d - 1) * O_TRLWE;
+            for (int w = 0; w < O_TRLWE; w++) out[w] -= row[w];
+        }
+    }
+}
+
+void orc_privks_batch(const uint64_t* tlwe, int64_t count, uint32_t n_src, const uint32_t* key,
+                      uint32_t* out)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t u = 0; u < count; u++)
+        orc_privks(tlwe + u * (n_src + 1), n_src, key, out + u * O_TRLWE);
+}
+
+/* signed gadget digits (L digits of bgbit bits, digit 0 most significant)
+ * of a Torus32 polynomial, with the offset + rounding of
+ * include/gatebootstrapping_gpu.cuh:20-29 */
+static void decompose_g(const uint32_t* poly, int L, int bgbit, int32_t* digits)
+{
+    const uint32_t half = 1u << (bgbit - 1), mask = (1u << bgbit) - 1;
+    uint32_t off = 0;
+    for (int i = 1; i <= L; i++) off += half << (32 - i * bgbit);
+    off += 1u << (32 - L * bgbit - 1);
+    for (int n = 0; n < O_N; n++) {
+        const uint32_t t = poly[n] + off;
+        for (int d = 0; d < L; d++)
+            digits[d * O_N + n] = (int32_t)((t >> (32 - (d + 1) * bgbit)) & mask) - (int32_t)half;
+    }
+}
+
+/* exact external product with a TRGSW of 2L rows (row r = j L + d) */
+void orc_extprod_exact_g(const uint32_t* trgsw, const uint32_t* in, int L, int bgbit, uint32_t* out)
+{
+    int32_t* dig = (int32_t*)malloc(sizeof(int32_t) * L * O_N);
+    memset(out, 0, sizeof(uint32_t) * O_TRLWE);
+    for (int j = 0; j < 2; j++) {
+        decompose_g(in + j * O_N, L, bgbit, dig);
+        for (int d = 0; d < L; d++)
+            for (int oj = 0; oj < 2; oj++)
+                negacyclic_mac_exact(out + oj * O_N, dig + d * O_N,
+                                     trgsw + ((size_t)(j * L + d) * 2 + oj) * O_N);
+    }
+    free(dig);
+}
+
+/* FP64 form: trgsw_f = [2L][2][N/2] Fourier rows (orc_polys_to_fft) */
+void orc_extprod_fp64_g(const orc_fft_t* c, const double complex* trgsw_f, const uint32_t* in,
+                        int L, int bgbit, uint32_t* out)
+{
+    int32_t* dig = (int32_t*)malloc(sizeof(int32_t) * L * O_N);
+    double complex* spec = (double complex*)malloc(sizeof(double complex) * (2 * L + 2) * O_HALF);
+    double complex* acc = spec + 2 * L * O_HALF;
+    double re[O_N];
+    for (int j = 0; j < 2; j++) {
+        decompose_g(in + j * O_N, L, bgbit, dig);
+        for (int d = 0; d < L; d++) {
+            for (int i = 0; i < O_N; i++) re[i] = (double)dig[d * O_N + i];
+            ffnt_forward(c, re, spec + (size_t)(j * L + d) * O_HALF);
+        }
+    }
+    memset(acc, 0, sizeof(double complex) * 2 * O_HALF);
+    for (int r = 0; r < 2 * L; r++)
+        for (int oj = 0; oj < 2; oj++)
+            for (int f = 0; f < O_HALF; f++)
+                acc[oj * O_HALF + f] += spec[r * O_HALF + f] * trgsw_f[(r * 2 + oj) * O_HALF + f];
+    for (int oj = 0; oj < 2; oj++) ffnt_inverse_round(c, acc + oj * O_HALF, out + oj * O_N, 0);
+    free(spec);
+    free(dig);
+}
+
+/* Torus32 polynomials -> Fourier domain (src/bootstrap_gpu.cu:59-112) */
+void orc_polys_to_fft(const orc_fft_t* c, const uint32_t* polys, int64_t npolys,
+                      double complex* out)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < npolys; p++) {
+        double re[O_N];
+        for (int i = 0; i < O_N; i++)
+            re[i] = (double)(int32_t)polys[p * O_N + i] * (1.0 / 4294967296.0);
+        ffnt_forward(c, re, out + p * O_HALF);
+    }
+}
+
+/* CMUX: out = d0 + ExtProd(C, d1 - d0) */
+void orc_cmux_g(const void* trgsw, const uint32_t* d1, const uint32_t* d0, int L, int bgbit,
+                int mode, const orc_fft_t* c, uint32_t* out)
+{
+    uint32_t diff[O_TRLWE], prod[O_TRLWE];
+    for (int w = 0; w < O_TRLWE; w++) diff[w] = d1[w] - d0[w];
+    if (mode == ORC_EXACT)
+        orc_extprod_exact_g((const uint32_t*)trgsw, diff, L, bgbit, prod);
+    else
+        orc_extprod_fp64_g(c, (const double complex*)trgsw, diff, L, bgbit, prod);
+    for (int w = 0; w < O_TRLWE; w++) out[w] = d0[w] + prod[w];
+}
+
+void orc_cmux_batch_g(const void* trgsw, const uint32_t* d1, const uint32_t* d0, int64_t count,
+                      int L, int bgbit, int mode, const orc_fft_t* c, uint32_t* out)
+{
+    const size_t tw = (size_t)2 * L * 2 * (mode == ORC_EXACT ? O_N : O_HALF);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < count; i++) {
+        const void* t = mode == ORC_EXACT ? (const void*)((const uint32_t*)trgsw + i * tw)
+                                          : (const void*)((const double complex*)trgsw + i * tw);
+        orc_cmux_g(t, d1 + i * O_TRLWE, d0 + i * O_TRLWE, L, bgbit, mode, c, out + i * O_TRLWE);
+    }
+}
+
+#define CB_L 3
+#define CB_BGBIT 6
+
+/* circuit bootstrapping of one lvl0 TLWE to TRGSW<lvl1> [6][2][N] */
+void orc_circuit_bootstrap(const uint32_t* tlwe0, const void* bk2, int kb, int mode,
+                           const orc_fft2_t* c2, const uint32_t* privks0, const uint32_t* privks1,
+                           uint32_t* trgsw)
+{
+    uint64_t* acc = (uint64_t*)malloc(sizeof(uint64_t) * (O2_TRLWE + O2_TLWE2));
+    uint64_t* t2 = acc + O2_TRLWE;
+    for (int i = 0; i < CB_L; i++) {
+        const uint64_t mu = 1ull << (64 - (i + 1) * CB_BGBIT - 1);
+        orc2_blind_rotate(tlwe0, mu, bk2, kb, mode, c2, -1, acc);
+        orc2_sample_extract(acc, t2);
+        t2[O2_N] += mu;
+        orc_privks(t2, O2_N, privks0, trgsw + (size_t)(0 * CB_L + i) * O_TRLWE);
+        orc_privks(t2, O2_N, privks1, trgsw + (size_t)(1 * CB_L + i) * O_TRLWE);
+    }
+    free(acc);
+}
+
+void orc_circuit_bootstrap_batch(const uint32_t* tlwe0, int64_t count, const void* bk2, int kb,
+                                 int mode, const orc_fft2_t* c2, const uint32_t* privks0,
+                                 const uint32_t* privks1, uint32_t* trgsw)
+{
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t u = 0; u < count; u++)
+        orc_circuit_bootstrap(tlwe0 + u * O_TLWE0, bk2, kb, mode, c2, privks0, privks1,
+                              trgsw + u * 2 * CB_L * O_TRLWE);
+}
+
+/* SampleExtract at coefficient k of a TRLWE<lvl1> */
+static void sample_extract_k(const uint32_t* acc, int k, uint32_t* tlwe1)
+{
+    for (int n = 0; n < O_N; n++)
+        tlwe1[n] = n <= k ? acc[k - n] : 0u - acc[O_N + k - n];
+    tlwe1[O_N] = acc[O_N + k];
+}
+
+/* 8-bit -> 8-bit lookup table by a CMUX tree over 8 address TRGSWs
+ * (trgsw[k] selects on address bit k, LSB first); the 8 output bits are
+ * packed in coefficients 0..7 of the leaves (+mu for 1, -mu for 0), and
+ * SampleExtract at coefficient b gives output bit b as a TLWE<lvl1>. */
+void orc_lut_eval(const void* trgsw8, const uint8_t* lut, uint32_t mu, int L, int bgbit, int mode,
+                  const orc_fft_t* c, uint32_t* out /* [8][N+1] */)
+{
+    uint32_t* nodes = (uint32_t*)calloc((size_t)256 * O_TRLWE, sizeof(uint32_t));
+    for (int x = 0; x < 256; x++)
+        for (int b = 0; b < 8; b++)
+            nodes[(size_t)x * O_TRLWE + O_N + b] = ((lut[x] >> b) & 1) ? mu : 0u - mu;
+    const size_t tw = (size_t)2 * L * 2 * (mode == ORC_EXACT ? O_N : O_HALF);
+    for (int k = 0, w = 256; k < 8; k++, w >>= 1) {
+        const void* t = mode == ORC_EXACT ? (const void*)((const uint32_t*)trgsw8 + k * tw)
+                                          : (const void*)((const double complex*)trgsw8 + k * tw);
+        for (int m = 0; m < w / 2; m++)
+            orc_cmux_g(t, nodes + (size_t)(2 * m + 1) * O_TRLWE, nodes + (size_t)(2 * m) * O_TRLWE,
+                       L, bgbit, mode, c, nodes + (size_t)m * O_TRLWE);
+    }
+    for (int b = 0; b < 8; b++) sample_extract_k(nodes, b, out + (size_t)b * O_TLWE1);
+    free(nodes);
+}
+
+void orc_lut_eval_batch(const void* trgsw, const uint8_t* luts, int64_t count, uint32_t mu, int L,
+                        int bgbit, int mode, const orc_fft_t* c, uint32_t* out)
+{
+    const size_t tw = (size_t)8 * 2 * L * 2 * (mode == ORC_EXACT ? O_N : O_HALF);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t q = 0; q < count; q++) {
+        const void* t = mode == ORC_EXACT ? (const void*)((const uint32_t*)trgsw + q * tw)
+                                          : (const void*)((const double complex*)trgsw + q * tw);
+        orc_lut_eval(t, luts + q * 256, mu, L, bgbit, mode, c, out + q * 8 * O_TLWE1);
+    }
+}
