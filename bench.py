@@ -66,6 +66,8 @@ def parse():
                     help="skip the lvl0->lvl2 NAND batches reported under the 'lvl02' key")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the uneven-circuit workload reported under the 'uneven' key")
+    ap.add_argument("--no-cb", action="store_true",
+                    help="skip the circuit-bootstrapping + lookup-table workload ('cb_lut' key)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the built-in lanes-per-CTA rule instead of the autotuner's table")
     return ap.parse_args()
@@ -518,6 +520,108 @@ def run_uneven(args, torch, engine, client, P, sk, ek, rank, ws, flush, ref_rate
             "dtype": "f64"}
 
 
+def run_cb(args, torch, engine, client, P, sk, ek1, rank, ws, flush, gates_wl):
+    """Circuit bootstrapping + CMUX lookup tables: 1024 lvl0 bits circuit-
+    bootstrapped to TRGSW<lvl1> (l = 3, Bgbit = 6; three lvl0 -> lvl2 blind
+    rotations and six private key switches lvl2 -> lvl1, basebit 4, t 10, per
+    bit), then 128 random 8-bit -> 8-bit tables evaluated by CMUX trees over
+    them; alone, and on one stream beside a 4096-gate lvl1 batch on another."""
+    cbk = client.CBKey.generate(sk)
+    engine.initialize(ek1)
+    engine.set_precision(P.FP64_FFNT)
+    engine.initialize_lvl02(cbk.ek02)
+    engine.initialize_cb(cbk)
+    q, nbits = 128, 1024
+    rng = np.random.default_rng(args.seed + 17 + rank)
+    luts = rng.integers(0, 256, (q, 256)).astype(np.uint8)
+    addr = rng.integers(0, 256, q)
+    bits = np.array([(int(addr[t]) >> k) & 1 for t in range(q) for k in range(8)], np.uint8)
+    d_x = engine.to_device(client.encrypt_bits(sk, bits, 0, seed=args.seed + 1700 + rank))
+    d_t = engine.DeviceBuffer(nbits * 6 * P.TRLWE1_WORDS * 4)
+    d_f = engine.DeviceBuffer(nbits * 6 * 2 * 512 * 16)
+    d_o = engine.DeviceBuffer(q * 8 * P.TLWE1_WORDS * 4)
+    gates, a, b, c = gates_wl
+    cts = [engine.to_device(client.encrypt_bits(sk, x, 1, seed=args.seed + 1800 + i))
+           for i, x in enumerate((a, b, c))]
+    g_out = engine.DeviceBuffer(gates.size * P.TLWE1_WORDS * 4)
+    sa, sb = engine.Stream(), engine.Stream()
+    ta = torch.cuda.ExternalStream(sa.cuda)
+    tb = torch.cuda.ExternalStream(sb.cuda)
+
+    def cb_step():
+        engine.circuit_bootstrap(d_x, nbits, d_t, sa)
+        engine.trgsw_to_fft(engine.GADGET_CB, d_t, nbits, d_f, sa)
+        engine.lut_eval(luts, d_f, P.MU32, d_o, sa)
+
+    def gate_step():
+        engine.gate_batch(gates, gates.size, 1, g_out, *cts, stream=sb)
+
+    def timed(fn_a, fn_b, n):
+        total = 0.0
+        for _ in range(n):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            ea = torch.cuda.Event()
+            eb = torch.cuda.Event()
+            e0.record(ta)
+            tb.wait_event(e0)
+            if fn_a:
+                fn_a()
+            if fn_b:
+                fn_b()
+            ea.record(ta)
+            eb.record(tb)
+            ta.wait_event(eb)
+            e1.record(ta)
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+            flush.zero_()
+        return max_over_ranks(torch, total, "cuda") / n
+
+    for _ in range(max(args.warmup, 3)):
+        cb_step()
+        gate_step()
+    torch.cuda.synchronize()
+    n = max(2, min(args.steps, 5))
+    engine.profile_reset()
+    engine.profile_enable(True)
+    l0 = engine.kernel_launches()
+    ms_cb = timed(cb_step, None, n)
+    launches = (engine.kernel_launches() - l0) / n
+    engine.profile_enable(False)
+    kern = {}
+    for cls, name in enumerate(engine.K_NAMES):
+        kms, kn = engine.profile_read(cls)
+        if kn:
+            kern[name] = kms / n
+    ms_gates = timed(None, gate_step, n)
+    ms_mixed = timed(cb_step, gate_step, n)
+    out = engine.from_device(d_o, (q, 8, P.TLWE1_WORDS))
+    got = client.decrypt_bits(sk, out.reshape(-1, P.TLWE1_WORDS), 1).reshape(q, 8)
+    want = np.array([[(int(luts[t][addr[t]]) >> k) & 1 for k in range(8)] for t in range(q)])
+    fails = int(np.count_nonzero(got != want))
+    nb = bootstraps(gates)
+    sa.destroy()
+    sb.destroy()
+    engine.cleanup_cb()
+    engine.cleanup_lvl02()
+    engine.cleanup()
+    return {"metric": "circuit-bootstrapped bits/s (1024 bits + 128 8-bit tables per step)",
+            "unit": "bits/s",
+            "workload": ("1024 lvl0 bits -> TRGSW<lvl1> (l=3, Bgbit=6) by 3 lvl0->lvl2 blind "
+                         "rotations + 6 private key switches lvl2->lvl1 (basebit 4, t 10) per bit; "
+                         "128 random 8-bit->8-bit tables by CMUX trees (255 CMUXes each)"),
+            "value": nbits * ws / (ms_cb * 1e-3), "ms_per_step": ms_cb,
+            "luts_per_s": q * ws / (ms_cb * 1e-3), "kernel_ms_per_step": kern,
+            "gpu_launches_per_step": launches, "decrypt_failures": fails,
+            "outputs_checked": q * 8,
+            "mixed": {"gate_batch": f"{gates.size} lvl1 gates ({nb} bootstraps) on a second stream",
+                      "ms_gates_alone": ms_gates, "ms_cb_alone": ms_cb, "ms_both": ms_mixed,
+                      "overlap_saving": 1.0 - ms_mixed / (ms_gates + ms_cb)},
+            "dtype": "f64 (blind rotations, CMUX) + integer (private key switching)"}
+
+
 _PEAK = {}
 
 
@@ -577,6 +681,10 @@ def run_ours(args):
         ek_u = client.EvalKey.generate(sk, keybundle=True)
         uneven = run_uneven(args, torch, engine, client, P, sk, ek_u, rank, ws, flush,
                             results["fp64"]["value"] if "fp64" in results else None)
+    cb = None
+    if not args.no_cb:
+        cb = run_cb(args, torch, engine, client, P, sk, client.EvalKey.generate(sk, keybundle=True),
+                    rank, ws, flush, workload)
     lvl02 = None
     if not args.no_lvl02:
         lvl02 = run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush)
@@ -612,6 +720,8 @@ def run_ours(args):
             line["lvl02"] = lvl02
         if uneven is not None:
             line["uneven"] = uneven
+        if cb is not None:
+            line["cb_lut"] = cb
         line["config"]["br_lanes_per_cta"] = (
             {"source": "autotuner (cufhe_autotune)", "table": tuned} if tuned
             else {"source": "built-in rule"})

@@ -13,12 +13,14 @@
 //              leaves and outputs of 8-bit -> 8-bit lookup tables evaluated as
 //              CMUX trees with the 8 output bits packed in coefficients 0..7.
 //
-// Private key switching layout.  A CTA owns 512 output words (of the 2048 of a
-// TRLWE) for 32 units (TLWEs); thread t accumulates words 2t, 2t+1 of all 32
+// Private key switching layout.  A CTA owns 128 output words (of the 2048 of a
+// TRLWE) for 128 units (TLWEs): warp pair g (threads 64g .. 64g+63) serves
+// units 32g .. 32g+31, thread t accumulating words 2(t mod 64), +1 of its 32
 // units in registers.  The 10 digits of coefficient i of a unit are the top
 // 40 bits of a_i + 2^23; a digit selects one of 15 key rows, read as 64-bit
-// words through L1, so the rows a digit position selects are fetched once per
-// CTA and serve all its units.  The digit branch is uniform across the CTA.
+// words through L1, so each selected row slice is fetched from L2 once per
+// CTA and serves all 128 units (the key, 2.5 GB per function, is streamed
+// once per 128 units).  The digit branch is uniform across a warp.
 #include "cufhe_b200.h"
 #include "engine.h"
 #include "fft64.cuh"
@@ -30,8 +32,9 @@ namespace {
 constexpr int kPksBasebit = 4;
 constexpr int kPksT = 10;
 constexpr int kPksNu = 15;
-constexpr int kPksUnits = 32;   // units per CTA
-constexpr int kPksWords = 512;  // output words per CTA
+constexpr int kPksUnits = 128;  // units per CTA
+constexpr int kPksWords = 128;  // output words per CTA
+constexpr int kPksGroup = 32;   // units per warp pair
 constexpr int kPksCoefBlock = 16;
 constexpr int kN2pks = CUFHE_LVL2_N;
 
@@ -41,12 +44,13 @@ __global__ void __launch_bounds__(256) k_privks(const uint64_t* __restrict__ tlw
 {
     __shared__ uint64_t abar[kPksCoefBlock][kPksUnits];
     const int tid = threadIdx.x;
-    const int w0 = blockIdx.x * kPksWords + 2 * tid;  // this thread's two words
+    const int w0 = blockIdx.x * kPksWords + 2 * (tid & 63);  // this thread's two words
+    const int ug = (tid >> 6) * kPksGroup;                  // first unit of its group
     const int u0 = blockIdx.y * kPksUnits;
     const int nu = min(kPksUnits, units - u0);
-    uint2 acc[kPksUnits];
+    uint2 acc[kPksGroup];
 #pragma unroll
-    for (int u = 0; u < kPksUnits; u++) acc[u] = make_uint2(0u, 0u);
+    for (int u = 0; u < kPksGroup; u++) acc[u] = make_uint2(0u, 0u);
     constexpr uint64_t kOff = 1ull << (64 - (1 + kPksBasebit * kPksT));
 
 #pragma unroll 1
@@ -73,8 +77,8 @@ __global__ void __launch_bounds__(256) k_privks(const uint64_t* __restrict__ tlw
                 const uint32_t* kj = kc + (size_t)j * kPksNu * 2 * CUFHE_LVL1_N;
                 const int sh = 64 - (j + 1) * kPksBasebit;
 #pragma unroll
-                for (int u = 0; u < kPksUnits; u++) {
-                    const uint32_t d = (uint32_t)(abar[cc][u] >> sh) & 15u;
+                for (int u = 0; u < kPksGroup; u++) {
+                    const uint32_t d = (uint32_t)(abar[cc][ug + u] >> sh) & 15u;
                     if (d) {
                         const uint2 k = __ldg(reinterpret_cast<const uint2*>(
                             kj + (size_t)(d - 1) * 2 * CUFHE_LVL1_N));
@@ -86,9 +90,9 @@ __global__ void __launch_bounds__(256) k_privks(const uint64_t* __restrict__ tlw
         }
     }
 #pragma unroll
-    for (int u = 0; u < kPksUnits; u++) {
-        if (u >= nu) break;
-        const int uu = u0 + u;
+    for (int u = 0; u < kPksGroup; u++) {
+        if (ug + u >= nu) break;
+        const int uu = u0 + ug + u;
         uint32_t* row = out + (size_t)(uu % map.per) * map.stride_lo +
                         (size_t)(uu / map.per) * map.stride_hi;
         *reinterpret_cast<uint2*>(row + w0) = acc[u];

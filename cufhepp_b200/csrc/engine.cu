@@ -933,6 +933,13 @@ int cufhe_stream_query(cufhe_stream_t st)
 
 int cufhe_stream_device(cufhe_stream_t st) { return resolve(st)->device; }
 
+int cufhe_stream_cuda(cufhe_stream_t st, void** cuda_stream)
+{
+    if (!cuda_stream) return fail(CUFHE_ERR_ARG, "null pointer");
+    *cuda_stream = static_cast<void*>(resolve(st)->st);
+    return CUFHE_OK;
+}
+
 int cufhe_stream_synchronize(cufhe_stream_t st)
 {
     cufhe_stream_s* s = resolve(st);

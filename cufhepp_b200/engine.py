@@ -34,6 +34,7 @@ SIGNATURES = {
     "cufhe_stream_query": ([_vp], _i),
     "cufhe_stream_device": ([_vp], _i),
     "cufhe_stream_synchronize": ([_vp], _i),
+    "cufhe_stream_cuda": ([_vp, _vp], _i),
     "cufhe_ctxt_alloc": ([_vp, _sz, _i], _i),
     "cufhe_ctxt_free": ([_vp, _i], _i),
     "cufhe_host_register": ([_vp, _sz], _i),
@@ -383,6 +384,26 @@ def autotune_table() -> list[tuple[int, int]]:
     if n < 0:
         check(n, "autotune_table")
     return [(int(b[i]), int(g[i])) for i in range(n)]
+
+
+class Stream:
+    """An engine stream (cufhe_stream_create) and its CUDA stream handle."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        check(load().cufhe_stream_create(C.byref(self.h), device), "stream_create")
+        self._as_parameter_ = self.h  # pass a Stream wherever the C-ABI takes a cufhe_stream_t
+        cs = C.c_void_p()
+        check(load().cufhe_stream_cuda(self.h, C.byref(cs)), "stream_cuda")
+        self.cuda = cs.value or 0
+
+    def synchronize(self) -> None:
+        check(load().cufhe_stream_synchronize(self.h), "stream_synchronize")
+
+    def destroy(self) -> None:
+        if self.h:
+            load().cufhe_stream_destroy(self.h)
+            self.h = None
 
 
 def profile_enable(on: bool = True) -> None:

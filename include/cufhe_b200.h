@@ -135,6 +135,9 @@ int cufhe_stream_destroy(cufhe_stream_t st);
 int cufhe_stream_query(cufhe_stream_t st);
 int cufhe_stream_device(cufhe_stream_t st);
 int cufhe_stream_synchronize(cufhe_stream_t st);
+/* The CUDA stream (cudaStream_t) behind st, for interoperation (events,
+ * other libraries' work ordered with the engine's); NULL = legacy default. */
+int cufhe_stream_cuda(cufhe_stream_t st, void** cuda_stream);
 
 /* ---- ciphertext buffers (Ctxt's per-GPU device buffer and pinned host
  *      copy: include/cufhe_gpu.cuh:78-121, 203-217) -------------------- */
