@@ -1,10 +1,6 @@
-// Circuit bootstrapping (CGGI17 form) and CMUX lookup tables.
+// CMUX and CMUX lookup tables (the private key switching of circuit
+// bootstrapping runs on the tensor cores, iks_tc.cu).
 //
-//   k_privks   private functional key switching TLWE<lvl2> (Torus64) ->
-//              TRLWE<lvl1>: out = -sum_{i <= n2} sum_{j < 10}
-//              KEY[i][j][d_ij - 1], d_ij the j-th 4-bit digit of
-//              a_i + 2^23 (TFHEpp PrivKeySwitch; basebit 4, t 10).  Integer,
-//              bit-exact.
 //   k_cmux     CMUX d0 + ExtProd(C, d1 - d0) with a Fourier-domain TRGSW<lvl1>
 //              of L digits of BGBIT bits (the reference's CMUX,
 //              src/bootstrap_gpu.cu:704-813, with its lvl1 gadget l = 2,
@@ -12,15 +8,7 @@
 //   k_lut_leaves / k_extract8
 //              leaves and outputs of 8-bit -> 8-bit lookup tables evaluated as
 //              CMUX trees with the 8 output bits packed in coefficients 0..7.
-//
-// Private key switching layout.  A CTA owns 128 output words (of the 2048 of a
-// TRLWE) for 128 units (TLWEs): warp pair g (threads 64g .. 64g+63) serves
-// units 32g .. 32g+31, thread t accumulating words 2(t mod 64), +1 of its 32
-// units in registers.  The 10 digits of coefficient i of a unit are the top
-// 40 bits of a_i + 2^23; a digit selects one of 15 key rows, read as 64-bit
-// words through L1, so each selected row slice is fetched from L2 once per
-// CTA and serves all 128 units (the key, 2.5 GB per function, is streamed
-// once per 128 units).  The digit branch is uniform across a warp.
+
 #include "cufhe_b200.h"
 #include "engine.h"
 #include "fft64.cuh"
@@ -29,75 +17,6 @@ namespace cufhe {
 
 namespace {
 
-constexpr int kPksBasebit = 4;
-constexpr int kPksT = 10;
-constexpr int kPksNu = 15;
-constexpr int kPksUnits = 128;  // units per CTA
-constexpr int kPksWords = 128;  // output words per CTA
-constexpr int kPksGroup = 32;   // units per warp pair
-constexpr int kPksCoefBlock = 16;
-constexpr int kN2pks = CUFHE_LVL2_N;
-
-__global__ void __launch_bounds__(256) k_privks(const uint64_t* __restrict__ tlwe, int units,
-                                                const uint32_t* __restrict__ key, PksMap map,
-                                                uint32_t* __restrict__ out)
-{
-    __shared__ uint64_t abar[kPksCoefBlock][kPksUnits];
-    const int tid = threadIdx.x;
-    const int w0 = blockIdx.x * kPksWords + 2 * (tid & 63);  // this thread's two words
-    const int ug = (tid >> 6) * kPksGroup;                  // first unit of its group
-    const int u0 = blockIdx.y * kPksUnits;
-    const int nu = min(kPksUnits, units - u0);
-    uint2 acc[kPksGroup];
-#pragma unroll
-    for (int u = 0; u < kPksGroup; u++) acc[u] = make_uint2(0u, 0u);
-    constexpr uint64_t kOff = 1ull << (64 - (1 + kPksBasebit * kPksT));
-
-#pragma unroll 1
-    for (int c0 = 0; c0 <= kN2pks; c0 += kPksCoefBlock) {
-        __syncthreads();
-        for (int q = tid; q < kPksCoefBlock * kPksUnits; q += blockDim.x) {
-            const int cc = q / kPksUnits, u = q % kPksUnits, c = c0 + cc;
-            uint64_t v = 0;
-            if (u < nu && c <= kN2pks) {
-                const int uu = u0 + u;
-                v = tlwe[(size_t)uu * (kN2pks + 1) + c];
-                if (c == kN2pks) v += map.badd[uu / map.per];
-                v += kOff;
-            }
-            abar[cc][u] = v;
-        }
-        __syncthreads();
-        const int cend = min(kPksCoefBlock, kN2pks + 1 - c0);
-#pragma unroll 1
-        for (int cc = 0; cc < cend; cc++) {
-            const uint32_t* kc = key + (size_t)(c0 + cc) * kPksT * kPksNu * 2 * CUFHE_LVL1_N + w0;
-#pragma unroll 1
-            for (int j = 0; j < kPksT; j++) {
-                const uint32_t* kj = kc + (size_t)j * kPksNu * 2 * CUFHE_LVL1_N;
-                const int sh = 64 - (j + 1) * kPksBasebit;
-#pragma unroll
-                for (int u = 0; u < kPksGroup; u++) {
-                    const uint32_t d = (uint32_t)(abar[cc][ug + u] >> sh) & 15u;
-                    if (d) {
-                        const uint2 k = __ldg(reinterpret_cast<const uint2*>(
-                            kj + (size_t)(d - 1) * 2 * CUFHE_LVL1_N));
-                        acc[u].x -= k.x;
-                        acc[u].y -= k.y;
-                    }
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int u = 0; u < kPksGroup; u++) {
-        if (ug + u >= nu) break;
-        const int uu = u0 + ug + u;
-        uint32_t* row = out + (size_t)(uu % map.per) * map.stride_lo +
-                        (size_t)(uu / map.per) * map.stride_hi;
-        *reinterpret_cast<uint2*>(row + w0) = acc[u];
-    }
-}
 
 // signed digit d (0 = most significant) of an offset Torus32 value, BGBIT bits
 template <int L, int BGBIT>
@@ -221,15 +140,6 @@ cudaError_t upload_cb_constants(void)
         w[k] = make_double2((double)cosl(a), (double)sinl(a));
     }
     return cudaMemcpyToSymbol(c_w32, w, sizeof(w));
-}
-
-cudaError_t launch_privks(const uint64_t* tlwe, int units, const uint32_t* key, const PksMap& map,
-                          uint32_t* out, cudaStream_t st)
-{
-    if (units <= 0) return cudaSuccess;
-    const dim3 grid(2 * CUFHE_LVL1_N / kPksWords, (units + kPksUnits - 1) / kPksUnits);
-    k_privks<<<grid, 256, 0, st>>>(tlwe, units, key, map, out);
-    return cudaGetLastError();
 }
 
 template <int L, int BGBIT>

@@ -43,7 +43,8 @@ struct DeviceState {
     int* err2 = nullptr;
     // circuit bootstrapping (cufhe_initialize_cb)
     bool ready_cb = false;
-    uint32_t* pks[2] = {nullptr, nullptr};  // private key-switching keys lvl2 -> lvl1
+    uint8_t* pks[2] = {nullptr, nullptr};   // private key-switching keys lvl2 -> lvl1 (limb tiles)
+    int* err_cb = nullptr;
     double2* cb_psi = nullptr;               // lvl1 FFT tables for CMUX
     double2* cb_tw512 = nullptr;
 };
@@ -68,6 +69,7 @@ struct Workspace {
     uint32_t* lut_a = nullptr;      // CMUX-tree node buffers [q][256] / [q][128] TRLWEs
     uint32_t* lut_b = nullptr;
     uint8_t* lut_tab = nullptr;     // the tables, [q][256] bytes
+    IksWorkspace iks_pks;           // one-hot tiles of the private key switch
 };
 
 }  // namespace
@@ -188,6 +190,7 @@ void free_ws(Workspace& w)
     cudaFree(w.lut_a);
     cudaFree(w.lut_b);
     cudaFree(w.lut_tab);
+    iks_tc_workspace_free(w.iks_pks);
     w = Workspace();
 }
 
@@ -274,6 +277,8 @@ void release_cb(int d)
     cudaFree(D.pks[1]);
     cudaFree(D.cb_psi);
     cudaFree(D.cb_tw512);
+    cudaFree(D.err_cb);
+    D.err_cb = nullptr;
     D.pks[0] = D.pks[1] = nullptr;
     D.cb_psi = D.cb_tw512 = nullptr;
     D.ready_cb = false;
@@ -388,12 +393,25 @@ int init_cb(int d, const cufhe_cbkeyview* kv)
     CK(cudaMalloc(&D.cb_tw512, tw.size() * sizeof(double2)));
     CK(cudaMemcpy(D.cb_psi, psi.data(), psi.size() * sizeof(double2), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(D.cb_tw512, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&D.err_cb, sizeof(int)));
+    CK(cudaMemset(D.err_cb, 0, sizeof(int)));
     const uint32_t* src[2] = {kv->privks0, kv->privks1};
+    uint32_t* raw = nullptr;
+    if (cudaMalloc(&raw, kv->words * sizeof(uint32_t)) != cudaSuccess)
+        return fail(CUFHE_ERR_NOMEM, "private key-switching key (%zu words)", kv->words);
     for (int f = 0; f < 2; f++) {
-        if (cudaMalloc(&D.pks[f], kv->words * sizeof(uint32_t)) != cudaSuccess)
-            return fail(CUFHE_ERR_NOMEM, "private key-switching key (%zu words)", kv->words);
-        CK(cudaMemcpy(D.pks[f], src[f], kv->words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        cudaError_t e = cudaMalloc(&D.pks[f], privks_tc_key_bytes());
+        if (e == cudaSuccess)
+            e = cudaMemcpy(raw, src[f], kv->words * sizeof(uint32_t), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = privks_tc_key_build(raw, D.pks[f], 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            cudaFree(raw);
+            return fail(CUFHE_ERR_CUDA, "private key-switching key tiles: %s", cudaGetErrorString(e));
+        }
+        g_launches.fetch_add(1);
     }
+    cudaFree(raw);
     D.ready_cb = true;
     return CUFHE_OK;
 }
@@ -480,7 +498,8 @@ int run_iks(cufhe_stream_s* s, int mode, const Plan& plan, const uint32_t* in0, 
 int check_device_error(int d)
 {
     DeviceState& D = g_dev[d];
-    int* flags[2] = {D.ready ? D.err : nullptr, D.ready2 ? D.err2 : nullptr};
+    int* flags[3] = {D.ready ? D.err : nullptr, D.ready2 ? D.err2 : nullptr,
+                     D.ready_cb ? D.err_cb : nullptr};
     for (int* f : flags) {
         if (!f) continue;
         int h = 0;
@@ -490,6 +509,22 @@ int check_device_error(int d)
             return fail(CUFHE_ERR_CUDA, "a tensor-core kernel's bounded wait timed out (code %d)", h);
         }
     }
+    return CUFHE_OK;
+}
+
+// private key switching lvl2 -> lvl1 on the tensor cores
+int run_privks(cufhe_stream_s* s, const uint64_t* tlwe2, int units, int func, const PksMap& map,
+               uint32_t* out)
+{
+    DeviceState& D = g_dev[s->device];
+    int launches = 0;
+    ProfRec pr;
+    prof_begin(s->st, pr, CUFHE_K_PRIVKS);
+    cudaError_t e = launch_privks_tc(tlwe2, units, D.pks[func], map, out, s->ws.iks_pks, D.err_cb,
+                                     s->st, &launches);
+    prof_end(s->st, pr);
+    g_launches.fetch_add(launches);
+    if (e != cudaSuccess) return fail(CUFHE_ERR_CUDA, "private key switching: %s", cudaGetErrorString(e));
     return CUFHE_OK;
 }
 
@@ -1397,8 +1432,7 @@ int cufhe_private_keyswitch(const uint64_t* tlwe2, size_t count, int func, uint3
     PksMap map = {};
     map.per = (int)count;
     map.stride_lo = CUFHE_TRLWE1_WORDS;
-    LAUNCH(CUFHE_K_PRIVKS, s->st, launch_privks(tlwe2, (int)count, D.pks[func], map, trlwe_out, s->st));
-    return CUFHE_OK;
+    return run_privks(s, tlwe2, (int)count, func, map, trlwe_out);
 }
 
 int cufhe_circuit_bootstrap(const uint32_t* tlwe0, size_t count, uint32_t* trgsw_out,
@@ -1426,10 +1460,11 @@ int cufhe_circuit_bootstrap(const uint32_t* tlwe0, size_t count, uint32_t* trgsw
         rc = run_br2(s, tlwe0, (int)count, mu, -1, nullptr, t2 + (size_t)i * count * CUFHE_TLWE2_WORDS);
         if (rc) return rc;
     }
-    for (int f = 0; f < 2; f++)
-        LAUNCH(CUFHE_K_PRIVKS, s->st,
-               launch_privks(t2, (int)(3 * count), D.pks[f], map,
-                             trgsw_out + (size_t)f * kL * CUFHE_TRLWE1_WORDS, s->st));
+    for (int f = 0; f < 2; f++) {
+        rc = run_privks(s, t2, (int)(3 * count), f, map,
+                        trgsw_out + (size_t)f * kL * CUFHE_TRLWE1_WORDS);
+        if (rc) return rc;
+    }
     return CUFHE_OK;
 }
 

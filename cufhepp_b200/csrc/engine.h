@@ -252,8 +252,13 @@ struct PksMap {
     size_t stride_lo, stride_hi;
     uint64_t badd[4];
 };
-cudaError_t launch_privks(const uint64_t* tlwe, int units, const uint32_t* key, const PksMap& map,
-                          uint32_t* out, cudaStream_t st);
+// on the tensor cores (iks_tc.cu): key tiles built once from the raw key
+// [2049][10][15][2][1024]; the workspace holds the per-call one-hot tiles
+size_t privks_tc_key_bytes();
+cudaError_t privks_tc_key_build(const uint32_t* key_dev, uint8_t* key_tiles, cudaStream_t st);
+cudaError_t launch_privks_tc(const uint64_t* tlwe, int units, const uint8_t* key_tiles,
+                             const PksMap& map, uint32_t* out, IksWorkspace& w, int* err,
+                             cudaStream_t st, int* launches);
 
 // Batched CMUX: CMUX c = (g, m) with g = c / per, m = c % per reads d0/d1 at
 // node g * node_stride_g + m * node_stride_m (TRLWE units), the Fourier TRGSW at

@@ -60,12 +60,14 @@ __host__ __device__ constexpr uint64_t iks20_offset_tc()
     return off + (1ull << (64 - (1 + CUFHE_LVL20_BASEBIT * CUFHE_LVL20_T)));
 }
 
-// key tiles [nt][kc][32 KB]: row = o_local * 4 + c, K-major, 128B-swizzled
-template <int CH>
+// key tiles [nt][kc][32 KB]: row = o_local * 4 + c, K-major, 128B-swizzled.
+// Key row k (k < KTOT) has OUTW words; rows k >= KTOT and columns o >= OUTW
+// are zero.
+template <int CH, int NT, int OUTW, int KTOT>
 __global__ void k_iks_key(const uint32_t* __restrict__ ksk, uint8_t* __restrict__ out)
 {
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t total = (size_t)kNTiles * CH * kBTile / 4;
+    const size_t total = (size_t)NT * CH * kBTile / 4;
     if (q >= total) return;
     const size_t byte = q * 4;
     const int tile = (int)(byte / kBTile);
@@ -78,7 +80,7 @@ __global__ void k_iks_key(const uint32_t* __restrict__ ksk, uint8_t* __restrict_
     uint32_t packed = 0;
     for (int e = 0; e < 4; e++) {
         const size_t k = (size_t)kc * kChunkK + kl + e;
-        const int8_t v = o < kTlwe0 ? limb(ksk[k * kTlwe0 + o], c) : (int8_t)0;
+        const int8_t v = (o < OUTW && k < (size_t)KTOT) ? limb(ksk[k * OUTW + o], c) : (int8_t)0;
         packed |= (uint32_t)(uint8_t)v << (8 * e);
     }
     reinterpret_cast<uint32_t*>(out)[q] = packed;
@@ -209,13 +211,67 @@ __global__ void __launch_bounds__(256) k_iks20_prep(Plan plan, const uint64_t* _
     }
 }
 
-template <int CH>
+// ---- private key switching TLWE<lvl2> -> TRLWE<lvl1> as a one-hot GEMM:
+// K = (i, j, u) = 2049 x 10 x 15 (i: input word, j: 4-bit digit level, u:
+// digit value - 1), A[unit][k] = -1 where digit j of word i of the unit is
+// u + 1, B[k][(o, c)] = limb c of key row k, word o (2048 words); each
+// digit selects one row, so |sum| <= 20490 x 128 fits INT32 exactly.
+constexpr int kPksT = 10;
+constexpr int kPksNu = 15;
+constexpr int kPksK = (CUFHE_LVL2_N + 1) * kPksT * kPksNu;           // 307,350
+constexpr int kPksChunks = (kPksK + kChunkK - 1) / kChunkK;          // 2402
+constexpr int kPksWordsOut = 2 * CUFHE_LVL1_N;                       // 2048
+constexpr int kPksNTiles = kPksWordsOut / kOutPerTile;               // 32
+
+__global__ void __launch_bounds__(256) k_pks_prep(const uint64_t* __restrict__ tlwe, int units,
+                                                  PksMap map, uint8_t* __restrict__ atiles)
+{
+    const int u = blockIdx.x;
+    if (u >= units) return;
+    const uint64_t* t = tlwe + (size_t)u * (CUFHE_LVL2_N + 1);
+    const uint64_t badd = map.badd[u / map.per];
+    constexpr uint64_t kOff = 1ull << (64 - (1 + 4 * kPksT));
+    const uint32_t row = (uint32_t)(u % kMGates);
+    uint8_t* tb = atiles + (size_t)(u / kMGates) * kPksChunks * kATile;
+    for (int q = threadIdx.x; q < kPksChunks * kChunkK / 16; q += blockDim.x) {
+        uint32_t wv[4] = {0, 0, 0, 0};
+        int ci = -1;
+        uint64_t ab = 0;
+#pragma unroll
+        for (int e = 0; e < 16; e++) {
+            const int k = 16 * q + e;
+            if (k >= kPksK) break;
+            const int c = k / (kPksT * kPksNu), rem = k % (kPksT * kPksNu);
+            const int j = rem / kPksNu, uu = rem % kPksNu;
+            if (c != ci) {
+                ci = c;
+                ab = t[c] + (c == CUFHE_LVL2_N ? badd : 0ull) + kOff;
+            }
+            const uint32_t d = (uint32_t)(ab >> (60 - 4 * j)) & 15u;
+            if (d == (uint32_t)uu + 1) wv[e >> 2] |= 0xFFu << (8 * (e & 3));
+        }
+        const int k0 = 16 * q;
+        *reinterpret_cast<uint4*>(tb + (size_t)(k0 / kChunkK) * kATile +
+                                  swz_offset(row, (uint32_t)(k0 % kChunkK))) =
+            make_uint4(wv[0], wv[1], wv[2], wv[3]);
+    }
+}
+
+// Output rows of the one-hot GEMM: unit u writes OUTW words at
+// dst + (idx ? idx[u] : u % per) * stride_lo + (u / per) * stride_hi.
+struct OutMap {
+    const int32_t* idx;
+    int per;
+    size_t stride_lo, stride_hi;
+};
+
+// xb (optional) is added to output word OUTW - 1; valid (optional) masks units.
+template <int CH, int NT, int OUTW>
 __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__ atiles,
                                                      const uint8_t* __restrict__ btiles,
                                                      const uint32_t* __restrict__ xb,
                                                      const int* __restrict__ valid, int units,
-                                                     uint32_t* __restrict__ dst,
-                                                     const int32_t* __restrict__ dst_idx,
+                                                     uint32_t* __restrict__ dst, OutMap om,
                                                      int* __restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -227,7 +283,7 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
     __shared__ int s_fail;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int gt = blockIdx.x / kNTiles, nt = blockIdx.x % kNTiles;
+    const int gt = blockIdx.x / NT, nt = blockIdx.x % NT;
     const uint8_t* ga = atiles + (size_t)gt * CH * kATile;
     const uint8_t* gb = btiles + (size_t)nt * CH * kBTile;
     int pend[kStages] = {0, 0, 0, 0};  // thread 0: 1 + parity of an outstanding fill
@@ -300,8 +356,11 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
     tc_fence_after();
     if (!s_fail) {
         const int u = gt * kMGates + warp * 32 + lane;  // this thread's TMEM lane = gate row
-        const bool live = u < units && valid[u];
-        const size_t row = live ? (dst_idx ? (size_t)dst_idx[u] : (size_t)u) : 0;
+        const bool live = u < units && (!valid || valid[u]);
+        uint32_t* rowp = dst;
+        if (live)
+            rowp += (om.idx ? (size_t)om.idx[u] : (size_t)(u % om.per)) * om.stride_lo +
+                    (size_t)(u / om.per) * om.stride_hi;
         const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
 #pragma unroll 1
         for (int cc = 0; cc < kNCols / 32; cc++) {
@@ -314,8 +373,8 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
                     const int o = nt * kOutPerTile + cc * 8 + oo;
                     uint32_t r = v[4 * oo] + (v[4 * oo + 1] << 8) + (v[4 * oo + 2] << 16) +
                                  (v[4 * oo + 3] << 24);
-                    if (o == kN0) r += xb[u];
-                    if (o < kTlwe0) dst[row * kTlwe0 + o] = r;
+                    if (xb && o == OUTW - 1) r += xb[u];
+                    if (o < OUTW) rowp[o] = r;
                 }
             }
         }
@@ -335,15 +394,17 @@ size_t iks20_tc_key_bytes() { return (size_t)kNTiles * iks_chunks<CUFHE_LVL2_N>(
 cudaError_t iks_tc_key_build(const uint32_t* ksk_dev, uint8_t* key_tiles, cudaStream_t st)
 {
     const size_t units = iks_tc_key_bytes() / 4;
-    k_iks_key<kChunks><<<(unsigned)((units + 255) / 256), 256, 0, st>>>(ksk_dev, key_tiles);
+    k_iks_key<kChunks, kNTiles, kTlwe0, kChunks * kChunkK>
+        <<<(unsigned)((units + 255) / 256), 256, 0, st>>>(ksk_dev, key_tiles);
     return cudaGetLastError();
 }
 
 cudaError_t iks20_tc_key_build(const uint32_t* ksk_dev, uint8_t* key_tiles, cudaStream_t st)
 {
     const size_t units = iks20_tc_key_bytes() / 4;
-    k_iks_key<iks_chunks<CUFHE_LVL2_N>()><<<(unsigned)((units + 255) / 256), 256, 0, st>>>(
-        ksk_dev, key_tiles);
+    constexpr int kCh2 = iks_chunks<CUFHE_LVL2_N>();
+    k_iks_key<kCh2, kNTiles, kTlwe0, kCh2 * kChunkK>
+        <<<(unsigned)((units + 255) / 256), 256, 0, st>>>(ksk_dev, key_tiles);
     return cudaGetLastError();
 }
 
@@ -375,14 +436,15 @@ void iks_tc_workspace_free(IksWorkspace& w)
     w = IksWorkspace();
 }
 
-template <int CH>
+template <int CH, int NT, int OUTW>
 static cudaError_t gemm_attr()
 {
     int dev = 0;
     cudaGetDevice(&dev);
     static bool attr[64] = {};
     if (!attr[dev & 63]) {
-        cudaError_t e = cudaFuncSetAttribute(k_iks_gemm<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_iks_gemm<CH, NT, OUTW>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)kSmem);
         if (e != cudaSuccess) return e;
         attr[dev & 63] = true;
@@ -399,12 +461,13 @@ cudaError_t launch_iks_tc(int mode, const Plan& plan, const uint32_t* in0, const
     const int units = mode == 0 ? plan.lanes : plan.count;
     if (units <= 0) return cudaSuccess;
     cudaError_t e = iks_tc_workspace(w, units, kChunks);
-    if (e == cudaSuccess) e = gemm_attr<kChunks>();
+    if (e == cudaSuccess) e = gemm_attr<kChunks, kNTiles, kTlwe0>();
     if (e != cudaSuccess) return e;
     k_iks_prep<<<units, 256, 0, st>>>(mode, plan, in0, in1, in2, lane_out, w.atiles, w.xb, w.valid);
     const int gtiles = (units + kMGates - 1) / kMGates;
-    k_iks_gemm<kChunks><<<gtiles * kNTiles, 128, kSmem, st>>>(
-        w.atiles, key_tiles, w.xb, w.valid, units, dst, mode == 1 ? plan.out_idx : nullptr, err);
+    const OutMap om = {mode == 1 ? plan.out_idx : nullptr, 0x7fffffff, (size_t)kTlwe0, 0};
+    k_iks_gemm<kChunks, kNTiles, kTlwe0>
+        <<<gtiles * kNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, w.xb, w.valid, units, dst, om, err);
     *launches = 2;
     return cudaGetLastError();
 }
@@ -418,12 +481,42 @@ cudaError_t launch_iks20_tc(const Plan& plan, const uint64_t* lane_out, const ui
     const int units = plan.count;
     if (units <= 0) return cudaSuccess;
     cudaError_t e = iks_tc_workspace(w, units, kCh);
-    if (e == cudaSuccess) e = gemm_attr<kCh>();
+    if (e == cudaSuccess) e = gemm_attr<kCh, kNTiles, kTlwe0>();
     if (e != cudaSuccess) return e;
     k_iks20_prep<<<units, 256, 0, st>>>(plan, lane_out, w.atiles, w.xb, w.valid);
     const int gtiles = (units + kMGates - 1) / kMGates;
-    k_iks_gemm<kCh><<<gtiles * kNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, w.xb, w.valid,
-                                                          units, dst, plan.out_idx, err);
+    const OutMap om = {plan.out_idx, 0x7fffffff, (size_t)kTlwe0, 0};
+    k_iks_gemm<kCh, kNTiles, kTlwe0>
+        <<<gtiles * kNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, w.xb, w.valid, units, dst, om, err);
+    *launches = 2;
+    return cudaGetLastError();
+}
+
+size_t privks_tc_key_bytes() { return (size_t)kPksNTiles * kPksChunks * kBTile; }
+
+cudaError_t privks_tc_key_build(const uint32_t* key_dev, uint8_t* key_tiles, cudaStream_t st)
+{
+    const size_t units = privks_tc_key_bytes() / 4;
+    k_iks_key<kPksChunks, kPksNTiles, kPksWordsOut, kPksK>
+        <<<(unsigned)((units + 255) / 256), 256, 0, st>>>(key_dev, key_tiles);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_privks_tc(const uint64_t* tlwe, int units, const uint8_t* key_tiles,
+                             const PksMap& map, uint32_t* out, IksWorkspace& w, int* err,
+                             cudaStream_t st, int* launches)
+{
+    *launches = 0;
+    if (units <= 0) return cudaSuccess;
+    cudaError_t e = iks_tc_workspace(w, units, kPksChunks);
+    if (e == cudaSuccess) e = gemm_attr<kPksChunks, kPksNTiles, kPksWordsOut>();
+    if (e != cudaSuccess) return e;
+    k_pks_prep<<<units, 256, 0, st>>>(tlwe, units, map, w.atiles);
+    const int gtiles = (units + kMGates - 1) / kMGates;
+    const OutMap om = {nullptr, map.per, map.stride_lo, map.stride_hi};
+    k_iks_gemm<kPksChunks, kPksNTiles, kPksWordsOut>
+        <<<gtiles * kPksNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, nullptr, nullptr, units, out,
+                                                  om, err);
     *launches = 2;
     return cudaGetLastError();
 }
