@@ -514,14 +514,14 @@ int check_device_error(int d)
 
 // private key switching lvl2 -> lvl1 on the tensor cores
 int run_privks(cufhe_stream_s* s, const uint64_t* tlwe2, int units, int func, const PksMap& map,
-               uint32_t* out)
+               uint32_t* out, bool prep = true)
 {
     DeviceState& D = g_dev[s->device];
     int launches = 0;
     ProfRec pr;
     prof_begin(s->st, pr, CUFHE_K_PRIVKS);
     cudaError_t e = launch_privks_tc(tlwe2, units, D.pks[func], map, out, s->ws.iks_pks, D.err_cb,
-                                     s->st, &launches);
+                                     s->st, &launches, prep);
     prof_end(s->st, pr);
     g_launches.fetch_add(launches);
     if (e != cudaSuccess) return fail(CUFHE_ERR_CUDA, "private key switching: %s", cudaGetErrorString(e));
@@ -1462,7 +1462,7 @@ int cufhe_circuit_bootstrap(const uint32_t* tlwe0, size_t count, uint32_t* trgsw
     }
     for (int f = 0; f < 2; f++) {
         rc = run_privks(s, t2, (int)(3 * count), f, map,
-                        trgsw_out + (size_t)f * kL * CUFHE_TRLWE1_WORDS);
+                        trgsw_out + (size_t)f * kL * CUFHE_TRLWE1_WORDS, f == 0);
         if (rc) return rc;
     }
     return CUFHE_OK;

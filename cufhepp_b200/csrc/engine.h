@@ -253,12 +253,14 @@ struct PksMap {
     uint64_t badd[4];
 };
 // on the tensor cores (iks_tc.cu): key tiles built once from the raw key
-// [2049][10][15][2][1024]; the workspace holds the per-call one-hot tiles
+// [2049][10][15][2][1024]; the workspace holds the per-call one-hot tiles,
+// which depend on the inputs only: prep = false reuses those of the previous
+// call on the same inputs (the second key function of circuit bootstrapping)
 size_t privks_tc_key_bytes();
 cudaError_t privks_tc_key_build(const uint32_t* key_dev, uint8_t* key_tiles, cudaStream_t st);
 cudaError_t launch_privks_tc(const uint64_t* tlwe, int units, const uint8_t* key_tiles,
                              const PksMap& map, uint32_t* out, IksWorkspace& w, int* err,
-                             cudaStream_t st, int* launches);
+                             cudaStream_t st, int* launches, bool prep = true);
 
 // Batched CMUX: CMUX c = (g, m) with g = c / per, m = c % per reads d0/d1 at
 // node g * node_stride_g + m * node_stride_m (TRLWE units), the Fourier TRGSW at

@@ -504,20 +504,20 @@ cudaError_t privks_tc_key_build(const uint32_t* key_dev, uint8_t* key_tiles, cud
 
 cudaError_t launch_privks_tc(const uint64_t* tlwe, int units, const uint8_t* key_tiles,
                              const PksMap& map, uint32_t* out, IksWorkspace& w, int* err,
-                             cudaStream_t st, int* launches)
+                             cudaStream_t st, int* launches, bool prep)
 {
     *launches = 0;
     if (units <= 0) return cudaSuccess;
     cudaError_t e = iks_tc_workspace(w, units, kPksChunks);
     if (e == cudaSuccess) e = gemm_attr<kPksChunks, kPksNTiles, kPksWordsOut>();
     if (e != cudaSuccess) return e;
-    k_pks_prep<<<units, 256, 0, st>>>(tlwe, units, map, w.atiles);
+    if (prep) k_pks_prep<<<units, 256, 0, st>>>(tlwe, units, map, w.atiles);
     const int gtiles = (units + kMGates - 1) / kMGates;
     const OutMap om = {nullptr, map.per, map.stride_lo, map.stride_hi};
     k_iks_gemm<kPksChunks, kPksNTiles, kPksWordsOut>
         <<<gtiles * kPksNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, nullptr, nullptr, units, out,
                                                   om, err);
-    *launches = 2;
+    *launches = prep ? 2 : 1;
     return cudaGetLastError();
 }
 

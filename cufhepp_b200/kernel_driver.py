@@ -6,6 +6,7 @@
     python -m cufhepp_b200.kernel_driver gates LANES [REPS]     # full mixed-gate batch (lvl1)
     python -m cufhepp_b200.kernel_driver br2_fp64 LANES [REPS] [STEPS]  # lvl0 -> lvl2 rotation
     python -m cufhepp_b200.kernel_driver gates02 LANES [REPS]   # mixed *_lvl02 gate batch
+    python -m cufhepp_b200.kernel_driver cb BITS [REPS]   # circuit bootstrapping + BITS/8 lookup tables
 
 Each stage is launched REPS times on LANES inputs, so a capture can skip the
 first (cold) launch.  Prints one line (with the wall time of the last REPS-1
@@ -26,8 +27,12 @@ def main(argv: list[str]) -> None:
     lanes = int(argv[1])
     reps = int(argv[2]) if len(argv) > 2 else 2
     sk = client.SecretKey.generate(5)
-    lvl02 = stage in ("br2_fp64", "gates02")
-    if lvl02:
+    lvl02 = stage in ("br2_fp64", "gates02", "cb")
+    if stage == "cb":
+        cbk = client.CBKey.generate(sk)
+        engine.initialize_lvl02(cbk.ek02)
+        engine.initialize_cb(cbk)
+    elif lvl02:
         engine.initialize_lvl02(client.EvalKey02.generate(sk, keybundle=True))
     else:
         engine.initialize(client.EvalKey.generate(sk, keybundle=(stage != "br_int8")))
@@ -41,7 +46,20 @@ def main(argv: list[str]) -> None:
             engine.synchronize()
             t0 = time.perf_counter()
 
-    if stage == "br2_fp64":
+    if stage == "cb":
+        q = max(1, lanes // 8)
+        luts = rng.integers(0, 256, (q, 256)).astype(np.uint8)
+        d_x = engine.to_device(client.encrypt_bits(sk, rng.integers(0, 2, 8 * q).astype(np.uint8),
+                                                   0, seed=3))
+        d_t = engine.DeviceBuffer(8 * q * 6 * P.TRLWE1_WORDS * 4)
+        d_f = engine.DeviceBuffer(8 * q * 6 * 2 * 512 * 16)
+        d_o = engine.DeviceBuffer(q * 8 * P.TLWE1_WORDS * 4)
+        for i in range(reps):
+            engine.circuit_bootstrap(d_x, 8 * q, d_t)
+            engine.trgsw_to_fft(engine.GADGET_CB, d_t, 8 * q, d_f)
+            engine.lut_eval(luts, d_f, P.MU32, d_o)
+            tick(i)
+    elif stage == "br2_fp64":
         steps = int(argv[3]) if len(argv) > 3 else -1
         d_in = engine.to_device(client.encrypt_bits(sk, bits, 0, seed=3))
         d_out = engine.DeviceBuffer(lanes * P.TLWE2_WORDS * 8)
@@ -79,6 +97,8 @@ def main(argv: list[str]) -> None:
         raise SystemExit(f"unknown stage {stage}")
     engine.synchronize()
     ms = (time.perf_counter() - t0) * 1e3 / (reps - 1) if (t0 is not None and reps > 1) else 0.0
+    if stage == "cb":
+        engine.cleanup_cb()
     engine.cleanup_lvl02() if lvl02 else engine.cleanup()
     print(f"ok {stage} lanes={lanes} reps={reps} wall_ms_per_rep={ms:.3f}")
 
