@@ -79,20 +79,23 @@ def main(argv: list[str]) -> None:
         x = client.encrypt_bits(sk, bits, 0, seed=3)
         d_in = engine.to_device(x)
         d_out = engine.DeviceBuffer(lanes * P.TLWE1_WORDS * 4)
-        for _ in range(reps):
+        for i in range(reps):
             engine.blind_rotate(d_in, lanes, P.MU32, steps, tlwe_out=d_out)
+            tick(i)
     elif stage == "iks":
         x = client.encrypt_bits(sk, bits, 1, seed=3)
         d_in = engine.to_device(x)
         d_out = engine.DeviceBuffer(lanes * P.TLWE0_WORDS * 4)
-        for _ in range(reps):
+        for i in range(reps):
             engine.identity_keyswitch(d_in, lanes, d_out)
+            tick(i)
     elif stage == "gates":
         gates = rng.choice([P.NAND, P.AND, P.OR, P.XOR, P.XNOR, P.MUX], size=lanes).astype(np.int32)
         cts = [engine.to_device(client.encrypt_bits(sk, bits, 1, seed=3 + i)) for i in range(3)]
         d_out = engine.DeviceBuffer(lanes * P.TLWE1_WORDS * 4)
-        for _ in range(reps):
+        for i in range(reps):
             engine.gate_batch(gates, lanes, 1, d_out, *cts)
+            tick(i)
     else:
         raise SystemExit(f"unknown stage {stage}")
     engine.synchronize()
