@@ -676,17 +676,21 @@ def run_ours(args):
         ek = client.EvalKey.generate(sk, keybundle=(p == "fp64"))
         results[p] = run_path(args, p, torch, engine, client, P, sk, ek, workload, rank, ws, flush)
     primary = results[paths[0]]
+    # the sub-workloads (uneven circuits, circuit bootstrapping, lvl02) are
+    # measured by a single process (N = 1); under torchrun every rank runs the
+    # headline batch only
+    single = ws == 1
     uneven = None
-    if not args.no_uneven:
+    if not args.no_uneven and single:
         ek_u = client.EvalKey.generate(sk, keybundle=True)
         uneven = run_uneven(args, torch, engine, client, P, sk, ek_u, rank, ws, flush,
                             results["fp64"]["value"] if "fp64" in results else None)
     cb = None
-    if not args.no_cb:
+    if not args.no_cb and single:
         cb = run_cb(args, torch, engine, client, P, sk, client.EvalKey.generate(sk, keybundle=True),
                     rank, ws, flush, workload)
     lvl02 = None
-    if not args.no_lvl02:
+    if not args.no_lvl02 and single:
         lvl02 = run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -722,6 +726,8 @@ def run_ours(args):
             line["uneven"] = uneven
         if cb is not None:
             line["cb_lut"] = cb
+        if not single:
+            line["sub_workloads"] = "measured at N = 1 only (uneven, cb_lut, lvl02)"
         line["config"]["br_lanes_per_cta"] = (
             {"source": "autotuner (cufhe_autotune)", "table": tuned} if tuned
             else {"source": "built-in rule"})
