@@ -14,6 +14,9 @@ C-ABI.  A MUX needs two blind rotations, so the unit is bootstraps/s
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W]
                        [--path fp64|int8|both] [--impl ours|reference]
+The default measures both precision forms on the same batch (FP64 FFNT is the
+headline `value`; each form's numbers are under `paths`), then the
+sub-workloads (uneven circuits, circuit bootstrapping + lookup tables, lvl02).
 Under torchrun each rank runs its own batch on its own GPU (weak scaling, no
 data-path collective: gates are independent).
 """
@@ -57,7 +60,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=4096)
-    ap.add_argument("--path", choices=["fp64", "int8", "both"], default="fp64")
+    ap.add_argument("--path", choices=["fp64", "int8", "both"], default="both")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
