@@ -366,13 +366,15 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
                                  "(cufhe_measure_fp64_peak; the peaks file has no FP64 figure)"}
         else:
             work = OPS_INT8[False] * nb
-            peak = int8_peak(torch)
+            peak = engine_peak_int8(engine)
             rl = {"bound": "tensor", "achieved": work / per_launch_s / 1e12, "peak": peak,
                   "unit": "TOP/s", "frac": work / per_launch_s / 1e12 / peak,
                   "traffic": ncu_traffic("br_int8"),
                   "kernel": "INT8 blind rotation (decompose + tcgen05 Toeplitz GEMM per step)",
                   "work_per_launch": work,
-                  "peak_source": "measured torch._int_mm int8 GEMM 8192^3 on this GPU"}
+                  "peak_source": "measured tcgen05.mma.kind::i8 M128 N256 K32 probe on this GPU "
+                                 "(cufhe_measure_int8_peak, random operands; the peaks file has "
+                                 "no INT8 figure)"}
     res = {
         "value": value, "ms_per_step": total_ms / args.steps,
         "p50_gate_latency_ms": statistics.median(step_ms),
@@ -634,22 +636,9 @@ def engine_peak_fp64(engine):
     return _PEAK["fp64"]
 
 
-def int8_peak(torch):
+def engine_peak_int8(engine):
     if "int8" not in _PEAK:
-        a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda")
-        b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device="cuda").t()
-        for _ in range(2):
-            torch._int_mm(a, b)
-        torch.cuda.synchronize()
-        best = 1e30
-        for _ in range(5):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            torch._int_mm(a, b)
-            e1.record()
-            torch.cuda.synchronize()
-            best = min(best, e0.elapsed_time(e1))
-        _PEAK["int8"] = 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+        _PEAK["int8"] = max(engine.measure_int8_peak() for _ in range(3))
     return _PEAK["int8"]
 
 

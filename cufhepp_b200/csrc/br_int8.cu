@@ -27,14 +27,15 @@
 //           cp.async.bulk (one contiguous copy per chunk).
 //  * acc  : [lanes][2][1024] Torus32.
 //
-// k_i8_gemm: CTA = (256-lane group, 128 output rows = 4 limbs x 32
-// coefficients of one j_out), warp-specialised: two generator warpgroups
-// write the Toeplitz A tiles of alternate K chunks straight into TMEM
-// (tcgen05.st; thread = row, one TMEM stage per warpgroup), one thread issues
-// 4 tcgen05.mma.kind::i8 (M=128, N=256, K=32) per chunk into the INT32
-// accumulator in TMEM, one thread streams the digit tiles through a 4-stage
-// shared-memory ring; hand-offs go through mbarriers only.  Every mbarrier wait is bounded and reports a timeout
-// through an error flag instead of hanging.
+// k_i8_gemm_p (one launch per step, one CTA per SM): tile = (256-lane group,
+// 128 output rows = 4 limbs x 32 coefficients of one j_out), warp-specialised:
+// two generator warpgroups write the Toeplitz A chunks straight into TMEM
+// (tcgen05.st; thread = row), one thread issues 4 tcgen05.mma.kind::i8
+// (M=128, N=256, K=32) per chunk into the INT32 accumulator in TMEM, two
+// threads stream the digit chunks through a 5-stage shared-memory ring, and
+// sixteen drain warps fold the limbs and add them into the global
+// accumulator.  Hand-offs go through mbarriers only; every wait is bounded
+// and reports a timeout through an error flag instead of hanging.
 #include <stdio.h>
 
 #include "br_int8.h"
@@ -50,22 +51,15 @@ constexpr int kChunkK = 128;                 // K bytes per chunk (one swizzle r
 constexpr int kChunks = 4 * kN / kChunkK;    // 32
 constexpr int kTileBytes = kGroup * kChunkK; // 32 KB
 constexpr int kRowsCoef = 32;                // coefficients per CTA tile (x4 limbs = 128 rows)
-constexpr int kMTiles = 2 * kN / kRowsCoef;  // 64 tiles per lane group
 constexpr int kVBytesStep = 2 * 4 * 4 * 2 * kN;  // 64 KB of key table per step
 constexpr int kVBytesJ = 4 * 4 * 2 * kN;         // 32 KB per output poly
-constexpr int kBStages = 4;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kAccCol = 0;      // accumulator columns [0, 256)
-constexpr uint32_t kACol = 256;      // A stages at 256 and 288 (32 columns each)
+constexpr uint32_t kACol = 256;      // A slots: 32 columns each from column 256
 
 // instruction descriptor: D s32, A s8, B s8, K-major both, N = 256, M = 128
 constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kGroup >> 3) << 17) |
                             ((uint32_t)(128 >> 4) << 24);
-
-constexpr size_t kSmemB = (size_t)kBStages * kTileBytes;  // 128 KB
-constexpr size_t kSmemV = kVBytesJ;                       // 32 KB
-constexpr size_t kSmemRed = 8 * 32 * 33 * 4;              // 33 KB (two warpgroups)
-constexpr size_t kSmemGemm = 1024 + kSmemB + kSmemV + kSmemRed + 256;
 
 // ------------------------------------------------------------ kernels ----
 
@@ -154,40 +148,78 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Warp roles: warps 0-3 and 4-7 are two generator warpgroups (chunks of even
-// / odd index, each with its own TMEM A stage), warp 8 issues the MMAs, warp
-// 9 streams digit tiles.  They hand off through mbarriers only; every wait is
-// bounded and an expired wait sets s_fail, which the other roles poll.
-constexpr int kGemmThreads = 320;
+// ---- persistent form of the step GEMM -------------------------------------
+// One CTA per SM; CTA b serves output polynomial j = b & 1 and walks that
+// polynomial's tiles t = b >> 1, + gridDim.x / 2, ... (tile = 256-lane digit
+// group x 128 rows = 4 limbs x 32 coefficients), so it keeps one 32 KB key
+// window, TMEM and the barriers for its whole life.  Each K chunk has ONE
+// full barrier (the producer's transaction bytes and the 128 A-generator
+// arrivals) and ONE empty barrier (the MMA commit): with one wait and one
+// commit per chunk the issuing thread keeps up with M128 N256 K32 MMAs.
+// Roles:
+//   warps 0-7   generators: Toeplitz A chunks into five 32-column TMEM slots
+//               (chunk g uses slot g mod 5; warpgroup g mod 2 writes it)
+//   warp 8      MMA issue: 4 x tcgen05.mma.kind::i8 M128 N256 K32 per chunk
+//   warps 9, 26 producers: the key window once (warp 9), then 32 KB digit
+//               chunks through a 5-stage ring across all tiles, even chunks
+//               from warp 9 and odd chunks from warp 26 (one issuing thread
+//               sustains about one bulk copy per 800 cycles, two keep the
+//               ring ahead of the MMAs)
+//   warps 10-25 drainers (four per TMEM lane quadrant, 64 columns each):
+//               read the accumulator, add the four limb rows into a shared
+//               [256 lanes][32 coefficients] buffer (limb q shifted by 8q),
+//               release the accumulator, then add the buffer into the global
+//               accumulator while the next tile's MMAs run
+// Every wait is bounded; an expired wait sets s_fail, which all roles poll.
+constexpr int kPStages = 5;
+constexpr size_t kSmemPB = (size_t)kPStages * kTileBytes;                // 160 KB
+constexpr size_t kSmemPV = kVBytesJ;                                      // 32 KB
+constexpr size_t kRedWords = (size_t)kGroup * kRowsCoef;                  // 8192
+constexpr size_t kSmemPRed = kRedWords * 4;                               // 32 KB
+constexpr size_t kSmemGemmP = 1024 + kSmemPB + kSmemPV + kSmemPRed + 512;
+constexpr int kDrainWarps = 16;
+constexpr int kGemmPThreads = 32 * (11 + kDrainWarps);                    // 864
 
-__global__ void __launch_bounds__(kGemmThreads, 1) k_i8_gemm(const int8_t* __restrict__ vkey,
-                                                             const uint8_t* __restrict__ tiles,
-                                                             uint32_t* __restrict__ acc, int lanes,
-                                                             int* __restrict__ err)
+// 32 lanes x 16 columns x 32 bit
+__device__ __forceinline__ void tmem_st16(uint32_t addr, const uint32_t (&v)[16])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15, %16};"
+        ::"r"(addr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),
+          "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]),
+          "r"(v[14]), "r"(v[15])
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __restrict__ vkey,
+                                                                const uint8_t* __restrict__ tiles,
+                                                                uint32_t* __restrict__ acc,
+                                                                int lanes, int tiles_j,
+                                                                int* __restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t raw_addr = smem_u32(smem_raw);
     unsigned char* smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
-    unsigned char* bst = smem;                                   // kBStages x 32 KB
-    int8_t* vs = reinterpret_cast<int8_t*>(smem + kSmemB);       // 32 KB
-    uint32_t* red = reinterpret_cast<uint32_t*>(smem + kSmemB + kSmemV);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kSmemB + kSmemV + kSmemRed);
-    uint64_t* b_full = bars;                    // [kBStages]
-    uint64_t* b_empty = bars + kBStages;        // [kBStages]
-    uint64_t* a_full = bars + 2 * kBStages;     // [2]
-    uint64_t* a_empty = a_full + 2;             // [2]
-    uint64_t* bar_v = a_empty + 2;
-    uint64_t* acc_full = bar_v + 1;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 1);
+    unsigned char* bst = smem;
+    int8_t* vs = reinterpret_cast<int8_t*>(smem + kSmemPB);
+    uint32_t* red = reinterpret_cast<uint32_t*>(smem + kSmemPB + kSmemPV);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kSmemPB + kSmemPV + kSmemPRed);
+    uint64_t* full = bars;                    // [kPStages]
+    uint64_t* empty = full + kPStages;        // [kPStages]
+    uint64_t* acc_full = empty + kPStages;
+    uint64_t* acc_empty = acc_full + 1;
+    uint64_t* bar_v = acc_empty + 1;
+    uint64_t* red_full = bar_v + 1;
+    uint64_t* red_clear = red_full + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(red_clear + 1);
     __shared__ volatile int s_fail;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int group = blockIdx.x / kMTiles;
-    const int mt = blockIdx.x % kMTiles;
-    const int j_out = mt / (kN / kRowsCoef);
-    const int n0 = (mt % (kN / kRowsCoef)) * kRowsCoef;
-    const uint8_t* gtiles = tiles + (size_t)group * kChunks * kTileBytes;
+    const int j_out = blockIdx.x & 1, cb = blockIdx.x >> 1, ncj = gridDim.x >> 1;
+    const int T = cb < tiles_j ? (tiles_j - 1 - cb) / ncj + 1 : 0;
 
+    for (size_t i = tid; i < kRedWords; i += blockDim.x) red[i] = 0u;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      ::"r"(smem_u32(tmem_slot)), "r"(kTmemCols));
@@ -195,16 +227,15 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_i8_gemm(const int8_t* __res
     }
     if (tid == 0) {
         s_fail = 0;
-        for (int s = 0; s < kBStages; s++) {
-            mbar_init(&b_full[s], 1);
-            mbar_init(&b_empty[s], 1);
+        for (int s = 0; s < kPStages; s++) {
+            mbar_init(&full[s], 128 + 1);
+            mbar_init(&empty[s], 1);
         }
-        for (int s = 0; s < 2; s++) {
-            mbar_init(&a_full[s], 128);
-            mbar_init(&a_empty[s], 1);
-        }
-        mbar_init(bar_v, 1);
         mbar_init(acc_full, 1);
+        mbar_init(acc_empty, kDrainWarps);
+        mbar_init(bar_v, 1);
+        mbar_init(red_full, kDrainWarps);
+        mbar_init(red_clear, kDrainWarps);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -212,121 +243,167 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_i8_gemm(const int8_t* __res
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 9) {
-        // ---- producer: key table once, then the digit tiles through the ring
+    if (warp == 9 || warp == 10 + kDrainWarps) {
+        // ---- producers: warp 9 even chunks, the last warp odd chunks
+        const int par = warp == 9 ? 0 : 1;
         if (lane == 0) {
-            mbar_expect_tx(bar_v, kVBytesJ);
-            bulk_g2s(vs, vkey + (size_t)j_out * kVBytesJ, kVBytesJ, bar_v);
-            for (int kc = 0; kc < kChunks && !s_fail; kc++) {
-                const int s = kc % kBStages;
-                if (kc >= kBStages && !mbar_wait(&b_empty[s], ((kc / kBStages) - 1) & 1)) {
-                    s_fail = 1;
-                    break;
+            if (par == 0) {
+                mbar_expect_tx(bar_v, (uint32_t)kSmemPV);
+                bulk_g2s(vs, vkey + (size_t)j_out * kVBytesJ, (uint32_t)kSmemPV, bar_v);
+            }
+            for (int it = 0; it < T && !s_fail; it++) {
+                const int group = (cb + it * ncj) / (kN / kRowsCoef);
+                const uint8_t* gt = tiles + (size_t)group * kChunks * kTileBytes;
+                for (int kc = par; kc < kChunks; kc += 2) {
+                    const int gc = it * kChunks + kc, s = gc % kPStages;
+                    if (s_fail) break;
+                    if (gc >= kPStages &&
+                        !mbar_wait(&empty[s], (uint32_t)((gc / kPStages) - 1) & 1)) {
+                        s_fail = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&full[s], kTileBytes);
+                    bulk_g2s(bst + s * kTileBytes, gt + (size_t)kc * kTileBytes, kTileBytes, &full[s]);
                 }
-                mbar_expect_tx(&b_full[s], kTileBytes);
-                bulk_g2s(bst + s * kTileBytes, gtiles + (size_t)kc * kTileBytes, kTileBytes,
-                         &b_full[s]);
             }
         }
     } else if (warp == 8) {
-        // ---- MMA issue: one thread
+        // ---- MMA issue
         if (lane == 0) {
-            for (int kc = 0; kc < kChunks; kc++) {
-                const int s = kc % kBStages, sa = kc & 1;
-                if (!mbar_wait(&b_full[s], (kc / kBStages) & 1) ||
-                    !mbar_wait(&a_full[sa], (kc >> 1) & 1)) {
+            int gc = 0;
+            for (int it = 0; it < T && !s_fail; it++) {
+                if (it >= 1 && !mbar_wait(acc_empty, (uint32_t)(it - 1) & 1)) {
                     s_fail = 1;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t bbase = smem_u32(bst + s * kTileBytes);
+                for (int kc = 0; kc < kChunks; kc++, gc++) {
+                    const int s = gc % kPStages;
+                    if (!mbar_wait(&full[s], (uint32_t)(gc / kPStages) & 1)) {
+                        s_fail = 1;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t bbase = smem_u32(bst + s * kTileBytes);
 #pragma unroll
-                for (int k = 0; k < kChunkK / 32; k++)
-                    tc_mma_i8(tmem + kAccCol, tmem + kACol + 32 * sa + 8 * k,
-                              desc_kmajor_sw128(bbase + 32 * k), kIdesc, (kc | k) != 0);
-                tc_commit(&b_empty[s]);
-                tc_commit(&a_empty[sa]);
+                    for (int k = 0; k < kChunkK / 32; k++)
+                        tc_mma_i8(tmem + kAccCol, tmem + kACol + 32 * s + 8 * k,
+                                  desc_kmajor_sw128(bbase + 32 * k), kIdesc, (kc | k) != 0);
+                    tc_commit(&empty[s]);
+                }
+                if (s_fail) break;
+                tc_commit(acc_full);
             }
-            tc_commit(acc_full);
         }
-    } else {
-        // ---- generators: warpgroup wg builds A for chunks kc = wg, wg + 2, ...
-        const int wg = warp >> 2, q = warp & 3;  // q: TMEM lane quarter = limb c
-        const int n = n0 + lane;
+    } else if (warp < 8) {
+        // ---- generators: warpgroup wg writes the chunks of parity wg
+        const int wg = warp >> 2, q = warp & 3;
         const uint32_t lane_base = (uint32_t)(32 * q) << 16;
-        // every branch below is taken by whole warps (votes), so the
-        // .sync.aligned tcgen05 instructions never run on a partial warp
         bool ok = __all_sync(0xffffffffu, mbar_wait(bar_v, 0));
-        for (int kc = wg; kc < kChunks && ok; kc += 2) {
-            if (__any_sync(0xffffffffu, s_fail != 0)) {
-                ok = false;
-                break;
+        for (int it = 0; it < T && ok; it++) {
+            const int n = ((cb + it * ncj) % (kN / kRowsCoef)) * kRowsCoef + lane;
+            for (int kc = wg; kc < kChunks; kc += 2) {
+                const int gc = it * kChunks + kc, s = gc % kPStages;
+                if (__any_sync(0xffffffffu, s_fail != 0)) {
+                    ok = false;
+                    break;
+                }
+                if (gc >= kPStages &&
+                    !__all_sync(0xffffffffu,
+                                mbar_wait(&empty[s], (uint32_t)((gc / kPStages) - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const int r = kc / (kN / kChunkK), m0 = (kc % (kN / kChunkK)) * kChunkK;
+                const uint32_t* vw =
+                    reinterpret_cast<const uint32_t*>(vs + (size_t)(r * 4 + q) * (2 * kN));
+                const int sst = kN - 1 - n + m0;
+                const int w0 = sst >> 2, sh = (sst & 3) * 8;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    uint32_t w[17];
+#pragma unroll
+                    for (int i = 0; i < 17; i++) w[i] = vw[w0 + 16 * h + i];
+                    uint32_t a[16];
+#pragma unroll
+                    for (int i = 0; i < 16; i++) a[i] = __funnelshift_r(w[i], w[i + 1], sh);
+                    tmem_st16(tmem + lane_base + kACol + 32 * s + 16 * h, a);
+                }
+                tmem_wait_st();
+                tc_fence_before();
+                mbar_arrive(&full[s]);
             }
-            if (kc >= 2 && !__all_sync(0xffffffffu, mbar_wait(&a_empty[wg], ((kc >> 1) - 1) & 1))) {
+        }
+        if (!ok) s_fail = 1;
+    } else {
+        // ---- drainers: warp d reads TMEM lane quadrant warp % 4 (the hardware
+        // ties a warp to quadrant warp % 4), accumulator columns [64 p, 64 p + 64)
+        const int d = warp - 10, q = warp & 3, p = d >> 2;
+        const uint32_t lane_base = (uint32_t)(32 * q) << 16;
+        bool ok = true;
+        for (int it = 0; it < T && ok; it++) {
+            const int t = cb + it * ncj;
+            const int group = t / (kN / kRowsCoef);
+            const int n0 = (t % (kN / kRowsCoef)) * kRowsCoef;
+            if (__any_sync(0xffffffffu, s_fail != 0) ||
+                !__all_sync(0xffffffffu, mbar_wait(acc_full, (uint32_t)it & 1))) {
                 ok = false;
                 break;
             }
             tc_fence_after();
-            // Toeplitz rows: A[n][m0 + k] = V_{r,j_out,c}[N - 1 - n + m0 + k]
-            const int r = kc / (kN / kChunkK), m0 = (kc % (kN / kChunkK)) * kChunkK;
-            const uint32_t* vw = reinterpret_cast<const uint32_t*>(vs + (r * 4 + q) * (2 * kN));
-            const int sst = kN - 1 - n + m0;
-            const int w0 = sst >> 2, sh = (sst & 3) * 8;
-            uint32_t w[33];
+#pragma unroll 1
+            for (int cc = 0; cc < 2; cc++) {
+                uint32_t v[32];
+                tmem_ld32(tmem + lane_base + kAccCol + 64 * p + 32 * cc, v);
+                tmem_wait_ld();
 #pragma unroll
-            for (int i = 0; i < 33; i++) w[i] = vw[w0 + i];
-            uint32_t a[32];
-#pragma unroll
-            for (int i = 0; i < 32; i++) a[i] = __funnelshift_r(w[i], w[i + 1], sh);
-            tmem_st32(tmem + lane_base + kACol + 32 * wg, a);
-            tmem_wait_st();
+                for (int i = 0; i < 32; i++)
+                    atomicAdd(&red[(size_t)(64 * p + 32 * cc + i) * kRowsCoef + lane], v[i] << (8 * q));
+            }
             tc_fence_before();
-            mbar_arrive(&a_full[wg]);
+            __threadfence_block();  // this warp's shared-buffer adds before the hand-off
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(acc_empty);
+                mbar_arrive(red_full);
+            }
+            if (!__all_sync(0xffffffffu, mbar_wait(red_full, (uint32_t)it & 1))) {
+                ok = false;
+                break;
+            }
+            // 16 rows per warp, all loads in flight before the stores
+            constexpr int kW = kGroup / kDrainWarps;
+            uint32_t old[kW];
+#pragma unroll
+            for (int i = 0; i < kW; i++) {
+                const int l = group * kGroup + d + kDrainWarps * i;
+                old[i] = l < lanes ? acc[(size_t)l * kTrlwe + j_out * kN + n0 + lane] : 0u;
+            }
+#pragma unroll
+            for (int i = 0; i < kW; i++) {
+                const int gl = d + kDrainWarps * i, l = group * kGroup + gl;
+                const uint32_t v = red[(size_t)gl * kRowsCoef + lane];
+                red[(size_t)gl * kRowsCoef + lane] = 0u;
+                if (l < lanes) acc[(size_t)l * kTrlwe + j_out * kN + n0 + lane] = old[i] + v;
+            }
+            __threadfence_block();  // the zeroed buffer before the next tile's adds
+            __syncwarp();
+            if (lane == 0) mbar_arrive(red_clear);
+            if (!__all_sync(0xffffffffu, mbar_wait(red_clear, (uint32_t)it & 1))) {
+                ok = false;
+                break;
+            }
         }
         if (!ok) s_fail = 1;
     }
 
-    // ---- epilogue (generator warps): wait for the accumulator, recombine limbs
-    const bool gen = warp < 8;
-    if (gen) {
-        const bool have_acc = __all_sync(0xffffffffu, s_fail == 0 && mbar_wait(acc_full, 0));
-        if (!have_acc) s_fail = 1;
-    }
     __syncthreads();
-    tc_fence_after();
-    if (!s_fail) {
-        // warpgroup wg reads accumulator columns [128 wg, 128 wg + 128)
-        for (int cc = 0; cc < kGroup / 64; cc++) {
-            if (gen) {
-                const int wg = warp >> 2, q = warp & 3;
-                uint32_t v[32];
-                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + kAccCol + 128 * wg + 32 * cc, v);
-                tmem_wait_ld();
-#pragma unroll
-                for (int g = 0; g < 32; g++)
-                    red[((wg * 4 + q) * 32 + lane) * 33 + g] = v[g] << (8 * q);
-            }
-            __syncthreads();
-            if (gen) {
-                const int wg = tid >> 7, t = tid & 127;
-                const int nl = t & 31, gs = t >> 5;
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const int g = gs + 4 * k;
-                    const int l = group * kGroup + 128 * wg + cc * 32 + g;
-                    const uint32_t* rb = red + (size_t)(wg * 4) * 32 * 33;
-                    const uint32_t sum = rb[(0 * 32 + nl) * 33 + g] + rb[(1 * 32 + nl) * 33 + g] +
-                                         rb[(2 * 32 + nl) * 33 + g] + rb[(3 * 32 + nl) * 33 + g];
-                    if (l < lanes) acc[(size_t)l * kTrlwe + j_out * kN + n0 + nl] += sum;
-                }
-            }
-            __syncthreads();
-        }
-    } else if (tid == 0) {
+    if (s_fail && tid == 0) {
         atomicOr(err, 1);
-        // drain: wait (bounded) for every copy and MMA batch that may be in flight
-        for (int s = 0; s < kBStages; s++) mbar_wait(&b_full[s], 0), mbar_wait(&b_full[s], 1);
-        mbar_wait(acc_full, 0);
+        // drain: wait (bounded) for copies and MMA batches that may be in flight
+        for (int s = 0; s < kPStages; s++) mbar_wait(&full[s], 0), mbar_wait(&full[s], 1);
+        mbar_wait(acc_full, 0), mbar_wait(acc_full, 1);
     }
     tc_fence_before();
     __syncthreads();
@@ -404,12 +481,13 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
     if (lanes <= 0) return cudaSuccess;
     cudaError_t e = ensure_ws(w, lanes);
     if (e != cudaSuccess) return e;
-    int dev = 0;
+    int dev = 0, sms = 148;
     cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     static bool attr[64] = {};
     if (!attr[dev & 63]) {
-        e = cudaFuncSetAttribute(k_i8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSmemGemm);
+        e = cudaFuncSetAttribute(k_i8_gemm_p, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSmemGemmP);
         if (e != cudaSuccess) return e;
         attr[dev & 63] = true;
     }
@@ -419,9 +497,12 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
     int n = 1;
     for (int i = 0; i < nsteps; i++) {
         k_i8_decompose<<<lanes, 256, 0, st>>>(w.acc, w.abar, lanes, i, (uint8_t*)w.digits);
-        k_i8_gemm<<<groups * kMTiles, kGemmThreads, kSmemGemm, st>>>(
-            (const int8_t*)k.limbs + (size_t)i * kVBytesStep, (const uint8_t*)w.digits, w.acc,
-            lanes, w.err);
+        const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * kVBytesStep;
+        // even grid: CTA b serves output polynomial b & 1
+        const int tiles_j = groups * (kN / kRowsCoef);
+        const int grid = 2 * (tiles_j < sms / 2 ? tiles_j : sms / 2);
+        k_i8_gemm_p<<<grid, kGemmPThreads, kSmemGemmP, st>>>(vk, (const uint8_t*)w.digits, w.acc,
+                                                            lanes, tiles_j, w.err);
         n += 2;
     }
     k_i8_extract<<<lanes, 256, 0, st>>>(w.acc, lanes, acc_out, lane_out);

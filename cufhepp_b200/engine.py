@@ -55,6 +55,7 @@ SIGNATURES = {
     "cufhe_profile_reset": ([], _i),
     "cufhe_profile_read": ([_i, _vp, _vp], _i),
     "cufhe_measure_fp64_peak": ([_vp], _i),
+    "cufhe_measure_int8_peak": ([_vp], _i),
     "cufhe_initialize_lvl02": ([_vp], _i),
     "cufhe_cleanup_lvl02": ([], _i),
     "cufhe_blind_rotate_lvl02": ([_vp, _sz, _u64, _i, _vp, _vp, _vp], _i),
@@ -424,6 +425,13 @@ def profile_read(cls: int) -> tuple[float, int]:
 def measure_fp64_peak() -> float:
     t = C.c_double()
     check(load().cufhe_measure_fp64_peak(C.byref(t)), "measure_fp64_peak")
+    return t.value
+
+
+def measure_int8_peak() -> float:
+    """INT8 tcgen05 throughput of the current device in TOP/s."""
+    t = C.c_double()
+    check(load().cufhe_measure_int8_peak(C.byref(t)), "measure_int8_peak")
     return t.value
 
 

@@ -346,6 +346,10 @@ int cufhe_profile_read(int kernel_class, double* total_ms, uint64_t* launches);
 /* FP64 FMA throughput of the current device in TFLOP/s (roof of the FFNT
  * path; runs a short probe kernel) */
 int cufhe_measure_fp64_peak(double* tflops);
+/* INT8 tensor-core throughput of the current device in TOP/s: back-to-back
+ * tcgen05.mma.kind::i8 M128 N256 K32 with random operands on every SM (roof
+ * of the exact path's step GEMM; runs a short probe kernel) */
+int cufhe_measure_int8_peak(double* tops);
 
 const char* cufhe_last_error(void);
 /* kernels launched by this process so far (all devices) */

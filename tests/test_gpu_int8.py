@@ -54,6 +54,27 @@ def test_int8_two_lane_groups_bit_exact(ctx):
     assert np.array_equal(got, ref)
 
 
+def test_int8_many_tiles_per_cta_bit_exact(ctx):
+    """2600 lanes = 11 digit groups (the last one partial): each CTA of the
+    persistent step GEMM walks several tiles, so the accumulator hand-off, the
+    drain buffer and the chunk ring carry over between tiles.  Lanes are
+    independent, so a spread of 24 lanes is checked against the oracle."""
+    sk, ek = ctx
+    count = 2600
+    _, x = lvl0(sk, count, 77)
+    got = rotate(x, 2, count)
+    pick = np.unique(np.concatenate([np.arange(0, count, 131), [255, 256, 2559, 2560, count - 1]]))
+    ref = O.blind_rotate(x[pick], P.MU32, ek.bk, False, O.EXACT, steps=2)
+    assert np.array_equal(got[pick], ref)
+
+
+def test_int8_peak_probe():
+    """The tcgen05 INT8 throughput probe (the exact path's roofline) runs and
+    reports a B200-like figure (nominal dense INT8: 4.5 POP/s)."""
+    tops = engine.measure_int8_peak()
+    assert 1000.0 < tops < 9000.0
+
+
 def test_int8_full_rotation_bit_exact(ctx):
     sk, ek = ctx
     bits, x = lvl0(sk, 4, 8)
