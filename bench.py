@@ -51,6 +51,10 @@ OPS_INT8 = {False: 2 * 636 * 4096 * 8192}
 # 10 transforms x 5*1024*10 + twist/untwist 10*1024*6 + combine/MAC 8*2*1024*32
 FLOP_FP64_LVL2_KB = (10 * 51_200 + 61_440 + 524_288) * 318
 LVL02_BATCHES = (512, 2048, 8192)
+# exact INT8 form at lvl02: K = 8 digit rows x 2048, M = 2 polys x 2048
+# coefficients x 8 key limbs, 2 digit limbs, 636 steps (a MAC is 2 ops)
+OPS_INT8_LVL2 = 2 * 636 * (8 * 2048) * (2 * 2048 * 8) * 2
+LVL02_INT8_BATCH = 2048
 WORKLOAD = ("lvl1 mixed-gate batch: 4096 independent gates uniform over "
             "NAND/AND/OR/XOR/XNOR/MUX, Ctxt<lvl1> I/O (IKS->BR->SampleExtract), "
             "n0=636 N=1024 l=2 Bgbit=8 IKS basebit=2 t=7, Torus32")
@@ -448,6 +452,7 @@ def run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush):
     L2 flushed between steps."""
     ek = client.EvalKey02.generate(sk, keybundle=True)
     engine.initialize_lvl02(ek)
+    engine.set_precision(P.FP64_FFNT)
     rng = np.random.default_rng(args.seed + 7 + rank)
     out = {}
     kern_share = None
@@ -498,6 +503,7 @@ def run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush):
         torch.cuda.synchronize()
         lat.append(e0.elapsed_time(e1))
     engine.cleanup_lvl02()
+    int8 = run_lvl02_int8(args, torch, engine, client, P, sk, rank, ws, flush)
     big = str(LVL02_BATCHES[-1])
     br_ms = kern_share.get("br_fp64_lvl02") if kern_share else None
     rl = None
@@ -515,7 +521,79 @@ def run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush):
                          "KeyBundle, lvl20 key switch basebit=2 t=7"),
             "batches": out, "value": out[big]["value"],
             "single_gate_latency_ms": statistics.median(lat), "roofline": rl,
-            "dtype": "f64"}
+            "dtype": "f64", "int8_exact": int8}
+
+
+def run_lvl02_int8(args, torch, engine, client, P, sk, rank, ws, flush):
+    """The exact INT8 form of the lvl02 gates (plain lvl02 key, eight key limbs
+    x two digit limbs, INT32 accumulation): NAND batch of LVL02_INT8_BATCH
+    gates timed like the FP64 form (3 warm-up, events, L2 flush, bounded to
+    a few steps: a batch takes about a second), and the FP64 form's phase
+    error against it after full rotations of the same 64 inputs."""
+    ek = client.EvalKey02.generate(sk, keybundle=False)
+    engine.initialize_lvl02(ek)
+    engine.set_precision(P.INT8_EXACT)
+    rng = np.random.default_rng(args.seed + 17 + rank)
+    B = LVL02_INT8_BATCH
+    steps = min(args.steps, 3)
+    try:
+        a, b = (rng.integers(0, 2, B).astype(np.uint8) for _ in range(2))
+        cts = [client.encrypt_bits(sk, x, 0, seed=args.seed + 600 + i) for i, x in enumerate((a, b))]
+        din = [engine.to_device(x) for x in cts]
+        dout = engine.DeviceBuffer(B * P.TLWE0_WORDS * 4)
+        for _ in range(max(args.warmup, 3)):
+            engine.gate_batch(None, B, engine.LVL02, dout, *din, uniform=P.NAND)
+        torch.cuda.synchronize()
+        res = engine.from_device(dout, (B, P.TLWE0_WORDS))
+        fails = int(np.count_nonzero(client.decrypt_bits(sk, res, 0) != (1 - (a & b))))
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        engine.profile_reset()
+        engine.profile_enable(True)
+        for k in range(steps):
+            ev[k][0].record()
+            engine.gate_batch(None, B, engine.LVL02, dout, *din, uniform=P.NAND)
+            ev[k][1].record()
+            flush.zero_()
+        torch.cuda.synchronize()
+        engine.profile_enable(False)
+        br_ms, _ = engine.profile_read(engine.K_NAMES.index("br_int8_lvl02"))
+        total = max_over_ranks(torch, sum(e0.elapsed_time(e1) for e0, e1 in ev), "cuda")
+        # FP64 rounding against the exact product: phase error after a full
+        # rotation (Torus64 units; the masks diverge once a step's FP64 error
+        # exceeds the lowest digit weight, so only the phase is comparable)
+        n = 64
+        x = client.encrypt_bits(sk, a[:n], 0, seed=args.seed + 700)
+        d_x = engine.to_device(x)
+        d_acc = engine.DeviceBuffer(n * P.TRLWE2_WORDS * 8)
+        engine.blind_rotate_lvl02(d_x, n, P.MU64, -1, acc_out=d_acc)
+        exact = engine.from_device(d_acc, (n, P.TRLWE2_WORDS), np.uint64).copy()
+        engine.set_precision(P.FP64_FFNT)
+        engine.blind_rotate_lvl02(d_x, n, P.MU64, -1, acc_out=d_acc)
+        fp64 = engine.from_device(d_acc, (n, P.TRLWE2_WORDS), np.uint64)
+        err = max(float(np.abs((client.trlwe64_phase(sk, fp64[i]) -
+                                client.trlwe64_phase(sk, exact[i])).view(np.int64)
+                               .astype(np.float64)).max()) for i in range(n))
+    finally:
+        engine.set_precision(P.FP64_FFNT)
+        engine.cleanup_lvl02()
+    work = OPS_INT8_LVL2 * B
+    peak = engine_peak_int8(engine)
+    ach = work / (br_ms / steps * 1e-3) / 1e12 if br_ms else None
+    return {"batch": B, "value": whole_job_rate(B, ws, steps, total), "steps": steps,
+            "ms_per_step": total / steps, "decrypt_failures": fails,
+            "fp64_phase_error_log2_torus64": float(np.log2(max(err, 1.0))),
+            "fp64_phase_error_rotations": n,
+            "roofline": {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TOP/s",
+                         "frac": ach / peak if ach else None,
+                         "kernel": "INT8 blind rotation to lvl2 (decompose + tcgen05 Toeplitz "
+                                   "GEMM per step)",
+                         "work_per_launch": work,
+                         "peak_source": "measured tcgen05.mma.kind::i8 probe on this GPU"},
+            "dtype": "int8 products, int32 accumulation, Torus64 recombination"}
 
 
 def run_uneven(args, torch, engine, client, P, sk, ek, rank, ws, flush, ref_rate):

@@ -34,6 +34,7 @@ ENGINE_SOURCES = [
     "noalloc.cu",
     "br_fp64_lvl02.cu",
     "cb.cu",
+    "br_int8_lvl02.cu",
 ]
 
 

@@ -143,11 +143,6 @@ __global__ void __launch_bounds__(256) k_i8_decompose(const uint32_t* __restrict
     }
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 // ---- persistent form of the step GEMM -------------------------------------
 // One CTA per SM; CTA b serves output polynomial j = b & 1 and walks that
 // polynomial's tiles t = b >> 1, + gridDim.x / 2, ... (tile = 256-lane digit

@@ -20,11 +20,28 @@ struct Int8Workspace {
     int* err = nullptr;   // set by a kernel whose bounded wait gave up
 };
 
+// lvl0 -> lvl2 form (N = 2048, l = 4, Bgbit = 10, Torus64): eight key limbs,
+// two digit limbs
+struct Int8Workspace2 {
+    size_t cap = 0;       // lanes
+    uint64_t* acc = nullptr;
+    int8_t* digits = nullptr;
+    uint16_t* abar = nullptr;
+    int* err = nullptr;
+};
+
 cudaError_t int8_key_build(Int8Key& k, const uint32_t* bk_dev, cudaStream_t st);
 void int8_key_free(Int8Key& k);
 void int8_workspace_free(Int8Workspace& w);
 cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* lane_in, int lanes,
                            uint32_t mu, int steps, uint32_t* acc_out, uint32_t* lane_out,
                            cudaStream_t st, int* launches);
+
+// bk2_dev: plain (non-KeyBundle) BootstrappingKey<lvl02>, TRGSW<lvl2>[636]
+cudaError_t int8_key2_build(Int8Key& k, const uint64_t* bk2_dev, cudaStream_t st);
+void int8_workspace2_free(Int8Workspace2& w);
+cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t* lane_in, int lanes,
+                            uint64_t mu, int steps, uint64_t* acc_out, uint64_t* lane_out,
+                            cudaStream_t st, int* launches);
 
 }  // namespace cufhe

@@ -32,6 +32,7 @@ struct DeviceState {
     double2* psi = nullptr;
     double2* tw512 = nullptr;
     Int8Key i8;              // INT8 exact-path key (non-KeyBundle only)
+    Int8Key i8_2;            // INT8 exact-path lvl02 key (non-KeyBundle only)
     uint8_t* iks_key = nullptr;  // KSK as signed byte-limb tiles (tensor-core IKS)
     int* err = nullptr;          // set by a device wait that timed out
     // lvl0 -> lvl2 path (Initialize_lvl02)
@@ -61,6 +62,7 @@ struct Workspace {
     unsigned char* stage = nullptr;  // pinned host staging for plan uploads
     cudaEvent_t stage_ev = nullptr;
     Int8Workspace i8;
+    Int8Workspace2 i8_2;
     IksWorkspace iks;
     size_t lane2_cap = 0;
     uint64_t* lane_out2 = nullptr;  // lvl2 lane outputs [lanes][2049]
@@ -184,6 +186,7 @@ void free_ws(Workspace& w)
     if (w.stage) cudaFreeHost(w.stage);
     if (w.stage_ev) cudaEventDestroy(w.stage_ev);
     int8_workspace_free(w.i8);
+    int8_workspace2_free(w.i8_2);
     iks_tc_workspace_free(w.iks);
     cudaFree(w.lane_out2);
     iks_tc_workspace_free(w.iks2);
@@ -262,6 +265,7 @@ void release_device02(int d)
     cudaFree(D.psi2);
     cudaFree(D.iks2_key);
     cudaFree(D.err2);
+    int8_key_free(D.i8_2);
     D.bkf2 = D.psi2 = nullptr;
     D.iks2_key = nullptr;
     D.err2 = nullptr;
@@ -371,6 +375,14 @@ int init_device02(int d, const cufhe_keyview02* ek)
     const int npolys = (int)(ek->bk_words / CUFHE_LVL2_N);
     CK(cudaMalloc(&D.bkf2, (size_t)npolys * 1024 * sizeof(double2)));
     CKL(launch_bk2_to_fft(raw, npolys, D.psi2, D.bkf2, 0));
+    if (!ek->keybundle) {
+        cudaError_t e = int8_key2_build(D.i8_2, raw, 0);
+        if (e != cudaSuccess) {
+            cudaFree(raw);
+            cudaFree(ksk);
+            return fail(CUFHE_ERR_CUDA, "INT8 lvl02 key conversion: %s", cudaGetErrorString(e));
+        }
+    }
     CK(cudaDeviceSynchronize());
     cudaFree(raw);
     cudaFree(ksk);
@@ -547,6 +559,21 @@ int run_br2(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint64_t mu, 
             uint64_t* acc_out, uint64_t* lane_out)
 {
     DeviceState& D = g_dev[s->device];
+    if (g_precision == CUFHE_INT8_EXACT) {
+        if (D.kb2 || !D.i8_2.ready)
+            return fail(CUFHE_ERR_STATE,
+                        "INT8_EXACT at lvl02 needs a lvl02 bootstrapping key without KeyBundle");
+        int launches = 0;
+        ProfRec pr;
+        prof_begin(s->st, pr, CUFHE_K_BR_INT8_LVL02);
+        cudaError_t e = launch_br2_int8(D.i8_2, s->ws.i8_2, lane_in, lanes, mu, steps, acc_out,
+                                        lane_out, s->st, &launches);
+        prof_end(s->st, pr);
+        g_launches.fetch_add(launches);
+        if (e != cudaSuccess)
+            return fail(CUFHE_ERR_CUDA, "INT8 lvl02 blind rotation: %s", cudaGetErrorString(e));
+        return CUFHE_OK;
+    }
     LAUNCH(CUFHE_K_BR_FP64_LVL02, s->st,
            launch_br2_fp64(D.kb2 != 0, lane_in, lanes, mu, D.bkf2, D.psi2, steps, acc_out, lane_out,
                            s->st));
@@ -1361,7 +1388,7 @@ int cufhe_circuit_run(cufhe_circuit_t c, uint32_t* wires, cufhe_stream_t st, int
         return fail(CUFHE_ERR_STATE, "keys of the circuit's level are not initialised");
     CK(cudaSetDevice(c->device));
     // the INT8 form synchronises inside its launcher, so it always runs directly
-    const bool graph = use_graph && !(c->level != CUFHE_LVL02 && g_precision == CUFHE_INT8_EXACT);
+    const bool graph = use_graph && g_precision != CUFHE_INT8_EXACT;
     if (!graph) {
         c->exec.st = s->st;
         for (size_t w = 0; w < c->waves.size(); w++) {

@@ -27,6 +27,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // bounded wait for the phase with the given parity; false on timeout
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
 {

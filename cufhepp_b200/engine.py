@@ -79,7 +79,7 @@ SIGNATURES = {
 (K_IKS, K_PREADD, K_BR_FP64, K_BR_INT8, K_FINALIZE, K_BR_FP64_LVL02, K_IKS_LVL20, K_PRIVKS,
  K_CMUX) = range(9)
 K_NAMES = ["iks", "preadd", "br_fp64", "br_int8", "finalize", "br_fp64_lvl02", "iks_lvl20",
-           "privks", "cmux"]
+           "privks", "cmux", "br_int8_lvl02"]
 GADGET_LVL1, GADGET_CB = 0, 1
 
 

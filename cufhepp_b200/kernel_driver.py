@@ -5,6 +5,7 @@
     python -m cufhepp_b200.kernel_driver iks LANES [REPS]       # identity key switching
     python -m cufhepp_b200.kernel_driver gates LANES [REPS]     # full mixed-gate batch (lvl1)
     python -m cufhepp_b200.kernel_driver br2_fp64 LANES [REPS] [STEPS]  # lvl0 -> lvl2 rotation
+    python -m cufhepp_b200.kernel_driver br2_int8 LANES [REPS] [STEPS]  # the same, INT8 exact
     python -m cufhepp_b200.kernel_driver gates02 LANES [REPS]   # mixed *_lvl02 gate batch
     python -m cufhepp_b200.kernel_driver cb BITS [REPS]   # circuit bootstrapping + BITS/8 lookup tables
 
@@ -27,13 +28,13 @@ def main(argv: list[str]) -> None:
     lanes = int(argv[1])
     reps = int(argv[2]) if len(argv) > 2 else 2
     sk = client.SecretKey.generate(5)
-    lvl02 = stage in ("br2_fp64", "gates02", "cb")
+    lvl02 = stage in ("br2_fp64", "br2_int8", "gates02", "cb")
     if stage == "cb":
         cbk = client.CBKey.generate(sk)
         engine.initialize_lvl02(cbk.ek02)
         engine.initialize_cb(cbk)
     elif lvl02:
-        engine.initialize_lvl02(client.EvalKey02.generate(sk, keybundle=True))
+        engine.initialize_lvl02(client.EvalKey02.generate(sk, keybundle=(stage != "br2_int8")))
     else:
         engine.initialize(client.EvalKey.generate(sk, keybundle=(stage != "br_int8")))
     rng = np.random.default_rng(1)
@@ -59,7 +60,8 @@ def main(argv: list[str]) -> None:
             engine.trgsw_to_fft(engine.GADGET_CB, d_t, 8 * q, d_f)
             engine.lut_eval(luts, d_f, P.MU32, d_o)
             tick(i)
-    elif stage == "br2_fp64":
+    elif stage in ("br2_fp64", "br2_int8"):
+        engine.set_precision(P.FP64_FFNT if stage == "br2_fp64" else P.INT8_EXACT)
         steps = int(argv[3]) if len(argv) > 3 else -1
         d_in = engine.to_device(client.encrypt_bits(sk, bits, 0, seed=3))
         d_out = engine.DeviceBuffer(lanes * P.TLWE2_WORDS * 8)

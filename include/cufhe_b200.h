@@ -122,8 +122,10 @@ int cufhe_cleanup_lvl02(void);
 int cufhe_synchronize(void);
 
 /* Chooses the external-product form used by subsequent gate calls (the
- * reference fixes it at compile time: CMakeLists.txt:49-62).  INT8_EXACT
- * needs a bootstrapping key without KeyBundle. */
+ * reference fixes it at compile time: CMakeLists.txt:49-62), at lvl1 and at
+ * lvl02 alike.  INT8_EXACT needs a bootstrapping key without KeyBundle at
+ * the level it runs (lvl1 keys for lvl0/lvl1 gates, lvl02 keys for lvl02
+ * gates, circuit bootstrapping and cufhe_blind_rotate_lvl02). */
 int cufhe_set_precision(int form);
 int cufhe_get_precision(void);
 
@@ -339,7 +341,8 @@ int cufhe_autotune_table(int32_t* lanes, int32_t* lanes_per_cta, int cap);
 #define CUFHE_K_IKS_LVL20 6  /* key switching lvl2 -> lvl0 */
 #define CUFHE_K_PRIVKS 7     /* private key switching lvl2 -> lvl1 */
 #define CUFHE_K_CMUX 8       /* CMUX (lookup tables, cufhe_cmux) */
-#define CUFHE_K_CLASSES 9
+#define CUFHE_K_BR_INT8_LVL02 9 /* INT8 exact blind rotation to lvl2 step kernels */
+#define CUFHE_K_CLASSES 10
 int cufhe_profile_enable(int on);
 int cufhe_profile_reset(void);
 int cufhe_profile_read(int kernel_class, double* total_ms, uint64_t* launches);
