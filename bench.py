@@ -315,6 +315,18 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
             kern[name] = (ms, n)
     step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
 
+    # single-gate latency on an idle GPU (one NAND through cufhe_gate)
+    lat = []
+    L = engine.load()
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        engine.check(L.cufhe_gate(0, level, engine.dptr(dev_out), engine.dptr(dev_in[0]),
+                                  engine.dptr(dev_in[1]), None, None), "gate")
+        e1.record()
+        torch.cuda.synchronize()
+        lat.append(e0.elapsed_time(e1))
+
     # throughput: consecutive batches alternate between two engine streams
     # (each with its own workspace and output buffer), as a streaming caller
     # would, so one batch's partial last wave overlaps the next batch's first
@@ -390,17 +402,6 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
     for st in streams:
         st.destroy()
 
-    # single-gate latency on an idle GPU (one NAND through cufhe_gate)
-    lat = []
-    L = engine.load()
-    for _ in range(5):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        engine.check(L.cufhe_gate(0, level, engine.dptr(dev_out), engine.dptr(dev_in[0]),
-                                  engine.dptr(dev_in[1]), None, None), "gate")
-        e1.record()
-        torch.cuda.synchronize()
-        lat.append(e0.elapsed_time(e1))
     engine.cleanup()
 
     br = "br_fp64" if path == "fp64" else "br_int8"
