@@ -121,16 +121,24 @@ __global__ void __launch_bounds__(256) k_i8_decompose(const uint32_t* __restrict
     uint8_t* gtile = tiles + (size_t)(l / kGroup) * kChunks * kTileBytes;
     const int m = threadIdx.x * 4;
     constexpr uint32_t kOff = (128u << 24) + (128u << 16) + (1u << 15);
+    // the rotated window a[(m - ab) ..  + 4) from two aligned 16-byte loads
+    const uint32_t base = ((uint32_t)m - ab) & (kN - 1), q0 = base & ~3u, off = base & 3u;
 #pragma unroll
     for (int j = 0; j < 2; j++) {
         const uint32_t* a = acc + (size_t)l * kTrlwe + j * kN;
+        const uint4 cur = *reinterpret_cast<const uint4*>(a + m);
+        const uint4 w0 = *reinterpret_cast<const uint4*>(a + q0);
+        const uint4 w1 = *reinterpret_cast<const uint4*>(a + ((q0 + 4) & (kN - 1)));
+        const uint32_t win[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+        const uint32_t cv[4] = {cur.x, cur.y, cur.z, cur.w};
         uint32_t d0 = 0, d1 = 0;
 #pragma unroll
         for (int e = 0; e < 4; e++) {
             const uint32_t n = (uint32_t)(m + e);
-            uint32_t rv = a[(n - ab) & (kN - 1)];
+            // win[off + e] without a dynamic register index
+            uint32_t rv = off == 0 ? win[e] : off == 1 ? win[e + 1] : off == 2 ? win[e + 2] : win[e + 3];
             rv = ((n < abm) ^ abn) ? 0u - rv : rv;
-            const uint32_t t = rv - a[n] + kOff;
+            const uint32_t t = rv - cv[e] + kOff;
             d0 |= (uint32_t)(uint8_t)((int)((t >> 24) & 255u) - 128) << (8 * e);
             d1 |= (uint32_t)(uint8_t)((int)((t >> 16) & 255u) - 128) << (8 * e);
         }
