@@ -439,10 +439,20 @@ cudaError_t ensure_ws(Int8Workspace& w, int lanes)
     if ((e = cudaMalloc(&w.abar, (size_t)lanes * 640 * 2)) != cudaSuccess) return e;
     if ((e = cudaMalloc((void**)&w.digits, (size_t)groups * kChunks * kTileBytes)) != cudaSuccess) return e;
     if ((e = cudaMemset(w.digits, 0, (size_t)groups * kChunks * kTileBytes)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&w.err, sizeof(int))) != cudaSuccess) return e;
-    if ((e = cudaMemset(w.err, 0, sizeof(int))) != cudaSuccess) return e;
     w.cap = (size_t)lanes;
     return cudaSuccess;
+}
+
+cudaError_t set_gemm_attr()
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr[64] = {};
+    if (attr[dev & 63]) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(k_i8_gemm_p, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)kSmemGemmP);
+    if (e == cudaSuccess) attr[dev & 63] = true;
+    return e;
 }
 
 }  // namespace
@@ -472,28 +482,26 @@ void int8_workspace_free(Int8Workspace& w)
     cudaFree(w.acc);
     cudaFree(w.abar);
     cudaFree(w.digits);
-    cudaFree(w.err);
     w = Int8Workspace();
+}
+
+cudaError_t int8_reserve(Int8Workspace& w, int lanes)
+{
+    const cudaError_t e = ensure_ws(w, lanes);
+    return e != cudaSuccess ? e : set_gemm_attr();
 }
 
 cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* lane_in, int lanes,
                            uint32_t mu, int steps, uint32_t* acc_out, uint32_t* lane_out,
-                           cudaStream_t st, int* launches)
+                           int* err, cudaStream_t st, int* launches)
 {
     *launches = 0;
     if (lanes <= 0) return cudaSuccess;
-    cudaError_t e = ensure_ws(w, lanes);
+    cudaError_t e = int8_reserve(w, lanes);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    static bool attr[64] = {};
-    if (!attr[dev & 63]) {
-        e = cudaFuncSetAttribute(k_i8_gemm_p, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSmemGemmP);
-        if (e != cudaSuccess) return e;
-        attr[dev & 63] = true;
-    }
     const int nsteps = (steps < 0 || steps > kN0) ? kN0 : steps;
     const int groups = (lanes + kGroup - 1) / kGroup;
     k_i8_init<<<lanes, 256, 0, st>>>(lane_in, lanes, mu, w.abar, w.acc);
@@ -505,25 +513,13 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
         const int tiles_j = groups * (kN / kRowsCoef);
         const int grid = 2 * (tiles_j < sms / 2 ? tiles_j : sms / 2);
         k_i8_gemm_p<<<grid, kGemmPThreads, kSmemGemmP, st>>>(vk, (const uint8_t*)w.digits, w.acc,
-                                                            lanes, tiles_j, w.err);
+                                                            lanes, tiles_j, err);
         n += 2;
     }
     k_i8_extract<<<lanes, 256, 0, st>>>(w.acc, lanes, acc_out, lane_out);
     n++;
     *launches = n;
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    // report a device-side wait timeout (the kernels never hang: waits are bounded)
-    int herr = 0;
-    e = cudaMemcpyAsync(&herr, w.err, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return e;
-    e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return e;
-    if (herr) {
-        cudaMemsetAsync(w.err, 0, sizeof(int), st);
-        return cudaErrorLaunchTimeout;
-    }
-    return cudaSuccess;
+    return cudaGetLastError();
 }
 
 }  // namespace cufhe

@@ -17,7 +17,6 @@ struct Int8Workspace {
     uint32_t* acc = nullptr;
     int8_t* digits = nullptr;
     uint16_t* abar = nullptr;
-    int* err = nullptr;   // set by a kernel whose bounded wait gave up
 };
 
 // lvl0 -> lvl2 form (N = 2048, l = 4, Bgbit = 10, Torus64): eight key limbs,
@@ -27,21 +26,27 @@ struct Int8Workspace2 {
     uint64_t* acc = nullptr;
     int8_t* digits = nullptr;
     uint16_t* abar = nullptr;
-    int* err = nullptr;
 };
 
 cudaError_t int8_key_build(Int8Key& k, const uint32_t* bk_dev, cudaStream_t st);
 void int8_key_free(Int8Key& k);
 void int8_workspace_free(Int8Workspace& w);
+// The launchers are asynchronous (stream-ordered, capturable into a CUDA
+// graph once the workspace is reserved): a kernel whose bounded wait gives
+// up sets *err, which the caller reads at synchronisation.
+// int8_reserve*: size the workspace for `lanes` and set the kernels'
+// attributes; call before a graph capture.
+cudaError_t int8_reserve(Int8Workspace& w, int lanes);
+cudaError_t int8_reserve2(Int8Workspace2& w, int lanes);
 cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* lane_in, int lanes,
                            uint32_t mu, int steps, uint32_t* acc_out, uint32_t* lane_out,
-                           cudaStream_t st, int* launches);
+                           int* err, cudaStream_t st, int* launches);
 
 // bk2_dev: plain (non-KeyBundle) BootstrappingKey<lvl02>, TRGSW<lvl2>[636]
 cudaError_t int8_key2_build(Int8Key& k, const uint64_t* bk2_dev, cudaStream_t st);
 void int8_workspace2_free(Int8Workspace2& w);
 cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t* lane_in, int lanes,
                             uint64_t mu, int steps, uint64_t* acc_out, uint64_t* lane_out,
-                            cudaStream_t st, int* launches);
+                            int* err, cudaStream_t st, int* launches);
 
 }  // namespace cufhe

@@ -507,10 +507,20 @@ cudaError_t ensure_ws2(Int8Workspace2& w, int lanes)
     if ((e = cudaMalloc(&w.abar, (size_t)lanes * kAbarStride * 2)) != cudaSuccess) return e;
     if ((e = cudaMalloc((void**)&w.digits, dbytes)) != cudaSuccess) return e;
     if ((e = cudaMemset(w.digits, 0, dbytes)) != cudaSuccess) return e;
-    if ((e = cudaMalloc(&w.err, sizeof(int))) != cudaSuccess) return e;
-    if ((e = cudaMemset(w.err, 0, sizeof(int))) != cudaSuccess) return e;
     w.cap = (size_t)lanes;
     return cudaSuccess;
+}
+
+cudaError_t set_gemm2_attr()
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr[64] = {};
+    if (attr[dev & 63]) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(k_i82_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)kSmemGemm);
+    if (e == cudaSuccess) attr[dev & 63] = true;
+    return e;
 }
 
 }  // namespace
@@ -534,28 +544,26 @@ void int8_workspace2_free(Int8Workspace2& w)
     cudaFree(w.acc);
     cudaFree(w.abar);
     cudaFree(w.digits);
-    cudaFree(w.err);
     w = Int8Workspace2();
+}
+
+cudaError_t int8_reserve2(Int8Workspace2& w, int lanes)
+{
+    const cudaError_t e = ensure_ws2(w, lanes);
+    return e != cudaSuccess ? e : set_gemm2_attr();
 }
 
 cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t* lane_in, int lanes,
                             uint64_t mu, int steps, uint64_t* acc_out, uint64_t* lane_out,
-                            cudaStream_t st, int* launches)
+                            int* err, cudaStream_t st, int* launches)
 {
     *launches = 0;
     if (lanes <= 0) return cudaSuccess;
-    cudaError_t e = ensure_ws2(w, lanes);
+    cudaError_t e = int8_reserve2(w, lanes);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    static bool attr[64] = {};
-    if (!attr[dev & 63]) {
-        e = cudaFuncSetAttribute(k_i82_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kSmemGemm);
-        if (e != cudaSuccess) return e;
-        attr[dev & 63] = true;
-    }
     const int nsteps = (steps < 0 || steps > kN0) ? kN0 : steps;
     const int groups = (lanes + kGroup2 - 1) / kGroup2;
     // even grid: CTA b serves output polynomial b & 1
@@ -567,25 +575,13 @@ cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t*
         k_i82_decompose<<<lanes, 256, 0, st>>>(w.acc, w.abar, lanes, i, (uint8_t*)w.digits);
         const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * kVStep;
         k_i82_gemm<<<grid, kGemmThreads, kSmemGemm, st>>>(vk, (const uint8_t*)w.digits, w.acc,
-                                                         lanes, blocks_j, w.err);
+                                                         lanes, blocks_j, err);
         n += 2;
     }
     k_i82_extract<<<lanes, 256, 0, st>>>(w.acc, lanes, acc_out, lane_out);
     n++;
     *launches = n;
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    // report a device-side wait timeout (the kernels never hang: waits are bounded)
-    int herr = 0;
-    e = cudaMemcpyAsync(&herr, w.err, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return e;
-    e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return e;
-    if (herr) {
-        cudaMemsetAsync(w.err, 0, sizeof(int), st);
-        return cudaErrorLaunchTimeout;
-    }
-    return cudaSuccess;
+    return cudaGetLastError();
 }
 
 }  // namespace cufhe

@@ -567,7 +567,7 @@ int run_br2(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint64_t mu, 
         ProfRec pr;
         prof_begin(s->st, pr, CUFHE_K_BR_INT8_LVL02);
         cudaError_t e = launch_br2_int8(D.i8_2, s->ws.i8_2, lane_in, lanes, mu, steps, acc_out,
-                                        lane_out, s->st, &launches);
+                                        lane_out, D.err2, s->st, &launches);
         prof_end(s->st, pr);
         g_launches.fetch_add(launches);
         if (e != cudaSuccess)
@@ -606,7 +606,7 @@ int run_br(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint32_t mu, i
         ProfRec pr;
         prof_begin(s->st, pr, CUFHE_K_BR_INT8);
         cudaError_t e = launch_br_int8(D.i8, s->ws.i8, lane_in, lanes, mu, steps, acc_out,
-                                       lane_out, s->st, &launches);
+                                       lane_out, D.err, s->st, &launches);
         prof_end(s->st, pr);
         g_launches.fetch_add(launches);
         if (e != cudaSuccess) return fail(CUFHE_ERR_CUDA, "INT8 blind rotation: %s", cudaGetErrorString(e));
@@ -730,6 +730,13 @@ void circuit_drop_graph(cufhe_circuit_s* c)
 int circuit_capture(cufhe_circuit_s* c, uint32_t* wires)
 {
     circuit_drop_graph(c);
+    if (g_precision == CUFHE_INT8_EXACT && c->max_lanes > 0) {
+        // the INT8 workspace must not be allocated inside the capture
+        const cudaError_t e = c->level == CUFHE_LVL02 ? int8_reserve2(c->exec.ws.i8_2, c->max_lanes)
+                                                      : int8_reserve(c->exec.ws.i8, c->max_lanes);
+        if (e != cudaSuccess)
+            return fail(CUFHE_ERR_NOMEM, "INT8 workspace: %s", cudaGetErrorString(e));
+    }
     const bool prof = g_prof;
     g_prof = false;  // per-kernel event timing is not recorded inside graphs
     const uint64_t l0 = g_launches.load();
@@ -1387,8 +1394,7 @@ int cufhe_circuit_run(cufhe_circuit_t c, uint32_t* wires, cufhe_stream_t st, int
     if (c->level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
         return fail(CUFHE_ERR_STATE, "keys of the circuit's level are not initialised");
     CK(cudaSetDevice(c->device));
-    // the INT8 form synchronises inside its launcher, so it always runs directly
-    const bool graph = use_graph && g_precision != CUFHE_INT8_EXACT;
+    const bool graph = use_graph != 0;
     if (!graph) {
         c->exec.st = s->st;
         for (size_t w = 0; w < c->waves.size(); w++) {

@@ -5,7 +5,8 @@
 * the CUDA-graph run, its replay and the direct run give identical wires;
 * the result is bit-identical to evaluating the same waves one by one
   through cufhe_gate_batch (the circuit adds scheduling, not arithmetic);
-* the INT8 form runs circuits (directly) and decrypts correctly;
+* the INT8 form runs circuits as a CUDA graph too (bit-identical to the
+  direct run) and decrypts correctly;
 * cufhe_autotune yields a table of lanes-per-CTA choices and gates stay
   correct under it.
 """
@@ -110,12 +111,9 @@ def test_circuit_int8_form(keys):
     try:
         net = CI.uneven_workload(5, dags=2, adders=1, dag_gates=(50, 80), adder_width=(8, 8))
         bits, host = prepare(sk, net, engine.LVL1, 55)
-        d = engine.to_device(host)
-        c = engine.Circuit(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1, net.in2, net.out)
-        c.run(d, graph=True)  # the INT8 form launches directly
-        wires = engine.from_device(d, host.shape)
-        c.destroy()
-        check_decrypts(sk, net, engine.LVL1, bits, wires)
+        direct, g1, g2, (waves, _, _) = run_circuit(net, engine.LVL1, host)
+        assert np.array_equal(direct, g1) and np.array_equal(g1, g2)
+        check_decrypts(sk, net, engine.LVL1, bits, direct)
     finally:
         engine.set_precision(P.FP64_FFNT)
         engine.initialize(keys[1])  # the KeyBundle key of the module's other tests

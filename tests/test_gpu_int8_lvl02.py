@@ -120,6 +120,32 @@ def test_fp64_rounding_error_against_exact(ctx):
         assert abs(abs(ph0) - MU2) < 2 ** 56
 
 
+def test_int8_lvl02_circuit_graph_matches_direct(ctx):
+    """A lvl02 circuit in the INT8 form: the CUDA-graph run equals the direct
+    run bit for bit and decrypts to the plaintext evaluation."""
+    from cufhepp_b200 import circuits as CI
+    sk, _ = ctx
+    net = CI.uneven_workload(21, dags=2, adders=1, dag_gates=(40, 80), adder_width=(8, 8))
+    rng = np.random.default_rng(22)
+    bits = rng.integers(0, 2, net.inputs.size).astype(np.uint8)
+    host = np.zeros((net.num_wires, P.TLWE0_WORDS), np.uint32)
+    host[net.inputs] = client.encrypt_bits(sk, bits, 0, seed=23)
+    d = engine.to_device(host)
+    c = engine.Circuit(engine.LVL02, net.num_wires, net.ops, net.in0, net.in1, net.in2, net.out)
+    try:
+        c.run(d, graph=False)
+        direct = engine.from_device(d, host.shape)
+        c.run(d, graph=True)
+        graph = engine.from_device(d, host.shape)
+    finally:
+        c.destroy()
+    engine.synchronize()
+    assert np.array_equal(direct, graph)
+    plain = CI.evaluate(net, bits)
+    got = client.decrypt_bits(sk, direct[net.out], 0)
+    assert int(np.count_nonzero(got != plain[net.out])) == 0
+
+
 def test_int8_lvl02_refuses_keybundle_key():
     sk = client.SecretKey.generate(0x1803)
     engine.initialize_lvl02(client.EvalKey02.generate(sk, keybundle=True))
