@@ -940,6 +940,17 @@ int cufhe_cleanup_lvl02(void)
     return CUFHE_OK;
 }
 
+int cufhe_selftest_wait_timeout(void)
+{
+    cufhe_stream_s* s = resolve(nullptr);
+    DeviceState& D = g_dev[s->device];
+    if (!D.ready) return fail(CUFHE_ERR_STATE, "cufhe_initialize() not called");
+    CK(cudaSetDevice(s->device));
+    CKL(launch_wait_timeout_probe(D.err, 1u << 14, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return check_device_error(s->device);
+}
+
 int cufhe_synchronize(void)
 {
     for (int d = 0; d < g_gpu_num; d++) {

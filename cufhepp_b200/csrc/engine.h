@@ -279,6 +279,9 @@ cudaError_t launch_lut_leaves(const uint8_t* luts, int q, uint32_t mu, uint32_t*
                               cudaStream_t st);
 cudaError_t launch_extract8(const uint32_t* roots, int q, uint32_t* out, cudaStream_t st);
 cudaError_t upload_cb_constants(void);
+// a one-thread kernel whose bounded mbarrier wait (polls tries) runs out and
+// sets *err like the tensor-core kernels do
+cudaError_t launch_wait_timeout_probe(int* err, uint32_t polls, cudaStream_t st);
 
 // Read-only view of the engine state that a gate call on stream `st` uses
 // (keys of the stream's device and the CUDA stream).  Returns 0 or a

@@ -24,6 +24,32 @@ using cufhe::tc_mma_i8;
 using cufhe::tmem_st32;
 using cufhe::tmem_wait_st;
 
+// Failure-path probe: one thread waits on an mbarrier that nothing arrives
+// at, with `polls` bounded polls (the same bounded-wait pattern as the
+// tensor-core kernels, with a short limit), then sets the error flag
+// exactly as those kernels do and returns.
+__global__ void k_wait_timeout_probe(int* err, uint32_t polls)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    cufhe::mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const uint32_t a = smem_u32(&bar);
+    bool done = false;
+    for (uint32_t i = 0; i < polls && !done; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(0u)
+            : "memory");
+        done = ok != 0;
+    }
+    if (!done) atomicOr(err, 4);
+}
+
 constexpr int kProbeSmem = 1024 + 32768 + 64;
 
 __global__ void __launch_bounds__(128, 1) k_i8_peak(int iters, int* err)
@@ -157,3 +183,11 @@ extern "C" int cufhe_measure_int8_peak(double* tops)
     *tops = 2.0 * 128.0 * 256.0 * 32.0 * 4.0 * iters * (double)sms / (ms * 1e-3) / 1e12;
     return CUFHE_OK;
 }
+
+namespace cufhe {
+cudaError_t launch_wait_timeout_probe(int* err, uint32_t polls, cudaStream_t st)
+{
+    k_wait_timeout_probe<<<1, 32, 0, st>>>(err, polls);
+    return cudaGetLastError();
+}
+}  // namespace cufhe

@@ -56,6 +56,7 @@ SIGNATURES = {
     "cufhe_profile_read": ([_i, _vp, _vp], _i),
     "cufhe_measure_fp64_peak": ([_vp], _i),
     "cufhe_measure_int8_peak": ([_vp], _i),
+    "cufhe_selftest_wait_timeout": ([], _i),
     "cufhe_initialize_lvl02": ([_vp], _i),
     "cufhe_cleanup_lvl02": ([], _i),
     "cufhe_blind_rotate_lvl02": ([_vp, _sz, _u64, _i, _vp, _vp, _vp], _i),

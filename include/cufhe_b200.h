@@ -349,6 +349,13 @@ int cufhe_profile_read(int kernel_class, double* total_ms, uint64_t* launches);
 /* FP64 FMA throughput of the current device in TFLOP/s (roof of the FFNT
  * path; runs a short probe kernel) */
 int cufhe_measure_fp64_peak(double* tflops);
+/* Failure-path self-test (no GPU fault): launches a kernel whose bounded
+ * mbarrier wait runs out (a barrier nothing arrives at, about 1 ms of polls),
+ * so it sets the device error flag exactly as a tensor-core kernel whose wait
+ * gave up; then reports like cufhe_synchronize.  Returns CUFHE_ERR_CUDA (the
+ * timeout was detected and the flag cleared) on a healthy engine; the CUDA
+ * context stays usable.  Needs cufhe_initialize. */
+int cufhe_selftest_wait_timeout(void);
 /* INT8 tensor-core throughput of the current device in TOP/s: back-to-back
  * tcgen05.mma.kind::i8 M128 N256 K32 with random operands on every SM (roof
  * of the exact path's step GEMM; runs a short probe kernel) */
