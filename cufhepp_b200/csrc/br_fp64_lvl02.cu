@@ -85,7 +85,8 @@ template <bool KB, int G>
 __global__ void __launch_bounds__(G * 256, G == 1 ? 2 : 1)
     k_br2_fp64(const uint32_t* __restrict__ lane_in, int lanes, uint64_t mu,
                const double2* __restrict__ bkf, const double2* __restrict__ psi2, int steps,
-               uint64_t* __restrict__ acc_out, uint64_t* __restrict__ lane_out)
+               uint64_t* __restrict__ acc_out, uint64_t* __restrict__ lane_out, int in_count,
+               int mu_shift)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     double2* spec = reinterpret_cast<double2*>(smem);       // [G][8][kSlotStride]
@@ -101,7 +102,11 @@ __global__ void __launch_bounds__(G * 256, G == 1 ? 2 : 1)
     for (int g = 0; g < G; g++) {
         const int l = lane_base + g;
         const bool ok = l < lanes;
-        const uint32_t* x = lane_in + (size_t)(ok ? l : 0) * kTlwe0;
+        // lane l rotates input l mod in_count with test value mu >> (mu_shift
+        // (l div in_count)): several test polynomials over one input batch
+        const int src = ok ? l % in_count : 0;
+        const uint64_t mul = mu >> (mu_shift * (ok ? l / in_count : 0));
+        const uint32_t* x = lane_in + (size_t)src * kTlwe0;
         for (int i = tid; i < kN0; i += blockDim.x)
             abar[g * kAbarStride2 + i] = ok ? (uint16_t)((x[i] + (1u << 19)) >> 20) : 0;
         const uint32_t bar = ok ? 2u * kN2 - (x[kN0] >> 20) : 2u * kN2;
@@ -109,9 +114,9 @@ __global__ void __launch_bounds__(G * 256, G == 1 ? 2 : 1)
             acc[g * kTrlwe2 + i] = 0;
             uint64_t v;
             if (bar == 2u * kN2)
-                v = mu;
+                v = mul;
             else
-                v = (((uint32_t)i < (bar & (kN2 - 1))) ^ (bar >> 11)) ? 0ull - mu : mu;
+                v = (((uint32_t)i < (bar & (kN2 - 1))) ^ (bar >> 11)) ? 0ull - mul : mul;
             acc[g * kTrlwe2 + kN2 + i] = v;
         }
     }
@@ -323,7 +328,7 @@ __global__ void __launch_bounds__(64) k_bk2_to_fft(const uint64_t* __restrict__ 
 template <bool KB, int G>
 cudaError_t launch2_g(const uint32_t* lane_in, int lanes, uint64_t mu, const double2* bkf,
                       const double2* psi2, int steps, uint64_t* acc_out, uint64_t* lane_out,
-                      cudaStream_t st)
+                      int in_count, int mu_shift, cudaStream_t st)
 {
     constexpr size_t smem = br2_smem_bytes<G>();
     int dev = 0;
@@ -337,7 +342,7 @@ cudaError_t launch2_g(const uint32_t* lane_in, int lanes, uint64_t mu, const dou
     }
     const int blocks = (lanes + G - 1) / G;
     k_br2_fp64<KB, G><<<blocks, G * 256, smem, st>>>(lane_in, lanes, mu, bkf, psi2, steps, acc_out,
-                                                     lane_out);
+                                                     lane_out, in_count, mu_shift);
     return cudaGetLastError();
 }
 
@@ -347,16 +352,21 @@ cudaError_t launch2_g(const uint32_t* lane_in, int lanes, uint64_t mu, const dou
 // CTA per SM whose key reads serve both lanes).
 cudaError_t launch_br2_fp64(bool kb, const uint32_t* lane_in, int lanes, uint64_t mu,
                             const double2* bkf, const double2* psi2, int steps, uint64_t* acc_out,
-                            uint64_t* lane_out, cudaStream_t st)
+                            uint64_t* lane_out, cudaStream_t st, int in_count, int mu_shift)
 {
     if (lanes <= 0) return cudaSuccess;
+    if (in_count <= 0) in_count = lanes;
     const char* e = getenv("CUFHE_BR2_LANES_PER_CTA");
     const int g = (e && atoi(e) == 2) ? 2 : 1;
     if (g == 2)
-        return kb ? launch2_g<true, 2>(lane_in, lanes, mu, bkf, psi2, steps, acc_out, lane_out, st)
-                  : launch2_g<false, 2>(lane_in, lanes, mu, bkf, psi2, steps, acc_out, lane_out, st);
-    return kb ? launch2_g<true, 1>(lane_in, lanes, mu, bkf, psi2, steps, acc_out, lane_out, st)
-              : launch2_g<false, 1>(lane_in, lanes, mu, bkf, psi2, steps, acc_out, lane_out, st);
+        return kb ? launch2_g<true, 2>(lane_in, lanes, mu, bkf, psi2, steps, acc_out, lane_out,
+                                       in_count, mu_shift, st)
+                  : launch2_g<false, 2>(lane_in, lanes, mu, bkf, psi2, steps, acc_out, lane_out,
+                                        in_count, mu_shift, st);
+    return kb ? launch2_g<true, 1>(lane_in, lanes, mu, bkf, psi2, steps, acc_out, lane_out,
+                                   in_count, mu_shift, st)
+              : launch2_g<false, 1>(lane_in, lanes, mu, bkf, psi2, steps, acc_out, lane_out,
+                                    in_count, mu_shift, st);
 }
 
 cudaError_t launch_bk2_to_fft(const uint64_t* bk, int npolys, const double2* psi2, double2* out,

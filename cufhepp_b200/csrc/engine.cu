@@ -555,8 +555,10 @@ int run_iks20(cufhe_stream_s* s, const Plan& plan, const uint64_t* lane_out, uin
     return CUFHE_OK;
 }
 
+// in_count > 0 (FP64 form only): lane l rotates input l mod in_count with
+// test value mu >> (mu_shift (l div in_count))
 int run_br2(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint64_t mu, int steps,
-            uint64_t* acc_out, uint64_t* lane_out)
+            uint64_t* acc_out, uint64_t* lane_out, int in_count = 0, int mu_shift = 0)
 {
     DeviceState& D = g_dev[s->device];
     if (g_precision == CUFHE_INT8_EXACT) {
@@ -576,7 +578,7 @@ int run_br2(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint64_t mu, 
     }
     LAUNCH(CUFHE_K_BR_FP64_LVL02, s->st,
            launch_br2_fp64(D.kb2 != 0, lane_in, lanes, mu, D.bkf2, D.psi2, steps, acc_out, lane_out,
-                           s->st));
+                           s->st, in_count, mu_shift));
     return CUFHE_OK;
 }
 
@@ -1498,10 +1500,17 @@ int cufhe_circuit_bootstrap(const uint32_t* tlwe0, size_t count, uint32_t* trgsw
     map.per = (int)count;  // unit u = i * count + bit
     map.stride_lo = (size_t)2 * kL * CUFHE_TRLWE1_WORDS;
     map.stride_hi = CUFHE_TRLWE1_WORDS;
-    for (int i = 0; i < kL; i++) {
-        const uint64_t mu = 1ull << (64 - (i + 1) * kBgbit - 1);
-        map.badd[i] = mu;
-        rc = run_br2(s, tlwe0, (int)count, mu, -1, nullptr, t2 + (size_t)i * count * CUFHE_TLWE2_WORDS);
+    for (int i = 0; i < kL; i++) map.badd[i] = 1ull << (64 - (i + 1) * kBgbit - 1);
+    if (g_precision == CUFHE_INT8_EXACT) {
+        for (int i = 0; i < kL; i++) {
+            rc = run_br2(s, tlwe0, (int)count, map.badd[i], -1, nullptr,
+                         t2 + (size_t)i * count * CUFHE_TLWE2_WORDS);
+            if (rc) return rc;
+        }
+    } else {
+        // one launch for the three digits: lane i count + b rotates bit b with
+        // test value mu_0 >> 6 i = mu_i (fills the partial last wave of each)
+        rc = run_br2(s, tlwe0, (int)(kL * count), map.badd[0], -1, nullptr, t2, (int)count, kBgbit);
         if (rc) return rc;
     }
     for (int f = 0; f < 2; f++) {

@@ -227,9 +227,12 @@ constexpr int kPsi2Entries = 514;  // 513 used, padded to an even count
 // FP64 FFNT blind rotation to lvl2 + SampleExtract of `lanes` lvl0 TLWEs;
 // acc_out: TRLWE<lvl2> [lanes][4096], lane_out: TLWE<lvl2> [lanes][2049]
 // (both optional, uint64 words).  bkf: Fourier BK [step][(e)][8][2][1024].
+// in_count > 0: lane l rotates input l mod in_count with test value
+// mu >> (mu_shift (l div in_count)) (several test polynomials in one launch)
 cudaError_t launch_br2_fp64(bool kb, const uint32_t* lane_in, int lanes, uint64_t mu,
                             const double2* bkf, const double2* psi2, int steps, uint64_t* acc_out,
-                            uint64_t* lane_out, cudaStream_t st);
+                            uint64_t* lane_out, cudaStream_t st, int in_count = 0,
+                            int mu_shift = 0);
 cudaError_t launch_bk2_to_fft(const uint64_t* bk, int npolys, const double2* psi2, double2* out,
                               cudaStream_t st);
 cudaError_t upload_fft2_constants(void);
