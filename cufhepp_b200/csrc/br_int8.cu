@@ -355,22 +355,25 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
                 break;
             }
             tc_fence_after();
-#pragma unroll 1
-            for (int cc = 0; cc < 2; cc++) {
-                uint32_t v[32];
-                tmem_ld32(tmem + lane_base + kAccCol + 64 * p + 32 * cc, v);
-                tmem_wait_ld();
-#pragma unroll
-                for (int i = 0; i < 32; i++)
-                    atomicAdd(&red[(size_t)(64 * p + 32 * cc + i) * kRowsCoef + lane], v[i] << (8 * q));
-            }
+            // both column blocks into registers first: the accumulator is
+            // released before the shared-buffer adds, so the next tile's MMAs
+            // wait only for the TMEM reads
+            uint32_t v0[32], v1[32];
+            tmem_ld32(tmem + lane_base + kAccCol + 64 * p, v0);
+            tmem_ld32(tmem + lane_base + kAccCol + 64 * p + 32, v1);
+            tmem_wait_ld();
             tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acc_empty);
+#pragma unroll
+            for (int i = 0; i < 32; i++)
+                atomicAdd(&red[(size_t)(64 * p + i) * kRowsCoef + lane], v0[i] << (8 * q));
+#pragma unroll
+            for (int i = 0; i < 32; i++)
+                atomicAdd(&red[(size_t)(64 * p + 32 + i) * kRowsCoef + lane], v1[i] << (8 * q));
             __threadfence_block();  // this warp's shared-buffer adds before the hand-off
             __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(acc_empty);
-                mbar_arrive(red_full);
-            }
+            if (lane == 0) mbar_arrive(red_full);
             if (!__all_sync(0xffffffffu, mbar_wait(red_full, (uint32_t)it & 1))) {
                 ok = false;
                 break;
