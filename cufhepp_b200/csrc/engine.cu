@@ -1262,12 +1262,41 @@ int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, si
     if (queue.size() != num_gates) return fail(CUFHE_ERR_ARG, "the circuit has a cycle");
     int nwaves = 0;
     for (size_t g = 0; g < num_gates; g++) nwaves = wave[g] + 1 > nwaves ? wave[g] + 1 : nwaves;
-    std::vector<std::vector<int32_t>> members(nwaves);
-    for (size_t g = 0; g < num_gates; g++) members[wave[g]].push_back((int32_t)g);
     const DeviceState& D = g_dev[device];
     if (level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
         return fail(CUFHE_ERR_STATE, level == CUFHE_LVL02 ? "cufhe_initialize_lvl02() not called"
                                                          : "cufhe_initialize() not called");
+    // ---- balancing: a wave of up to `cap` blind-rotation lanes costs one
+    // rotation latency whatever its width, so gates with slack move out of
+    // waves above `cap` into the latest later wave with room (never at or past
+    // a consumer's wave).  Gates go in reverse topological order, so every
+    // consumer's wave is final when its producer moves; the number of waves
+    // stays the critical path.
+    {
+        int sms = 148;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+            sms = 148;
+        const long cap = (long)(level == CUFHE_LVL02 ? 2 : 4) * sms;
+        std::vector<long> load(nwaves, 0);
+        for (size_t g = 0; g < num_gates; g++) load[wave[g]] += lanes_of_gate(gate_ops[g]);
+        for (size_t qi = num_gates; qi-- > 0;) {
+            const int32_t g = queue[qi];
+            if (load[wave[g]] <= cap) continue;
+            int maxw = nwaves - 1;
+            for (int32_t e = head[g]; e >= 0; e = nxt[e])
+                maxw = wave[to[e]] - 1 < maxw ? wave[to[e]] - 1 : maxw;
+            const long lg = lanes_of_gate(gate_ops[g]);
+            for (int w = maxw; w > wave[g]; w--)
+                if (load[w] + lg <= cap) {
+                    load[wave[g]] -= lg;
+                    load[w] += lg;
+                    wave[g] = w;
+                    break;
+                }
+        }
+    }
+    std::vector<std::vector<int32_t>> members(nwaves);
+    for (size_t g = 0; g < num_gates; g++) members[wave[g]].push_back((int32_t)g);
 
     // ---- per-wave plan arrays, packed into one buffer (16-byte aligned)
     auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
