@@ -155,7 +155,10 @@ __global__ void __launch_bounds__(256) k_i8_decompose(const uint32_t* __restrict
 // One CTA per SM; CTA b serves output polynomial j = b & 1 and walks that
 // polynomial's tiles t = b >> 1, + gridDim.x / 2, ... (tile = 256-lane digit
 // group x 128 rows = 4 limbs x 32 coefficients), so it keeps one 32 KB key
-// window, TMEM and the barriers for its whole life.  Each K chunk has ONE
+// window, TMEM and the barriers for its whole life.  The tiles of the last,
+// partial round are split along K (unit_of), so a batch whose tile count is
+// not a multiple of the CTA count ends with a fraction of a tile, not a whole
+// one; the drain adds every unit into the global accumulator atomically.  Each K chunk has ONE
 // full barrier (the producer's transaction bytes and the 128 A-generator
 // arrivals) and ONE empty barrier (the MMA commit): with one wait and one
 // commit per chunk the issuing thread keeps up with M128 N256 K32 MMAs.
@@ -171,8 +174,8 @@ __global__ void __launch_bounds__(256) k_i8_decompose(const uint32_t* __restrict
 //   warps 10-25 drainers (four per TMEM lane quadrant, 64 columns each):
 //               read the accumulator, add the four limb rows into a shared
 //               [256 lanes][32 coefficients] buffer (limb q shifted by 8q),
-//               release the accumulator, then add the buffer into the global
-//               accumulator while the next tile's MMAs run
+//               release the accumulator, then add the buffer atomically into
+//               the global accumulator while the next unit's MMAs run
 // Every wait is bounded; an expired wait sets s_fail, which all roles poll.
 constexpr int kPStages = 5;
 constexpr size_t kSmemPB = (size_t)kPStages * kTileBytes;                // 160 KB
@@ -195,10 +198,30 @@ __device__ __forceinline__ void tmem_st16(uint32_t addr, const uint32_t (&v)[16]
         : "memory");
 }
 
+// Work unit `it` of CTA cb: the first R units are whole tiles
+// t = cb + it * ncj (all 32 K chunks); the tiles of the last, partial round
+// are split along K into `split` units of 32 / split chunks each, dealt out
+// over the CTAs, so that the last round costs 1 / split of a tile.
+__device__ __forceinline__ void unit_of(int it, const int* geo, int& t, int& k0, int& nk)
+{
+    // geo = {R, cb, ncj, split}
+    const int R = geo[0], cb = geo[1], ncj = geo[2];
+    if (it < R) {
+        t = cb + it * ncj;
+        k0 = 0;
+        nk = kChunks;
+    } else {
+        const int split = geo[3], u = cb + (it - R) * ncj;
+        t = R * ncj + u / split;
+        nk = kChunks / split;
+        k0 = (u % split) * nk;
+    }
+}
+
 __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __restrict__ vkey,
                                                                 const uint8_t* __restrict__ tiles,
                                                                 uint32_t* __restrict__ acc,
-                                                                int lanes, int tiles_j,
+                                                                int lanes, int tiles_j, int split,
                                                                 int* __restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -217,10 +240,12 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
     uint64_t* red_clear = red_full + 1;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(red_clear + 1);
     __shared__ volatile int s_fail;
+    __shared__ int s_geo[4];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int j_out = blockIdx.x & 1, cb = blockIdx.x >> 1, ncj = gridDim.x >> 1;
-    const int T = cb < tiles_j ? (tiles_j - 1 - cb) / ncj + 1 : 0;
+    const int R = tiles_j / ncj, NU = (tiles_j - R * ncj) * split;
+    const int T = R + (cb < NU ? (NU - 1 - cb) / ncj + 1 : 0);
 
     for (size_t i = tid; i < kRedWords; i += blockDim.x) red[i] = 0u;
     if (warp == 0) {
@@ -230,6 +255,10 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
     }
     if (tid == 0) {
         s_fail = 0;
+        s_geo[0] = R;
+        s_geo[1] = cb;
+        s_geo[2] = ncj;
+        s_geo[3] = split;
         for (int s = 0; s < kPStages; s++) {
             mbar_init(&full[s], 128 + 1);
             mbar_init(&empty[s], 1);
@@ -254,11 +283,14 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
                 mbar_expect_tx(bar_v, (uint32_t)kSmemPV);
                 bulk_g2s(vs, vkey + (size_t)j_out * kVBytesJ, (uint32_t)kSmemPV, bar_v);
             }
+            int gbase = 0;
             for (int it = 0; it < T && !s_fail; it++) {
-                const int group = (cb + it * ncj) / (kN / kRowsCoef);
+                int t, k0, nk;
+                unit_of(it, s_geo, t, k0, nk);
+                const int group = t / (kN / kRowsCoef);
                 const uint8_t* gt = tiles + (size_t)group * kChunks * kTileBytes;
-                for (int kc = par; kc < kChunks; kc += 2) {
-                    const int gc = it * kChunks + kc, s = gc % kPStages;
+                for (int lk = par; lk < nk; lk += 2) {
+                    const int kc = k0 + lk, gc = gbase + lk, s = gc % kPStages;
                     if (s_fail) break;
                     if (gc >= kPStages &&
                         !mbar_wait(&empty[s], (uint32_t)((gc / kPStages) - 1) & 1)) {
@@ -268,6 +300,7 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
                     mbar_expect_tx(&full[s], kTileBytes);
                     bulk_g2s(bst + s * kTileBytes, gt + (size_t)kc * kTileBytes, kTileBytes, &full[s]);
                 }
+                gbase += nk;
             }
         }
     } else if (warp == 8) {
@@ -275,12 +308,14 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
         if (lane == 0) {
             int gc = 0;
             for (int it = 0; it < T && !s_fail; it++) {
+                int t, k0, nk;
+                unit_of(it, s_geo, t, k0, nk);
                 if (it >= 1 && !mbar_wait(acc_empty, (uint32_t)(it - 1) & 1)) {
                     s_fail = 1;
                     break;
                 }
                 tc_fence_after();
-                for (int kc = 0; kc < kChunks; kc++, gc++) {
+                for (int lk = 0; lk < nk; lk++, gc++) {
                     const int s = gc % kPStages;
                     if (!mbar_wait(&full[s], (uint32_t)(gc / kPStages) & 1)) {
                         s_fail = 1;
@@ -291,7 +326,7 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
 #pragma unroll
                     for (int k = 0; k < kChunkK / 32; k++)
                         tc_mma_i8(tmem + kAccCol, tmem + kACol + 32 * s + 8 * k,
-                                  desc_kmajor_sw128(bbase + 32 * k), kIdesc, (kc | k) != 0);
+                                  desc_kmajor_sw128(bbase + 32 * k), kIdesc, (lk | k) != 0);
                     tc_commit(&empty[s]);
                 }
                 if (s_fail) break;
@@ -303,10 +338,13 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
         const int wg = warp >> 2, q = warp & 3;
         const uint32_t lane_base = (uint32_t)(32 * q) << 16;
         bool ok = __all_sync(0xffffffffu, mbar_wait(bar_v, 0));
+        int gbase = 0;
         for (int it = 0; it < T && ok; it++) {
-            const int n = ((cb + it * ncj) % (kN / kRowsCoef)) * kRowsCoef + lane;
-            for (int kc = wg; kc < kChunks; kc += 2) {
-                const int gc = it * kChunks + kc, s = gc % kPStages;
+            int t, k0, nk;
+            unit_of(it, s_geo, t, k0, nk);
+            const int n = (t % (kN / kRowsCoef)) * kRowsCoef + lane;
+            for (int lk = wg; lk < nk; lk += 2) {
+                const int kc = k0 + lk, gc = gbase + lk, s = gc % kPStages;
                 if (__any_sync(0xffffffffu, s_fail != 0)) {
                     ok = false;
                     break;
@@ -337,6 +375,7 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
                 tc_fence_before();
                 mbar_arrive(&full[s]);
             }
+            gbase += nk;
         }
         if (!ok) s_fail = 1;
     } else {
@@ -346,9 +385,6 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
         const uint32_t lane_base = (uint32_t)(32 * q) << 16;
         bool ok = true;
         for (int it = 0; it < T && ok; it++) {
-            const int t = cb + it * ncj;
-            const int group = t / (kN / kRowsCoef);
-            const int n0 = (t % (kN / kRowsCoef)) * kRowsCoef;
             if (__any_sync(0xffffffffu, s_fail != 0) ||
                 !__all_sync(0xffffffffu, mbar_wait(acc_full, (uint32_t)it & 1))) {
                 ok = false;
@@ -378,20 +414,19 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
                 ok = false;
                 break;
             }
-            // 16 rows per warp, all loads in flight before the stores
+            int t, k0, nk;
+            unit_of(it, s_geo, t, k0, nk);
+            const int group = t / (kN / kRowsCoef);
+            const int n0 = (t % (kN / kRowsCoef)) * kRowsCoef;
             constexpr int kW = kGroup / kDrainWarps;
-            uint32_t old[kW];
-#pragma unroll
-            for (int i = 0; i < kW; i++) {
-                const int l = group * kGroup + d + kDrainWarps * i;
-                old[i] = l < lanes ? acc[(size_t)l * kTrlwe + j_out * kN + n0 + lane] : 0u;
-            }
+            // a tile split along K is added by several CTAs: atomic adds
+            // (mod 2^32, so their order does not matter)
 #pragma unroll
             for (int i = 0; i < kW; i++) {
                 const int gl = d + kDrainWarps * i, l = group * kGroup + gl;
                 const uint32_t v = red[(size_t)gl * kRowsCoef + lane];
                 red[(size_t)gl * kRowsCoef + lane] = 0u;
-                if (l < lanes) acc[(size_t)l * kTrlwe + j_out * kN + n0 + lane] = old[i] + v;
+                if (l < lanes) atomicAdd(&acc[(size_t)l * kTrlwe + j_out * kN + n0 + lane], v);
             }
             __threadfence_block();  // the zeroed buffer before the next tile's adds
             __syncwarp();
@@ -514,9 +549,14 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
         const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * kVBytesStep;
         // even grid: CTA b serves output polynomial b & 1
         const int tiles_j = groups * (kN / kRowsCoef);
-        const int grid = 2 * (tiles_j < sms / 2 ? tiles_j : sms / 2);
-        k_i8_gemm_p<<<grid, kGemmPThreads, kSmemGemmP, st>>>(vk, (const uint8_t*)w.digits, w.acc,
-                                                            lanes, tiles_j, err);
+        // tiles of the last, partial round are split along K so that the
+        // round's units fit one per CTA pair (split = 1, 2, 4 or 8)
+        const int ncj = sms / 2, rem = tiles_j % ncj;
+        int split = 1;
+        while (rem && split < 8 && rem * split * 2 <= ncj) split *= 2;
+        const int units = tiles_j < ncj ? tiles_j * split : ncj;
+        k_i8_gemm_p<<<2 * units, kGemmPThreads, kSmemGemmP, st>>>(vk, (const uint8_t*)w.digits, w.acc,
+                                                               lanes, tiles_j, split, err);
         n += 2;
     }
     k_i8_extract<<<lanes, 256, 0, st>>>(w.acc, lanes, acc_out, lane_out);
