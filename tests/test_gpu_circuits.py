@@ -5,6 +5,8 @@
 * the CUDA-graph run, its replay and the direct run give identical wires;
 * the result is bit-identical to evaluating the same waves one by one
   through cufhe_gate_batch (the circuit adds scheduling, not arithmetic);
+* gates with scheduling slack move into narrow later waves without adding
+  waves;
 * the INT8 form runs circuits as a CUDA graph too (bit-identical to the
   direct run) and decrypts correctly;
 * cufhe_autotune yields a table of lanes-per-CTA choices and gates stay
@@ -102,6 +104,45 @@ def test_circuit_with_not_copy_and_nmux(lvl1_ctx):
         direct, g1, _, (waves, _, _) = run_circuit(net, engine.LVL1, host)
         assert waves == 3 and np.array_equal(direct, g1)
         check_decrypts(sk, net, engine.LVL1, bits, direct)
+
+
+def test_slack_gates_fill_narrow_waves(lvl1_ctx):
+    """A 6-gate chain beside 1400 independent gates: levelised as soon as
+    possible, wave 0 would hold 1401 gates and waves 1-5 one each.  Gates
+    with slack move into the narrow later waves (none wider than one resident
+    round, 4 lanes per SM); the wave count stays the chain length and every
+    wire equals the level-by-level evaluation."""
+    import torch
+
+    sk = lvl1_ctx
+    width, depth = 1400, 6
+    ins = np.arange(width + 1, dtype=np.int32)
+    chain_out = width + 1 + np.arange(depth, dtype=np.int32)
+    side_out = width + 1 + depth + np.arange(width, dtype=np.int32)
+    in0 = np.concatenate([[0], chain_out[:-1], ins[:width]]).astype(np.int32)
+    in1 = np.concatenate([np.ones(depth, np.int32), ins[1:width + 1]]).astype(np.int32)
+    out = np.concatenate([chain_out, side_out]).astype(np.int32)
+    ops = np.full(out.size, P.NAND, np.int32)
+    net = CI.Netlist(int(out.max()) + 1, ins, ops, in0, in1, np.full(out.size, -1, np.int32),
+                     out, out)
+    assert int(CI.levels(net).max()) + 1 == depth
+    bits, host = prepare(sk, net, engine.LVL1, 61)
+    d = engine.to_device(host)
+    c = engine.Circuit(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1, net.in2, net.out)
+    try:
+        waves, _, max_lanes = c.info()
+        gates, lanes = c.wave_sizes()
+        c.run(d, graph=False)
+        wires = engine.from_device(d, host.shape)
+    finally:
+        c.destroy()
+    cap = 4 * torch.cuda.get_device_properties(0).multi_processor_count
+    assert waves == depth
+    assert int(gates.sum()) == net.gates and int(lanes.sum()) == net.bootstraps()
+    assert max_lanes == int(lanes.max()) <= cap
+    assert int(lanes[-1]) > 1  # the narrow waves (latest first) took gates
+    check_decrypts(sk, net, engine.LVL1, bits, wires)
+    assert np.array_equal(wires, wave_by_wave(net, engine.LVL1, host))
 
 
 def test_circuit_int8_form(keys):
