@@ -22,7 +22,14 @@
 //            (psi^{(1+4f) a} - 1) instead of the reference's 16 MB xai table
 //   phase 3  warp (g, j): inverse FFT, untwist, round, write acc[g][j]
 // Epilogue: SampleExtract straight from shared memory to the lane output.
+// Batches of up to 16 lanes run the latency form k_br_fp64_clu instead: one
+// lane per cluster of four CTAs on four SMs, each multiplying a quarter of the
+// bins with the key (a lone lane is bound by one SM's L2 bandwidth for the
+// 196 KB of key rows per step) and gathering the other quarters through
+// distributed shared memory for the inverse transforms.
 #include <stdlib.h>
+
+#include <cooperative_groups.h>
 
 #include "engine.h"
 #include "fft64.cuh"
@@ -289,6 +296,213 @@ cudaError_t launch_g(const uint32_t* lane_in, int lanes, uint32_t mu, const doub
     return cudaGetLastError();
 }
 
+// ---- latency form for small batches: one lane per cluster of four CTAs on
+// four SMs.  A single lane's step is bound by the rate at which one SM pulls
+// the step's key rows from L2 (196 KB per KeyBundle step); here every CTA of
+// the cluster runs the lane's transforms (redundantly, on its own copy of the
+// accumulator) but multiplies only its quarter of the frequency bins with the
+// key, and the inverse transforms gather the four quarters from the peers'
+// shared memory (distributed shared memory).  The arithmetic of every bin is
+// that of k_br_fp64, so the result is bit-identical.
+constexpr int kCluRanks = 4;
+constexpr int kCluMaxLanes = 16;         // measured: faster than one CTA per lane up to 16 lanes
+constexpr size_t kCluSmem = 120 * 1024;  // > half an SM: one CTA per SM
+
+template <bool KB>
+__global__ void __cluster_dims__(kCluRanks, 1, 1) __launch_bounds__(128, 1)
+    k_br_fp64_clu(const uint32_t* __restrict__ lane_in, int lanes, uint32_t mu,
+                  const double2* __restrict__ bkf, const double2* __restrict__ psi, int steps,
+                  uint32_t* __restrict__ acc_out, uint32_t* __restrict__ lane_out)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2* spec = reinterpret_cast<double2*>(smem);
+    double2* psi_s = spec + 4 * kSlotStride;
+    uint32_t* acc = reinterpret_cast<uint32_t*>(psi_s + kN);
+    uint16_t* abar = reinterpret_cast<uint16_t*>(acc + kTrlwe);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int rank = (int)cluster.block_rank();
+    const int l = blockIdx.x / kCluRanks;
+    const bool ok = l < lanes;
+
+    for (int t = tid; t < kN; t += blockDim.x) psi_s[psi_pos((uint32_t)t)] = psi[t];
+    {
+        const uint32_t* x = lane_in + (size_t)(ok ? l : 0) * kTlwe0;
+        for (int i = tid; i < kN0; i += blockDim.x)
+            abar[i] = ok ? (uint16_t)((x[i] + (1u << 20)) >> 21) : 0;
+        const uint32_t bar = ok ? 2u * kN - (x[kN0] >> 21) : 2u * kN;
+        for (int i = tid; i < kN; i += blockDim.x) {
+            acc[i] = 0;
+            uint32_t v;
+            if (bar == 2u * kN)
+                v = mu;
+            else
+                v = (((uint32_t)i < (bar & (kN - 1))) ^ (bar >> 10)) ? 0u - mu : mu;
+            acc[kN + i] = v;
+        }
+    }
+    // the peers' transform slots 0 and 1 (the multiply-accumulate results)
+    const double2* peer[kCluRanks];
+#pragma unroll
+    for (int k = 0; k < kCluRanks; k++) peer[k] = cluster.map_shared_rank(spec, k);
+    cluster.sync();
+
+    const int total = KB ? kN0 / 2 : kN0;
+    const int nsteps = (steps < 0 || steps > total) ? total : steps;
+    constexpr size_t kTrgswF = 4 * 2 * kHalfN;
+
+#pragma unroll 1
+    for (int p = 0; p < nsteps; p++) {
+        // ---- phase 1 (every rank): decompose + fold + twist + forward FFT, warp r
+        {
+            const int r = warp, j = r >> 1, d = r & 1;
+            const uint32_t* a = acc + j * kN;
+            double2 v[16];
+            const uint32_t ab = KB ? 0u : abar[p];
+            const uint32_t abm = ab & (kN - 1), abn = ab >> 10;
+#pragma unroll
+            for (int n2 = 0; n2 < 16; n2++) {
+                const int n = lane + 32 * n2;
+                uint32_t lo = a[n], hi = a[n + kHalfN];
+                if (!KB) {
+                    uint32_t rl = a[(n - ab) & (kN - 1)];
+                    uint32_t rh = a[(n + kHalfN - ab) & (kN - 1)];
+                    rl = (((uint32_t)n < abm) ^ abn) ? 0u - rl : rl;
+                    rh = (((uint32_t)(n + kHalfN) < abm) ^ abn) ? 0u - rh : rh;
+                    lo = rl - lo;
+                    hi = rh - hi;
+                }
+                v[n2] = make_double2(digit_of(lo + kDecOffset, d), digit_of(hi + kDecOffset, d));
+            }
+            double2* slot = spec + r * kSlotStride;
+            ffnt_forward_warp(v, slot, psi_s, lane);
+#pragma unroll
+            for (int m = 0; m < 16; m++) slot[(lane & 15) + 16 * m + 256 * (lane >> 4)] = v[m];
+        }
+        __syncthreads();
+
+        // ---- phase 2 (rank k): key multiply-accumulate of bins [128 k, 128 k + 128)
+        {
+            const int f = rank * 128 + tid;
+            double2 D[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) D[r] = spec[r * kSlotStride + f];
+            double2 out0;
+            if (KB) {
+                const double2* bk = bkf + (size_t)p * 3 * kTrgswF;
+                const uint32_t ef = 1u + 4u * (uint32_t)f;
+                const uint32_t a0 = abar[2 * p], a1 = abar[2 * p + 1];
+                double2 x0 = psi_at(psi_s, ef * a0);
+                double2 x1 = psi_at(psi_s, ef * a1);
+                double2 x01 = psi_at(psi_s, ef * (a0 + a1));
+                x0.x -= 1.0;
+                x1.x -= 1.0;
+                x01.x -= 1.0;
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    double2 b[3][4];
+#pragma unroll
+                    for (int e = 0; e < 3; e++)
+#pragma unroll
+                        for (int r = 0; r < 4; r++)
+                            b[e][r] = __ldg(&bk[((e * 4 + r) * 2 + j) * kHalfN + f]);
+                    double2 s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0;
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        s0 = cfma(s0, D[r], b[0][r]);
+                        s1 = cfma(s1, D[r], b[1][r]);
+                        s2 = cfma(s2, D[r], b[2][r]);
+                    }
+                    double2 o = make_double2(fma(D[2 * j].x, 0x1p-8, D[2 * j + 1].x * 0x1p-16),
+                                             fma(D[2 * j].y, 0x1p-8, D[2 * j + 1].y * 0x1p-16));
+                    o = cfma(o, x01, s0);
+                    o = cfma(o, x0, s1);
+                    o = cfma(o, x1, s2);
+                    if (j == 0)
+                        out0 = o;
+                    else {
+                        spec[0 * kSlotStride + f] = out0;
+                        spec[1 * kSlotStride + f] = o;
+                    }
+                }
+            } else {
+                const double2* bk = bkf + (size_t)p * kTrgswF;
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    double2 o = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int r = 0; r < 4; r++)
+                        o = cfma(o, D[r], __ldg(&bk[(r * 2 + j) * kHalfN + f]));
+                    if (j == 0)
+                        out0 = o;
+                    else {
+                        spec[0 * kSlotStride + f] = out0;
+                        spec[1 * kSlotStride + f] = o;
+                    }
+                }
+            }
+        }
+        cluster.sync();  // every rank's quarter of slots 0 and 1 is written
+
+        // ---- phase 3 (every rank): gather, inverse FFT, untwist, round, warp j
+        if (warp < 2) {
+            const int j = warp;
+            double2 v[16];
+#pragma unroll
+            for (int n2 = 0; n2 < 16; n2++)
+                v[n2] = peer[n2 >> 2][j * kSlotStride + lane + 32 * n2];
+            double2* scratch = spec + (2 + j) * kSlotStride;  // rows 2, 3 are free now
+            ffnt_inverse_warp(v, scratch, psi_s, lane);
+            uint32_t* a = acc + j * kN;
+#pragma unroll
+            for (int m = 0; m < 16; m++) {
+                const int n = (lane & 15) + 16 * m + 256 * (lane >> 4);
+                const double2 u = v[m];
+                const uint32_t lo = (uint32_t)__double2ll_rn(u.x * 0x1p23);
+                const uint32_t hi = (uint32_t)__double2ll_rn(u.y * 0x1p23);
+                if (KB) {
+                    a[n] = lo;
+                    a[n + kHalfN] = hi;
+                } else {
+                    a[n] += lo;
+                    a[n + kHalfN] += hi;
+                }
+            }
+        }
+        cluster.sync();  // the gathers are done before slots 0 and 1 are rewritten
+    }
+
+    if (ok && rank == 0) {
+        if (acc_out)
+            for (int i = tid; i < kTrlwe; i += blockDim.x) acc_out[(size_t)l * kTrlwe + i] = acc[i];
+        if (lane_out) {
+            uint32_t* o = lane_out + (size_t)l * kTlwe1;
+            for (int i = tid; i <= kN; i += blockDim.x)
+                o[i] = i == kN ? acc[kN] : (i == 0 ? acc[0] : 0u - acc[kN - i]);
+        }
+    }
+}
+
+template <bool KB>
+cudaError_t launch_clu(const uint32_t* lane_in, int lanes, uint32_t mu, const double2* bkf,
+                       const Fp64Tables& t, int steps, uint32_t* acc_out, uint32_t* lane_out,
+                       cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr[64] = {};
+    if (!attr[dev & 63]) {
+        cudaError_t e = cudaFuncSetAttribute(k_br_fp64_clu<KB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCluSmem);
+        if (e != cudaSuccess) return e;
+        attr[dev & 63] = true;
+    }
+    k_br_fp64_clu<KB><<<lanes * kCluRanks, 128, kCluSmem, st>>>(lane_in, lanes, mu, bkf, t.psi, steps,
+                                                              acc_out, lane_out);
+    return cudaGetLastError();
+}
 }  // namespace
 
 // Lanes per CTA: 1 (three CTAs per SM), 2 (two CTAs per SM, whose phases
@@ -362,6 +576,22 @@ cudaError_t launch_br_fp64_g(int g, bool kb, const uint32_t* lane_in, int lanes,
                              uint32_t* acc_out, uint32_t* lane_out, cudaStream_t st)
 {
     if (lanes <= 0) return cudaSuccess;
+    if (g == 1 && lanes <= kCluMaxLanes) {
+        // small batches: one lane per cluster of four SMs (CUFHE_BR_CLUSTER=0
+        // keeps one CTA per lane); a device that cannot place the clusters
+        // runs the one-CTA kernel instead
+        int sms = 148, dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const char* e = getenv("CUFHE_BR_CLUSTER");
+        if (lanes * kCluRanks <= sms && !(e && atoi(e) == 0)) {
+            const cudaError_t r =
+                kb ? launch_clu<true>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st)
+                   : launch_clu<false>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st);
+            if (r == cudaSuccess) return r;
+            cudaGetLastError();
+        }
+    }
     if (g == 1)
         return kb ? launch_g<true, 1>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st)
                   : launch_g<false, 1>(lane_in, lanes, mu, bkf, t, steps, acc_out, lane_out, st);

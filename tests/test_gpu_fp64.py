@@ -4,9 +4,12 @@
 * blind rotation (KeyBundle and plain): FP64 rounding against the exact
   schoolbook oracle -- one step bit-exact up to +-1 per coefficient, full
   rotations within a phase tolerance of 2^-12 (torus) of the exact result;
+* small batches (the cluster form) equal the one-CTA-per-lane form bit for bit;
 * gates, both orders, every gate id: decrypt to the truth tables
   (test/plain.h:1-70) and match the oracle's phase within 2^-12.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -56,6 +59,31 @@ def test_identity_keyswitch_bit_exact(ctx):
     ref = O.iks_batch(c1, None, 1, 0, 0, ek.ksk)
     assert np.array_equal(got, ref)
     assert np.array_equal(client.decrypt_bits(sk, got, 0), bits)
+
+
+@pytest.mark.parametrize("lanes", [1, 9, 16])
+def test_cluster_form_for_small_batches_is_bit_identical(ctx, lanes):
+    """Up to 16 lanes the rotation runs one lane per cluster of four CTAs (the
+    key multiply-accumulate split over four SMs, partial spectra gathered
+    through distributed shared memory); CUFHE_BR_CLUSTER=0 keeps one CTA per
+    lane.  Both must give the same accumulators bit for bit."""
+    sk, ek, _ = ctx
+    _, x = lvl0_inputs(sk, lanes, 31 + lanes)
+    d_in = engine.to_device(x)
+    got = {}
+    for cluster in (False, True):
+        if cluster:
+            os.environ.pop("CUFHE_BR_CLUSTER", None)
+        else:
+            os.environ["CUFHE_BR_CLUSTER"] = "0"
+        try:
+            d_acc = engine.DeviceBuffer(lanes * P.TRLWE1_WORDS * 4)
+            engine.blind_rotate(d_in, lanes, P.MU32, -1, acc_out=d_acc)
+            engine.synchronize()
+            got[cluster] = engine.from_device(d_acc, (lanes, P.TRLWE1_WORDS))
+        finally:
+            os.environ.pop("CUFHE_BR_CLUSTER", None)
+    assert np.array_equal(got[True], got[False])
 
 
 def test_blind_rotate_one_step(ctx):
