@@ -21,9 +21,14 @@
 //   M  thread (bin pair, lane): radix-2 join, key MAC into registers
 //      (after the second chunk: inverse radix-2 split -> slots)
 //   I  warp (g, j, parity): inverse 512-point FFT, untwist, Torus64 rounding
+// Batches of up to SMs / 2 lanes run k_br2_fp64_clu instead: one lane per
+// cluster of two CTAs on two SMs, the key MAC split between them and the
+// products gathered through distributed shared memory.
 // The root table psi2^s (psi2 = e^{i pi / 2048}) keeps s in [0, 512] only
 // (8 KB); other powers follow from psi2^{1024} = i and
 // psi2^{1024 - s} = i conj(psi2^s).
+#include <cooperative_groups.h>
+
 #include "engine.h"
 #include "fft64.cuh"
 
@@ -346,6 +351,246 @@ cudaError_t launch2_g(const uint32_t* lane_in, int lanes, uint64_t mu, const dou
     return cudaGetLastError();
 }
 
+// ---- latency form for small batches: one lane per cluster of R CTAs on R
+// SMs.  A lone lane's step is bound by one SM pulling the step's 786 KB of
+// key rows (KeyBundle) from L2, and two lanes sharing an SM are held to 128
+// registers per thread; here every CTA has an SM to itself, runs the lane's
+// transforms on its own copy of the accumulator, multiplies only 1/R of the
+// bin pairs with the key, and the inverse transforms gather the other parts
+// from the peers' shared memory (distributed shared memory).  Per bin the
+// arithmetic is that of k_br2_fp64, so the result is bit-identical.
+constexpr int kClu2Ranks = 2;              // measured: 2 beats 4 and 8 beyond one lane
+constexpr size_t kClu2Smem = 120 * 1024;  // > half an SM: one CTA per SM
+static_assert(br2_smem_bytes<1>() <= kClu2Smem, "lvl2 cluster CTA layout");
+
+template <bool KB, int R>
+__global__ void __launch_bounds__(256, 1)
+    k_br2_fp64_clu(const uint32_t* __restrict__ lane_in, int lanes, uint64_t mu,
+                   const double2* __restrict__ bkf, const double2* __restrict__ psi2, int steps,
+                   uint64_t* __restrict__ acc_out, uint64_t* __restrict__ lane_out, int in_count,
+                   int mu_shift)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2* spec = reinterpret_cast<double2*>(smem);       // [8][kSlotStride]
+    double2* tab = spec + 8 * kSlotStride;                  // [kPsi2Entries]
+    uint64_t* acc = reinterpret_cast<uint64_t*>(tab + kPsi2Entries);  // [2][2048]
+    uint16_t* abar = reinterpret_cast<uint16_t*>(acc + kTrlwe2);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int rank = (int)cluster.block_rank();
+    const int l = blockIdx.x / R;
+    const bool ok = l < lanes;
+
+    for (int t = tid; t < kPsi2Entries; t += blockDim.x) tab[t] = psi2[t];
+    {
+        const int src = ok ? l % in_count : 0;
+        const uint64_t mul = mu >> (mu_shift * (ok ? l / in_count : 0));
+        const uint32_t* x = lane_in + (size_t)src * kTlwe0;
+        for (int i = tid; i < kN0; i += blockDim.x)
+            abar[i] = ok ? (uint16_t)((x[i] + (1u << 19)) >> 20) : 0;
+        const uint32_t bar = ok ? 2u * kN2 - (x[kN0] >> 20) : 2u * kN2;
+        for (int i = tid; i < kN2; i += blockDim.x) {
+            acc[i] = 0;
+            uint64_t v;
+            if (bar == 2u * kN2)
+                v = mul;
+            else
+                v = (((uint32_t)i < (bar & (kN2 - 1))) ^ (bar >> 11)) ? 0ull - mul : mul;
+            acc[kN2 + i] = v;
+        }
+    }
+    const double2* peer[R];
+#pragma unroll
+    for (int k = 0; k < R; k++) peer[k] = cluster.map_shared_rank(spec, k);
+    cluster.sync();
+
+    const int total = KB ? kN0 / 2 : kN0;
+    const int nsteps = (steps < 0 || steps > total) ? total : steps;
+
+#pragma unroll 1
+    for (int p = 0; p < nsteps; p++) {
+        double2 out[2][2];  // [j][bin half] of this thread's bin pair
+        const double2* bk = bkf + (size_t)p * (KB ? 3 : 1) * kTrgswF2;
+#pragma unroll 1
+        for (int c = 0; c < 2; c++) {
+            // ---- F (every rank): digits of input polynomial c, row d, parity par
+            {
+                const int s = warp, d = s >> 1, par = s & 1;
+                const uint64_t* a = acc + c * kN2;
+                const uint32_t ab = KB ? 0u : abar[p];
+                const uint32_t abm = ab & (kN2 - 1), abn = ab >> 11;
+                double2 v[16];
+#pragma unroll
+                for (int n2 = 0; n2 < 16; n2++) {
+                    const int n = 2 * (lane + 32 * n2) + par;
+                    uint64_t lo = a[n], hi = a[n + 1024];
+                    if constexpr (!KB) {
+                        uint64_t rl = a[(n - ab) & (kN2 - 1)];
+                        uint64_t rh = a[(n + 1024 - ab) & (kN2 - 1)];
+                        rl = (((uint32_t)n < abm) ^ abn) ? 0ull - rl : rl;
+                        rh = (((uint32_t)(n + 1024) < abm) ^ abn) ? 0ull - rh : rh;
+                        lo = rl - lo;
+                        hi = rh - hi;
+                    }
+                    v[n2] = make_double2(digit2_of(lo + kDecOffset2, d),
+                                         digit2_of(hi + kDecOffset2, d));
+                    if (n2) v[n2] = cmul(v[n2], c_tw32[n2]);
+                }
+                double2* slot = spec + s * kSlotStride;
+                dft512_fwd_post(v, slot, lane, psi2_at(tab, 2u * lane + par),
+                                psi2_at(tab, 8u * lane));
+#pragma unroll
+                for (int m = 0; m < 16; m++) slot[(lane & 15) + 16 * m + 256 * (lane >> 4)] = v[m];
+            }
+            __syncthreads();
+
+            // ---- M (rank r): radix-2 join + key MAC of bin pairs [128 r, 128 r + 128)
+            if (tid < 512 / R) {
+                const int k = rank * (512 / R) + tid;  // bin pair (k, k + 512)
+                const double2 w4 = psi2_at(tab, 4u * (uint32_t)k);
+                double2 fac[2][3];
+                if (KB) {
+                    const uint32_t a0 = abar[2 * p];
+                    const uint32_t a1 = abar[2 * p + 1];
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const uint32_t e = 1u + 4u * (uint32_t)(k + 512 * h);
+                        fac[h][0] = psi2_at(tab, e * (a0 + a1));
+                        fac[h][1] = psi2_at(tab, e * a0);
+                        fac[h][2] = psi2_at(tab, e * a1);
+#pragma unroll
+                        for (int f = 0; f < 3; f++) fac[h][f].x -= 1.0;
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int bin = k + 512 * h;
+                    double2 Z[4];
+#pragma unroll
+                    for (int d = 0; d < 4; d++) {
+                        const double2 E = spec[(2 * d) * kSlotStride + k];
+                        const double2 wo = cmul(spec[(2 * d + 1) * kSlotStride + k], w4);
+                        Z[d] = h ? csub(E, wo) : cadd(E, wo);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 2; j++) {
+                        double2 o = c ? out[j][h] : make_double2(0.0, 0.0);
+                        if (KB) {
+                            double2 s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0;
+#pragma unroll
+                            for (int d = 0; d < 4; d++) {
+                                const int r = c * 4 + d;
+                                const size_t ki = ((size_t)r * 2 + j) * 1024 + bin;
+                                s0 = cfma(s0, Z[d], __ldg(&bk[0 * kTrgswF2 + ki]));
+                                s1 = cfma(s1, Z[d], __ldg(&bk[1 * kTrgswF2 + ki]));
+                                s2 = cfma(s2, Z[d], __ldg(&bk[2 * kTrgswF2 + ki]));
+                            }
+                            if (j == c) {
+#pragma unroll
+                                for (int d = 0; d < 4; d++) {
+                                    const double sc = d == 0 ? 0x1p-10 : d == 1 ? 0x1p-20
+                                                    : d == 2 ? 0x1p-30 : 0x1p-40;
+                                    o.x = fma(Z[d].x, sc, o.x);
+                                    o.y = fma(Z[d].y, sc, o.y);
+                                }
+                            }
+                            o = cfma(o, fac[h][0], s0);
+                            o = cfma(o, fac[h][1], s1);
+                            o = cfma(o, fac[h][2], s2);
+                        } else {
+#pragma unroll
+                            for (int d = 0; d < 4; d++) {
+                                const int r = c * 4 + d;
+                                o = cfma(o, Z[d], __ldg(&bk[((size_t)r * 2 + j) * 1024 + bin]));
+                            }
+                        }
+                        out[j][h] = o;
+                    }
+                }
+                if (c == 1) {
+#pragma unroll
+                    for (int j = 0; j < 2; j++) {
+                        spec[(2 * j) * kSlotStride + k] = cadd(out[j][0], out[j][1]);
+                        spec[(2 * j + 1) * kSlotStride + k] = cmulc(csub(out[j][0], out[j][1]), w4);
+                    }
+                }
+            }
+            if (c == 0) __syncthreads();
+        }
+        cluster.sync();  // every rank's quarter of slots 0-3 is written
+
+        // ---- I (every rank): gather, inverse 512-point FFT, untwist, round
+        if (warp < 4) {
+            const int j = (warp >> 1) & 1, par = warp & 1;
+            double2 v[16];
+#pragma unroll
+            for (int n2 = 0; n2 < 16; n2++)
+                v[n2] = peer[(n2 * 32) / (512 / R)][(2 * j + par) * kSlotStride + lane + 32 * n2];
+            double2* scratch = spec + (4 + 2 * j + par) * kSlotStride;  // rows d = 2, 3 are free
+            dft512_inv_raw(v, scratch, lane, psi2_at(tab, 8u * lane));
+            const int k2 = lane & 15, hh = lane >> 4;
+            const double2 u = psi2_at(tab, 2u * (uint32_t)(k2 + 256 * hh) + par);
+            uint64_t* a = acc + j * kN2;
+#pragma unroll
+            for (int m = 0; m < 16; m++) {
+                const int n = 2 * (k2 + 16 * m + 256 * hh) + par;
+                const double2 z = cmul(cmulc(v[m], u), c_utw16[m]);
+                const uint64_t lo = to_torus64(z.x * 0x1p54);
+                const uint64_t hi = to_torus64(z.y * 0x1p54);
+                if (KB) {
+                    a[n] = lo;
+                    a[n + 1024] = hi;
+                } else {
+                    a[n] += lo;
+                    a[n + 1024] += hi;
+                }
+            }
+        }
+        cluster.sync();  // the gathers are done before slots 0-3 are rewritten
+    }
+
+    if (ok && rank == 0) {
+        if (acc_out)
+            for (int i = tid; i < kTrlwe2; i += blockDim.x) acc_out[(size_t)l * kTrlwe2 + i] = acc[i];
+        if (lane_out) {
+            uint64_t* o = lane_out + (size_t)l * kTlwe2;
+            for (int i = tid; i <= kN2; i += blockDim.x)
+                o[i] = i == kN2 ? acc[kN2] : (i == 0 ? acc[0] : 0ull - acc[kN2 - i]);
+        }
+    }
+}
+
+template <bool KB, int R>
+cudaError_t launch2_clu(const uint32_t* lane_in, int lanes, uint64_t mu, const double2* bkf,
+                        const double2* psi2, int steps, uint64_t* acc_out, uint64_t* lane_out,
+                        int in_count, int mu_shift, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr[64] = {};
+    if (!attr[dev & 63]) {
+        const cudaError_t e = cudaFuncSetAttribute(
+            k_br2_fp64_clu<KB, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClu2Smem);
+        if (e != cudaSuccess) return e;
+        attr[dev & 63] = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(lanes * R);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = kClu2Smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = R;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_br2_fp64_clu<KB, R>, lane_in, lanes, mu, bkf, psi2, steps,
+                              acc_out, lane_out, in_count, mu_shift);
+}
 }  // namespace
 
 // Lanes per CTA: 1 (two CTAs per SM) unless CUFHE_BR2_LANES_PER_CTA=2 (one
@@ -356,6 +601,24 @@ cudaError_t launch_br2_fp64(bool kb, const uint32_t* lane_in, int lanes, uint64_
 {
     if (lanes <= 0) return cudaSuccess;
     if (in_count <= 0) in_count = lanes;
+    {
+        // batches that fit one cluster per SM pair: the cluster form
+        // (CUFHE_BR_CLUSTER=0 keeps one CTA per lane); a device that cannot
+        // place the clusters runs the one-CTA kernel instead
+        int sms = 148, dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const char* ce = getenv("CUFHE_BR_CLUSTER");
+        if (lanes * kClu2Ranks <= sms && !(ce && atoi(ce) == 0)) {
+            const cudaError_t r =
+                kb ? launch2_clu<true, kClu2Ranks>(lane_in, lanes, mu, bkf, psi2, steps, acc_out,
+                                                   lane_out, in_count, mu_shift, st)
+                   : launch2_clu<false, kClu2Ranks>(lane_in, lanes, mu, bkf, psi2, steps, acc_out,
+                                                    lane_out, in_count, mu_shift, st);
+            if (r == cudaSuccess) return r;
+            cudaGetLastError();
+        }
+    }
     const char* e = getenv("CUFHE_BR2_LANES_PER_CTA");
     const int g = (e && atoi(e) == 2) ? 2 : 1;
     if (g == 2)

@@ -9,10 +9,13 @@ switching: the *_lvl02 gates, src/cufhe_gates_gpu.cu:826-979), through the C-ABI
   any two FP64 implementations (the oracle's FP64 form parts from its own
   exact form the same way); parity is therefore on the phase, within
   PHASE_TOL of the oracle's, which is what decryption reads;
+* small batches (the cluster form) equal the one-CTA-per-lane form bit for bit;
 * gates: every gate id decrypts to the truth table (test/plain.h:1-70), the
   reference's test_gate_gpu_lvl02.cc check, and 65,536 random gates decrypt
   without a failure.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -66,6 +69,28 @@ def rotate(x, count, steps):
     acc = engine.from_device(d_acc, (count, P.TRLWE2_WORDS), np.uint64)
     t2 = engine.from_device(d_t2, (count, P.TLWE2_WORDS), np.uint64)
     return acc, t2
+
+
+@pytest.mark.parametrize("lanes", [1, 5, 40])
+def test_cluster_form_for_small_batches_is_bit_identical(ctx, lanes):
+    """Batches of up to SMs / 2 lanes rotate one lane per cluster of two CTAs
+    (key multiply-accumulate split over two SMs, products gathered through
+    distributed shared memory); CUFHE_BR_CLUSTER=0 keeps one CTA per lane.
+    Both give the same accumulators and extracted TLWEs bit for bit."""
+    sk, _, _ = ctx
+    _, x = lvl0(sk, lanes, 70 + lanes)
+    got = {}
+    for cluster in (False, True):
+        if cluster:
+            os.environ.pop("CUFHE_BR_CLUSTER", None)
+        else:
+            os.environ["CUFHE_BR_CLUSTER"] = "0"
+        try:
+            got[cluster] = rotate(x, lanes, -1)
+        finally:
+            os.environ.pop("CUFHE_BR_CLUSTER", None)
+    assert np.array_equal(got[True][0], got[False][0])
+    assert np.array_equal(got[True][1], got[False][1])
 
 
 def test_keyswitch20_bit_exact(ctx):
