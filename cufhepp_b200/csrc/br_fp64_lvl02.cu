@@ -21,7 +21,7 @@
 //   M  thread (bin pair, lane): radix-2 join, key MAC into registers
 //      (after the second chunk: inverse radix-2 split -> slots)
 //   I  warp (g, j, parity): inverse 512-point FFT, untwist, Torus64 rounding
-// Batches of up to SMs / 2 lanes run k_br2_fp64_clu instead: one lane per
+// Batches of up to one lane per SM run k_br2_fp64_clu instead: one lane per
 // cluster of two CTAs on two SMs, the key MAC split between them and the
 // products gathered through distributed shared memory.
 // The root table psi2^s (psi2 = e^{i pi / 2048}) keeps s in [0, 512] only
@@ -602,14 +602,15 @@ cudaError_t launch_br2_fp64(bool kb, const uint32_t* lane_in, int lanes, uint64_
     if (lanes <= 0) return cudaSuccess;
     if (in_count <= 0) in_count = lanes;
     {
-        // batches that fit one cluster per SM pair: the cluster form
-        // (CUFHE_BR_CLUSTER=0 keeps one CTA per lane); a device that cannot
-        // place the clusters runs the one-CTA kernel instead
+        // batches of up to one lane per SM (at most two rounds of clusters;
+        // measured faster than two single-lane CTAs per SM up to there): the
+        // cluster form (CUFHE_BR_CLUSTER=0 keeps one CTA per lane); a device
+        // that cannot place the clusters runs the one-CTA kernel instead
         int sms = 148, dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const char* ce = getenv("CUFHE_BR_CLUSTER");
-        if (lanes * kClu2Ranks <= sms && !(ce && atoi(ce) == 0)) {
+        if (lanes <= sms && !(ce && atoi(ce) == 0)) {
             const cudaError_t r =
                 kb ? launch2_clu<true, kClu2Ranks>(lane_in, lanes, mu, bkf, psi2, steps, acc_out,
                                                    lane_out, in_count, mu_shift, st)

@@ -71,9 +71,9 @@ def rotate(x, count, steps):
     return acc, t2
 
 
-@pytest.mark.parametrize("lanes", [1, 5, 40])
+@pytest.mark.parametrize("lanes", [1, 5, 40, 100])
 def test_cluster_form_for_small_batches_is_bit_identical(ctx, lanes):
-    """Batches of up to SMs / 2 lanes rotate one lane per cluster of two CTAs
+    """Batches of up to one lane per SM rotate one lane per cluster of two CTAs
     (key multiply-accumulate split over two SMs, products gathered through
     distributed shared memory); CUFHE_BR_CLUSTER=0 keeps one CTA per lane.
     Both give the same accumulators and extracted TLWEs bit for bit."""
