@@ -279,6 +279,10 @@ def set_precision(form: int) -> None:
     check(load().cufhe_set_precision(form), "set_precision")
 
 
+def get_precision() -> int:
+    return int(load().cufhe_get_precision())
+
+
 def gate_batch(gates, count: int, level: int, out, in0, in1=None, in2=None, stream=None,
                uniform: int = 0) -> None:
     g = None

@@ -72,3 +72,33 @@ def test_prefix_batches_reproduce_the_full_batch(form, level):
         part = engine.gate_batch_host(gates[:n], level, *(c[:n] for c in cts))
         engine.synchronize()
         assert np.array_equal(part, full[:n]), n
+
+
+def test_lvl02_prefix_batches_reproduce_the_full_batch():
+    """lvl02 gates (Ctxt<lvl0> I/O through lvl2): prefixes across the cluster
+    form's limit (one lane per SM) and the key-switch tiles give the same rows
+    as a 400-gate batch, and the full batch decrypts to its truth table."""
+    sk = client.SecretKey.generate(0xED6E)
+    prev = engine.get_precision()
+    engine.set_precision(P.FP64_FFNT)  # the KeyBundle key needs the FP64 form
+    engine.initialize_lvl02(client.EvalKey02.generate(sk, keybundle=True))
+    try:
+        rng = np.random.default_rng(7)
+        n_full = 400
+        gates = rng.choice(GATES, n_full).astype(np.int32)
+        bits = [rng.integers(0, 2, n_full).astype(np.uint8) for _ in range(3)]
+        cts = [client.encrypt_bits(sk, b, 0, seed=300 + i) for i, b in enumerate(bits)]
+        dev = [engine.to_device(c) for c in cts]
+        d_out = engine.DeviceBuffer(n_full * P.TLWE0_WORDS * 4)
+        engine.gate_batch(gates, n_full, engine.LVL02, d_out, *dev)
+        engine.synchronize()
+        full = engine.from_device(d_out, (n_full, P.TLWE0_WORDS))
+        exp = np.array([P.TRUTH[g](int(x), int(y), int(z)) for g, x, y, z in zip(gates, *bits)])
+        assert np.array_equal(client.decrypt_bits(sk, full, 0), exp)
+        for n in (1, 3, 127, 128, 129, 147, 148, 149, 200):
+            engine.gate_batch(gates[:n], n, engine.LVL02, d_out, *dev)
+            engine.synchronize()
+            assert np.array_equal(engine.from_device(d_out, (n, P.TLWE0_WORDS)), full[:n]), n
+    finally:
+        engine.cleanup_lvl02()
+        engine.set_precision(prev)
