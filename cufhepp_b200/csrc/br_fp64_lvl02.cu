@@ -21,7 +21,7 @@
 //   M  thread (bin pair, lane): radix-2 join, key MAC into registers
 //      (after the second chunk: inverse radix-2 split -> slots)
 //   I  warp (g, j, parity): inverse 512-point FFT, untwist, Torus64 rounding
-// Batches of up to one lane per SM run k_br2_fp64_clu instead: one lane per
+// Batches of up to one lane per SM pair run k_br2_fp64_clu instead: one lane per
 // cluster of two CTAs on two SMs, the key MAC split between them and the
 // products gathered through distributed shared memory.
 // The root table psi2^s (psi2 = e^{i pi / 2048}) keeps s in [0, 512] only
@@ -50,6 +50,10 @@ constexpr size_t br2_smem_bytes()
     return sizeof(double2) * G * 8 * kSlotStride + sizeof(double2) * kPsi2Entries +
            sizeof(uint64_t) * G * kTrlwe2 + sizeof(uint16_t) * G * kAbarStride2;
 }
+
+// shared memory requested per CTA: more than half an SM, so that every CTA
+// has an SM (and its whole register file) to itself
+constexpr size_t kSmemOneCta = 120 * 1024;
 
 // psi2^t for any t (mod 4096) from the table of s in [0, 512]
 __device__ __forceinline__ double2 psi2_at(const double2* tab, uint32_t t)
@@ -86,8 +90,12 @@ __device__ __forceinline__ uint64_t to_torus64(double x)
     return (i >> 63) ? 0ull - v : v;
 }
 
+// One CTA per SM (launch bound 1, and at least 120 KB of shared memory
+// requested): the transforms and the MAC want more than the 128 registers per
+// thread that two CTAs per SM would leave (2048 lanes 70.1 -> 66.2 ms, 148
+// lanes 9.2 -> 4.7 ms against two one-lane CTAs per SM).
 template <bool KB, int G>
-__global__ void __launch_bounds__(G * 256, G == 1 ? 2 : 1)
+__global__ void __launch_bounds__(G * 256, 1)
     k_br2_fp64(const uint32_t* __restrict__ lane_in, int lanes, uint64_t mu,
                const double2* __restrict__ bkf, const double2* __restrict__ psi2, int steps,
                uint64_t* __restrict__ acc_out, uint64_t* __restrict__ lane_out, int in_count,
@@ -335,7 +343,7 @@ cudaError_t launch2_g(const uint32_t* lane_in, int lanes, uint64_t mu, const dou
                       const double2* psi2, int steps, uint64_t* acc_out, uint64_t* lane_out,
                       int in_count, int mu_shift, cudaStream_t st)
 {
-    constexpr size_t smem = br2_smem_bytes<G>();
+    constexpr size_t smem = br2_smem_bytes<G>() < kSmemOneCta ? kSmemOneCta : br2_smem_bytes<G>();
     int dev = 0;
     cudaGetDevice(&dev);
     static bool attr[64] = {};
@@ -360,7 +368,7 @@ cudaError_t launch2_g(const uint32_t* lane_in, int lanes, uint64_t mu, const dou
 // from the peers' shared memory (distributed shared memory).  Per bin the
 // arithmetic is that of k_br2_fp64, so the result is bit-identical.
 constexpr int kClu2Ranks = 2;              // measured: 2 beats 4 and 8 beyond one lane
-constexpr size_t kClu2Smem = 120 * 1024;  // > half an SM: one CTA per SM
+constexpr size_t kClu2Smem = kSmemOneCta;
 static_assert(br2_smem_bytes<1>() <= kClu2Smem, "lvl2 cluster CTA layout");
 
 template <bool KB, int R>
@@ -602,15 +610,14 @@ cudaError_t launch_br2_fp64(bool kb, const uint32_t* lane_in, int lanes, uint64_
     if (lanes <= 0) return cudaSuccess;
     if (in_count <= 0) in_count = lanes;
     {
-        // batches of up to one lane per SM (at most two rounds of clusters;
-        // measured faster than two single-lane CTAs per SM up to there): the
-        // cluster form (CUFHE_BR_CLUSTER=0 keeps one CTA per lane); a device
-        // that cannot place the clusters runs the one-CTA kernel instead
+        // batches of up to one lane per SM pair: the cluster form
+        // (CUFHE_BR_CLUSTER=0 keeps one CTA per lane); a device that cannot
+        // place the clusters runs the one-CTA kernel instead
         int sms = 148, dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const char* ce = getenv("CUFHE_BR_CLUSTER");
-        if (lanes <= sms && !(ce && atoi(ce) == 0)) {
+        if (lanes * kClu2Ranks <= sms && !(ce && atoi(ce) == 0)) {
             const cudaError_t r =
                 kb ? launch2_clu<true, kClu2Ranks>(lane_in, lanes, mu, bkf, psi2, steps, acc_out,
                                                    lane_out, in_count, mu_shift, st)
