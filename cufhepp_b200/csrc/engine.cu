@@ -1197,20 +1197,20 @@ int cufhe_identity_keyswitch_lvl20(const uint64_t* tlwe2, size_t count, uint32_t
     return run_iks20(s, plan, tlwe2, tlwe0_out);
 }
 
-int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, size_t num_gates,
-                         const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
-                         const int32_t* in2, const int32_t* out, int device)
+// Validation, levelisation and balancing of a circuit on the host (no GPU):
+// wave[g] for every gate, nwaves = the critical path.  `sms` sets the
+// balancing's round of lanes (4 x sms at lvl0/lvl1, 2 x sms at lvl02).
+static int plan_waves(int level, size_t num_wires, size_t num_gates, const int32_t* gate_ops,
+                      const int32_t* in0, const int32_t* in1, const int32_t* in2,
+                      const int32_t* out, int sms, std::vector<int32_t>& wave, int& nwaves)
 {
-    if (!out_c) return fail(CUFHE_ERR_ARG, "null circuit handle");
-    *out_c = nullptr;
     if (level != CUFHE_LVL0 && level != CUFHE_LVL1 && level != CUFHE_LVL02)
         return fail(CUFHE_ERR_ARG, "bad level %d", level);
-    if (device < 0) device = 0;
-    if (device >= g_gpu_num) return fail(CUFHE_ERR_ARG, "device %d >= gpu num", device);
     if (num_gates == 0 || num_wires == 0) return fail(CUFHE_ERR_ARG, "empty circuit");
     if (num_gates > (1u << 26) || num_wires > (1u << 30))
         return fail(CUFHE_ERR_ARG, "circuit too large");
     if (!gate_ops || !in0 || !out) return fail(CUFHE_ERR_ARG, "null circuit array");
+    if (sms <= 0) sms = 148;
 
     // ---- validation: gate ids, operand and result wires, single assignment
     std::vector<int32_t> producer(num_wires, -1);
@@ -1232,8 +1232,8 @@ int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, si
         producer[out[g]] = (int32_t)g;
     }
     // ---- levelisation (Kahn): wave of a gate = 1 + latest wave of its producers
-    std::vector<int32_t> indeg(num_gates, 0), wave(num_gates, 0), head(num_gates, -1),
-        nxt, to;
+    std::vector<int32_t> indeg(num_gates, 0), head(num_gates, -1), nxt, to;
+    wave.assign(num_gates, 0);
     for (size_t g = 0; g < num_gates; g++) {
         const int op = gate_ops[g];
         const int nin = (op == kNot || op == kCopy) ? 1 : ((op == kMux || op == kNMux) ? 3 : 2);
@@ -1260,12 +1260,8 @@ int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, si
         }
     }
     if (queue.size() != num_gates) return fail(CUFHE_ERR_ARG, "the circuit has a cycle");
-    int nwaves = 0;
+    nwaves = 0;
     for (size_t g = 0; g < num_gates; g++) nwaves = wave[g] + 1 > nwaves ? wave[g] + 1 : nwaves;
-    const DeviceState& D = g_dev[device];
-    if (level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
-        return fail(CUFHE_ERR_STATE, level == CUFHE_LVL02 ? "cufhe_initialize_lvl02() not called"
-                                                         : "cufhe_initialize() not called");
     // ---- balancing: a wave of up to `cap` blind-rotation lanes costs one
     // rotation latency whatever its width, so gates with slack move out of
     // waves above `cap` into the latest later wave with room (never at or past
@@ -1273,9 +1269,6 @@ int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, si
     // consumer's wave is final when its producer moves; the number of waves
     // stays the critical path.
     {
-        int sms = 148;
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
-            sms = 148;
         const long cap = (long)(level == CUFHE_LVL02 ? 2 : 4) * sms;
         std::vector<long> load(nwaves, 0);
         for (size_t g = 0; g < num_gates; g++) load[wave[g]] += lanes_of_gate(gate_ops[g]);
@@ -1295,6 +1288,48 @@ int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, si
                 }
         }
     }
+    return CUFHE_OK;
+}
+
+int cufhe_circuit_plan(int level, size_t num_wires, size_t num_gates, const int32_t* gate_ops,
+                       const int32_t* in0, const int32_t* in1, const int32_t* in2,
+                       const int32_t* out, int sms, int32_t* wave_of_gate, int* num_waves)
+{
+    if (!wave_of_gate || !num_waves) return fail(CUFHE_ERR_ARG, "null plan output");
+    std::vector<int32_t> wave;
+    int nwaves = 0;
+    const int rc = plan_waves(level, num_wires, num_gates, gate_ops, in0, in1, in2, out, sms, wave,
+                              nwaves);
+    if (rc != CUFHE_OK) return rc;
+    for (size_t g = 0; g < num_gates; g++) wave_of_gate[g] = wave[g];
+    *num_waves = nwaves;
+    return CUFHE_OK;
+}
+
+int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, size_t num_gates,
+                         const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
+                         const int32_t* in2, const int32_t* out, int device)
+{
+    if (!out_c) return fail(CUFHE_ERR_ARG, "null circuit handle");
+    *out_c = nullptr;
+    if (level != CUFHE_LVL0 && level != CUFHE_LVL1 && level != CUFHE_LVL02)
+        return fail(CUFHE_ERR_ARG, "bad level %d", level);
+    if (device < 0) device = 0;
+    if (device >= g_gpu_num) return fail(CUFHE_ERR_ARG, "device %d >= gpu num", device);
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 148;
+    }
+    std::vector<int32_t> wave;
+    int nwaves = 0;
+    const int prc = plan_waves(level, num_wires, num_gates, gate_ops, in0, in1, in2, out, sms, wave,
+                               nwaves);
+    if (prc != CUFHE_OK) return prc;
+    const DeviceState& D = g_dev[device];
+    if (level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
+        return fail(CUFHE_ERR_STATE, level == CUFHE_LVL02 ? "cufhe_initialize_lvl02() not called"
+                                                         : "cufhe_initialize() not called");
     std::vector<std::vector<int32_t>> members(nwaves);
     for (size_t g = 0; g < num_gates; g++) members[wave[g]].push_back((int32_t)g);
 

@@ -62,6 +62,7 @@ SIGNATURES = {
     "cufhe_blind_rotate_lvl02": ([_vp, _sz, _u64, _i, _vp, _vp, _vp], _i),
     "cufhe_identity_keyswitch_lvl20": ([_vp, _sz, _vp, _vp], _i),
     "cufhe_circuit_create": ([_vp, _i, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i], _i),
+    "cufhe_circuit_plan": ([_i, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp], _i),
     "cufhe_circuit_info": ([_vp, _vp, _vp, _vp], _i),
     "cufhe_circuit_wave_sizes": ([_vp, _vp, _vp, _sz], _i),
     "cufhe_circuit_run": ([_vp, _vp, _vp, _i], _i),
@@ -328,6 +329,18 @@ def identity_keyswitch_lvl20(tlwe2, count: int, out, stream=None) -> None:
 def identity_keyswitch(tlwe1, count: int, out, stream=None) -> None:
     check(load().cufhe_identity_keyswitch(dptr(tlwe1), count, dptr(out), stream),
           "identity_keyswitch")
+
+
+def circuit_plan(level: int, num_wires: int, ops, in0, in1, in2, out, sms: int = 0):
+    """cufhe_circuit_plan: validation, levelisation into waves and balancing on
+    the host (no GPU, no keys).  Returns (wave of every gate, number of waves)."""
+    ops = np.ascontiguousarray(ops, np.int32)
+    arrs = [np.ascontiguousarray(x, np.int32) for x in (in0, in1, in2, out)]
+    wave = np.empty(ops.size, np.int32)
+    n = C.c_int()
+    check(load().cufhe_circuit_plan(level, num_wires, ops.size, _p(ops), *(_p(a) for a in arrs),
+                                    sms, _p(wave), C.byref(n)), "circuit_plan")
+    return wave, n.value
 
 
 class Circuit:

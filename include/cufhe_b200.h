@@ -242,19 +242,26 @@ int cufhe_identity_keyswitch_lvl20(const uint64_t* tlwe2, size_t count, uint32_t
  *
  * cufhe_circuit_create checks the DAG (ranges, single assignment, no cycle),
  * levelises it into waves of independent gates (a gate's wave is one more than
- * the latest wave among the gates it reads from), uploads every wave's plan
- * and wire indices once and sizes a private workspace for the widest wave.
+ * the latest wave among the gates it reads from), moves gates with slack out
+ * of waves wider than one resident round of blind rotations (4 x SMs lanes at
+ * lvl0/lvl1, 2 x SMs at lvl02) into later narrow waves without adding waves,
+ * uploads every wave's plan and wire indices once and sizes a private
+ * workspace for the widest wave.  cufhe_circuit_plan runs the same checks,
+ * levelisation and balancing on the host only (no GPU, no keys) for a given
+ * SM count (<= 0: 148) and returns each gate's wave.
  * cufhe_circuit_run runs all waves in order on `st` over the device wire
  * table `wires` ([num_wires][words of the level]); with use_graph = 1 the
  * waves are captured into one CUDA graph the first time (and again when
- * `wires` or the precision form changes) and replayed afterwards.  Runs of
- * one circuit share its workspace: do not overlap them on the GPU.  The INT8
- * form always launches directly.  Per-kernel profiling does not see graph
- * replays. */
+ * `wires` or the precision form changes) and replayed afterwards, in either
+ * precision form.  Runs of one circuit share its workspace: do not overlap
+ * them on the GPU.  Per-kernel profiling does not see graph replays. */
 typedef struct cufhe_circuit_s* cufhe_circuit_t;
 int cufhe_circuit_create(cufhe_circuit_t* c, int level, size_t num_wires, size_t num_gates,
                          const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
                          const int32_t* in2, const int32_t* out, int device);
+int cufhe_circuit_plan(int level, size_t num_wires, size_t num_gates, const int32_t* gate_ops,
+                       const int32_t* in0, const int32_t* in1, const int32_t* in2,
+                       const int32_t* out, int sms, int32_t* wave_of_gate, int* num_waves);
 int cufhe_circuit_info(cufhe_circuit_t c, int* waves, int* max_wave_gates, int* max_wave_lanes);
 /* gates and blind rotations of each wave; returns the number of waves */
 int cufhe_circuit_wave_sizes(cufhe_circuit_t c, int32_t* gates, int32_t* lanes, size_t cap);

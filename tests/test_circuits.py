@@ -1,5 +1,7 @@
 """Circuit workload generators and the circuit executor's host-side checks
-(no GPU: cufhe_circuit_create validates and levelises before it needs keys)."""
+(no GPU: cufhe_circuit_create validates and levelises before it needs keys,
+and cufhe_circuit_plan runs the validation, levelisation and wave balancing on
+the host alone)."""
 import ctypes as C
 
 import numpy as np
@@ -91,3 +93,72 @@ def test_valid_circuit_needs_keys_without_a_gpu():
     # a valid DAG passes validation and then needs the level's keys
     rc, err = create(1, 5, [P.NAND, P.XOR, P.NOT], [0, 2, 3], [1, 1, -1], [-1, -1, -1], [2, 3, 4])
     assert rc == -2 and "initialize" in err
+
+
+def lanes_of(ops):
+    ops = np.asarray(ops)
+    return np.where((ops == P.NOT) | (ops == P.COPY), 0,
+                    np.where((ops == P.MUX) | (ops == P.NMUX), 2, 1))
+
+
+def check_plan(net, level, sms):
+    """cufhe_circuit_plan's waves keep every dependency, use exactly the
+    critical path's number of waves, keep the total work, and never push a
+    wave above one resident round of lanes unless levelisation already had
+    it there (gates only move into waves with room)."""
+    asap = CI.levels(net)
+    wave, nwaves = engine.circuit_plan(level, net.num_wires, net.ops, net.in0, net.in1, net.in2,
+                                       net.out, sms)
+    assert nwaves == int(asap.max()) + 1
+    assert np.all(wave >= asap) and wave.max() == nwaves - 1
+    prod = np.full(net.num_wires, -1)
+    prod[net.out] = np.arange(net.gates)
+    for x in (net.in0, net.in1, net.in2):
+        has = (x >= 0) & (prod[np.where(x >= 0, x, 0)] >= 0)
+        src = prod[x[has]]
+        assert np.all(wave[src] < wave[has])
+    cap = (2 if level == engine.LVL02 else 4) * sms
+    lanes = lanes_of(net.ops)
+    load_asap = np.bincount(asap, weights=lanes, minlength=nwaves)
+    load = np.bincount(wave, weights=lanes, minlength=nwaves)
+    assert load.sum() == load_asap.sum()
+    assert np.all(load <= np.maximum(cap, load_asap))
+    return wave, load, cap
+
+
+@pytest.mark.parametrize("level", [engine.LVL1, engine.LVL02], ids=["lvl1", "lvl02"])
+def test_plan_balances_an_uneven_workload(level):
+    net = CI.uneven_workload(21, dags=24, adders=6, dag_gates=(50, 600), adder_width=(8, 32))
+    asap_load = np.bincount(CI.levels(net), weights=lanes_of(net.ops))
+    for sms in (8, 148):
+        _, load, cap = check_plan(net, level, sms)
+        # narrow waves (below one round) never become more numerous; with a
+        # small round (8 SMs) this workload has gates with slack for all of them
+        assert (load < cap).sum() <= (asap_load < cap).sum()
+        if sms == 8:
+            assert (asap_load < cap).sum() > 0 and (load < cap).sum() == 0
+
+
+def test_plan_moves_slack_gates_into_the_narrow_tail():
+    # a 6-gate chain beside 1400 independent gates (the GPU test's circuit)
+    width, depth = 1400, 6
+    ins = np.arange(width + 1, dtype=np.int32)
+    chain_out = width + 1 + np.arange(depth, dtype=np.int32)
+    side_out = width + 1 + depth + np.arange(width, dtype=np.int32)
+    in0 = np.concatenate([[0], chain_out[:-1], ins[:width]]).astype(np.int32)
+    in1 = np.concatenate([np.ones(depth, np.int32), ins[1:width + 1]]).astype(np.int32)
+    out = np.concatenate([chain_out, side_out]).astype(np.int32)
+    net = CI.Netlist(int(out.max()) + 1, ins, np.full(out.size, P.NAND, np.int32), in0, in1,
+                     np.full(out.size, -1, np.int32), out, out)
+    wave, load, cap = check_plan(net, engine.LVL1, 148)
+    assert cap == 592 and load.max() <= cap
+    # latest waves first: the last wave fills up to the round, then the one before
+    assert load[-1] == cap and load[0] == cap
+    assert np.all(wave[:depth] == np.arange(depth))  # the chain itself does not move
+
+
+def test_plan_reports_the_same_errors_as_create():
+    with pytest.raises(RuntimeError, match="cycle"):
+        engine.circuit_plan(engine.LVL1, 4, [P.NAND, P.NAND], [0, 3], [1, 1], [-1, -1], [2, 3], 148)
+    with pytest.raises(RuntimeError, match="written by gates"):
+        engine.circuit_plan(engine.LVL1, 4, [P.NAND, P.AND], [0, 0], [1, 1], [-1, -1], [2, 2], 148)
