@@ -113,6 +113,9 @@ __global__ void __launch_bounds__(256) k_i8_decompose(const uint32_t* __restrict
                                                       const uint16_t* __restrict__ abar, int lanes,
                                                       int step, uint8_t* __restrict__ tiles)
 {
+    // launched as a programmatic dependent of the previous step's GEMM: wait
+    // for its accumulator updates before reading the accumulator
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int l = blockIdx.x;
     if (l >= lanes) return;
     const uint32_t ab = abar[(size_t)l * 640 + step];
@@ -283,6 +286,9 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
                 mbar_expect_tx(bar_v, (uint32_t)kSmemPV);
                 bulk_g2s(vs, vkey + (size_t)j_out * kVBytesJ, (uint32_t)kSmemPV, bar_v);
             }
+            // the key window above is constant; the digit tiles are the
+            // previous kernel's output (programmatic dependent launch)
+            asm volatile("griddepcontrol.wait;" ::: "memory");
             int gbase = 0;
             for (int it = 0; it < T && !s_fail; it++) {
                 int t, k0, nk;
@@ -383,6 +389,7 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
         // ties a warp to quadrant warp % 4), accumulator columns [64 p, 64 p + 64)
         const int d = warp - 10, q = warp & 3, p = d >> 2;
         const uint32_t lane_base = (uint32_t)(32 * q) << 16;
+        asm volatile("griddepcontrol.wait;" ::: "memory");
         bool ok = true;
         for (int it = 0; it < T && ok; it++) {
             if (__any_sync(0xffffffffu, s_fail != 0) ||
@@ -545,7 +552,21 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
     k_i8_init<<<lanes, 256, 0, st>>>(lane_in, lanes, mu, w.abar, w.acc);
     int n = 1;
     for (int i = 0; i < nsteps; i++) {
-        k_i8_decompose<<<lanes, 256, 0, st>>>(w.acc, w.abar, lanes, i, (uint8_t*)w.digits);
+        // both kernels are programmatic dependents of the one before: each
+        // starts (TMEM, barriers, key window) while the previous one drains
+        cudaLaunchAttribute pdl[1];
+        pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        pdl[0].val.programmaticStreamSerializationAllowed = 1;
+        {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(lanes);
+            cfg.blockDim = dim3(256);
+            cfg.stream = st;
+            cfg.attrs = pdl;
+            cfg.numAttrs = 1;
+            cudaLaunchKernelEx(&cfg, k_i8_decompose, (const uint32_t*)w.acc, (const uint16_t*)w.abar,
+                               lanes, i, (uint8_t*)w.digits);
+        }
         const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * kVBytesStep;
         // even grid: CTA b serves output polynomial b & 1
         const int tiles_j = groups * (kN / kRowsCoef);
@@ -555,8 +576,17 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
         int split = 1;
         while (rem && split < 8 && rem * split * 2 <= ncj) split *= 2;
         const int units = tiles_j < ncj ? tiles_j * split : ncj;
-        k_i8_gemm_p<<<2 * units, kGemmPThreads, kSmemGemmP, st>>>(vk, (const uint8_t*)w.digits, w.acc,
-                                                               lanes, tiles_j, split, err);
+        {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(2 * units);
+            cfg.blockDim = dim3(kGemmPThreads);
+            cfg.dynamicSmemBytes = kSmemGemmP;
+            cfg.stream = st;
+            cfg.attrs = pdl;
+            cfg.numAttrs = 1;
+            cudaLaunchKernelEx(&cfg, k_i8_gemm_p, vk, (const uint8_t*)w.digits, w.acc, lanes, tiles_j,
+                               split, err);
+        }
         n += 2;
     }
     k_i8_extract<<<lanes, 256, 0, st>>>(w.acc, lanes, acc_out, lane_out);

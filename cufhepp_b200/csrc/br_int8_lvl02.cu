@@ -146,6 +146,9 @@ __global__ void __launch_bounds__(256) k_i82_decompose(const uint64_t* __restric
                                                        int lanes, int step,
                                                        uint8_t* __restrict__ tiles)
 {
+    // launched as a programmatic dependent of the previous step's GEMM: wait
+    // for its accumulator updates before reading the accumulator
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int l = blockIdx.x;
     if (l >= lanes) return;
     const uint32_t ab = abar[(size_t)l * kAbarStride + step];
@@ -273,6 +276,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_i82_gemm(const int8_t* __re
     if (warp == 9) {
         // ---- digit-chunk producer
         if (lane == 0) {
+            // the digit tiles are the previous kernel's output (programmatic
+            // dependent launch)
+            asm volatile("griddepcontrol.wait;" ::: "memory");
             for (int it = 0; it < T && !s_fail; it++) {
                 const int group = (cb + (it >> 1) * ncj) / kNBlocks;
                 const uint8_t* gt = tiles + (size_t)group * kChunks2 * kTileBytes;
@@ -400,6 +406,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_i82_gemm(const int8_t* __re
         // digit limbs (columns 32 p + i and 128 + 32 p + i)
         const int d = warp - 10, q = warp & 3, p = d >> 2;
         const uint32_t lane_base = (uint32_t)(32 * q) << 16;
+        asm volatile("griddepcontrol.wait;" ::: "memory");
         bool ok = true;
         for (int it = 0; it < T && ok; it++) {
             const int blk = cb + (it >> 1) * ncj, lg = it & 1;
@@ -572,10 +579,25 @@ cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t*
     k_i82_init<<<lanes, 256, 0, st>>>(lane_in, lanes, mu, w.abar, w.acc);
     int n = 1;
     for (int i = 0; i < nsteps; i++) {
-        k_i82_decompose<<<lanes, 256, 0, st>>>(w.acc, w.abar, lanes, i, (uint8_t*)w.digits);
+        // both kernels are programmatic dependents of the one before: each
+        // starts (TMEM, barriers, key windows) while the previous one drains
+        cudaLaunchAttribute pdl[1];
+        pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        pdl[0].val.programmaticStreamSerializationAllowed = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(lanes);
+        cfg.blockDim = dim3(256);
+        cfg.stream = st;
+        cfg.attrs = pdl;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_i82_decompose, (const uint64_t*)w.acc, (const uint16_t*)w.abar,
+                           lanes, i, (uint8_t*)w.digits);
         const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * kVStep;
-        k_i82_gemm<<<grid, kGemmThreads, kSmemGemm, st>>>(vk, (const uint8_t*)w.digits, w.acc,
-                                                         lanes, blocks_j, err);
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(kGemmThreads);
+        cfg.dynamicSmemBytes = kSmemGemm;
+        cudaLaunchKernelEx(&cfg, k_i82_gemm, vk, (const uint8_t*)w.digits, w.acc, lanes, blocks_j,
+                           err);
         n += 2;
     }
     k_i82_extract<<<lanes, 256, 0, st>>>(w.acc, lanes, acc_out, lane_out);
