@@ -15,12 +15,17 @@ C-ABI.  A MUX needs two blind rotations, so the unit is bootstraps/s
          batch's copies overlap the previous batch's bootstrapping
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W]
-                       [--path fp64|int8|both] [--impl ours|reference]
-The default measures both precision forms on the same batch (FP64 FFNT is the
-headline `value`; each form's numbers are under `paths`), then the
-sub-workloads (uneven circuits, circuit bootstrapping + lookup tables, lvl02).
-Under torchrun each rank runs its own batch on its own GPU (weak scaling, no
-data-path collective: gates are independent).
+                       [--path all|fp64_kb|fp64_plain|int8_kb|int8_plain]
+                       [--impl ours|reference]
+The default measures both precision forms with both bootstrapping-key forms
+on the same batch (FP64 FFNT with the KeyBundle key is the headline `value`;
+each form's numbers are under `paths`, and `int8_vs_fp64` compares the two
+precision forms on the same key form), then 1000 random NAND pairs with the
+plain key (`nand1000`, with the CPU port timed on the same pairs), the FP64
+form's rounding error against the exact form at lvl1 (`fp64_error_lvl1`),
+and the sub-workloads (uneven circuits, circuit bootstrapping + lookup
+tables, lvl02).  Under torchrun each rank runs its own batch on its own GPU
+(weak scaling, no data-path collective: gates are independent).
 """
 from __future__ import annotations
 
@@ -46,7 +51,13 @@ GATE_SET = [0, 4, 1, 8, 9, 12]  # NAND, AND, OR, XOR, XNOR, MUX
 A100_PUBLISHED = 1.0 / 0.12e-3   # reference README: 0.12 ms/gate, lvl1 NAND FP64 + KeyBundle
 # algorithmic work per bootstrap (lvl1): FP64 FFNT flops, INT8 tensor ops
 FLOP_FP64 = {True: 287_744 * 318, False: 189_440 * 636}
-OPS_INT8 = {False: 2 * 636 * 4096 * 8192}
+# INT8: 2 ops per MAC x K = 4096 (4 digit rows x 1024) x M = 8192 (2 polys x
+# 1024 coefficients x 4 key limbs) per GEMM; 636 GEMMs (plain) or 318 pairs x
+# 3 keys (KeyBundle)
+OPS_INT8 = {False: 2 * 636 * 4096 * 8192, True: 2 * 318 * 3 * 4096 * 8192}
+PATHS = {"fp64_kb": ("fp64", True), "fp64_plain": ("fp64", False),
+         "int8_kb": ("int8", True), "int8_plain": ("int8", False)}
+NAND_PAIRS = 1000  # configs: plain lvl1 NAND, FP64 FFNT, no KeyBundle
 # lvl2 (N = 2048, 1024-point transforms, 8 digit rows): per KeyBundle step
 # 10 transforms x 5*1024*10 + twist/untwist 10*1024*6 + combine/MAC 8*2*1024*32
 FLOP_FP64_LVL2_KB = (10 * 51_200 + 61_440 + 524_288) * 318
@@ -66,7 +77,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--batch", type=int, default=4096)
-    ap.add_argument("--path", choices=["fp64", "int8", "both"], default="both")
+    ap.add_argument("--path", choices=["all"] + list(PATHS), default="all")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -75,6 +86,10 @@ def parse():
                     help="skip the lvl0->lvl2 NAND batches reported under the 'lvl02' key")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the uneven-circuit workload reported under the 'uneven' key")
+    ap.add_argument("--no-nand1000", action="store_true",
+                    help="skip the 1000 random NAND pairs (plain key) under the 'nand1000' key")
+    ap.add_argument("--no-error", action="store_true",
+                    help="skip the lvl1 FP64-vs-exact error figures ('fp64_error_lvl1' key)")
     ap.add_argument("--no-cb", action="store_true",
                     help="skip the circuit-bootstrapping + lookup-table workload ('cb_lut' key)")
     ap.add_argument("--no-autotune", action="store_true",
@@ -97,6 +112,15 @@ def make_workload(rng, batch):
 
 def bootstraps(gates):
     return int(gates.size + np.count_nonzero(gates == 12))
+
+
+def common_config(batch, nb):
+    """The `config` of both arms (same workload, same keys, same units)."""
+    return {"workload": WORKLOAD, "gates_per_step": batch, "bootstraps_per_step": nb,
+            "keybundle": True,
+            "l2": ("GPU arm: flushed between timed steps (256 MiB write); CPU arm: no flush "
+                   "(the keys exceed the host caches)"),
+            "parallelism": "replicas: an independent gate batch per GPU"}
 
 
 def max_over_ranks(torch, x: float, device) -> float:
@@ -165,29 +189,29 @@ class Clocks:
 
 
 # ----------------------------------------------------------- reference arm ---
-def cpu_gate_rate(seconds, seed, sample_gates=None):
-    """Oracle port of the reference's CPU gate (FP64 FFNT restatement,
-    KeyBundle), OpenMP over gates on all host cores; bounded sample."""
+def cpu_gate_rate(seed, batch, keybundle=True):
+    """Oracle port of the reference's CPU gate (FP64 FFNT restatement),
+    OpenMP over gates on all host cores: the bench's own gate batch (same
+    seed, size and gate mix as the GPU arm), timed once."""
     from cufhepp_b200 import client
     from oracle import oracle as O
     sk = client.SecretKey.generate(seed)
-    ek = client.EvalKey.generate(sk, keybundle=True)
+    ek = client.EvalKey.generate(sk, keybundle=keybundle)
     fft = O.FFT()
     bkf = O.bk_to_fft(fft, ek.bk)
     cores = os.cpu_count() or 1
-    n = sample_gates or max(8, cores) * 2
     rng = np.random.default_rng(seed)
-    gates, a, b, c = make_workload(rng, n)
+    gates, a, b, c = make_workload(rng, batch)
     cts = [client.encrypt_bits(sk, x, 1, seed=seed + i) for i, x in enumerate((a, b, c))]
-    done = 0
+    n_warm = min(batch, 2 * cores)
+    O.gate_batch(gates[:n_warm], 1, *(x[:n_warm] for x in cts), bkf, ek.ksk, keybundle, O.FP64,
+                 fft)
     t0 = time.perf_counter()
-    while True:
-        O.gate_batch(gates, 1, *cts, bkf, ek.ksk, True, O.FP64, fft)
-        done += bootstraps(gates)
-        el = time.perf_counter() - t0
-        if el >= seconds:
-            break
-    return done / el, cores, f"{n}-gate batches of the same mix, repeated for {el:.1f} s"
+    O.gate_batch(gates, 1, *cts, bkf, ek.ksk, keybundle, O.FP64, fft)
+    el = time.perf_counter() - t0
+    return bootstraps(gates) / el, cores, (
+        f"the full {batch}-gate batch of the workload ({bootstraps(gates)} bootstraps), once, "
+        f"{el:.1f} s; FP64 FFNT, {'KeyBundle' if keybundle else 'plain'} key")
 
 
 def cpu_gate2_rate(seconds, seed):
@@ -218,11 +242,15 @@ def cpu_gate2_rate(seconds, seed):
 
 
 def run_reference(args):
+    """The reference's CPU gate (oracle port: TFHEpp, which the reference's
+    CPU path calls, is absent) on the workload of our arm: every timed step
+    is the whole --batch gate batch of the same seed and mix, KeyBundle key,
+    OpenMP over gates on all host threads.  Warm-up steps run a short prefix
+    of the batch (they only spin up the threads and fault in the key)."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    n = max(8, cores) * 2
     from cufhepp_b200 import client
     from oracle import oracle as O
     sk = client.SecretKey.generate(args.seed)
@@ -230,31 +258,45 @@ def run_reference(args):
     fft = O.FFT()
     bkf = O.bk_to_fft(fft, ek.bk)
     rng = np.random.default_rng(args.seed)
-    gates, a, b, c = make_workload(rng, n)
+    gates, a, b, c = make_workload(rng, args.batch)
     cts = [client.encrypt_bits(sk, x, 1, seed=args.seed + i) for i, x in enumerate((a, b, c))]
+    n_warm = min(args.batch, 2 * cores)
     for _ in range(args.warmup):
-        O.gate_batch(gates, 1, *cts, bkf, ek.ksk, True, O.FP64, fft)
+        O.gate_batch(gates[:n_warm], 1, *(x[:n_warm] for x in cts), bkf, ek.ksk, True, O.FP64,
+                     fft)
     times = []
     for _ in range(args.steps):
         t = time.perf_counter()
         O.gate_batch(gates, 1, *cts, bkf, ek.ksk, True, O.FP64, fft)
         times.append(time.perf_counter() - t)
-    value = bootstraps(gates) * args.steps / sum(times)
-    sample = (f"{n}-gate sample of the workload's gate mix per step (FP64 FFNT, KeyBundle), "
-              f"OpenMP over gates on {cores} host threads")
+    nb = bootstraps(gates)
+    value = nb * args.steps / sum(times)
+    sample = (f"the full {args.batch}-gate batch ({nb} bootstraps) every step (FP64 FFNT, "
+              f"KeyBundle), OpenMP over gates on {cores} host threads; warm-up steps run a "
+              f"{n_warm}-gate prefix")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: seeded keys, random bits", "impl": "reference",
-        "config": {"workload": WORKLOAD, "gates_per_step": n, "keybundle": True,
-                   "path": "cpu: oracle port of the reference algorithm (reference not buildable: "
-                           "TFHEpp submodule absent)"},
+        "config": common_config(args.batch, nb),
+        "impl_detail": ("cpu: oracle port of the reference algorithm (reference not buildable: "
+                        "TFHEpp submodule absent)"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": sample},
+                         "sample": sample, "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 # -------------------------------------------------------------- our arm ---
@@ -267,11 +309,14 @@ def ncu_traffic(kernel: str):
     return None
 
 
-def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, flush):
+def run_path(args, path, torch, engine, client, P, sk, workload, rank, ws, flush):
+    """One precision form with one bootstrapping-key form (PATHS[path]) on the
+    bench's gate batch."""
     gates, a, b, c = workload
-    kb = ek.keybundle
+    form, kb = PATHS[path]
+    ek = client.EvalKey.generate(sk, keybundle=kb)
     engine.initialize(ek)
-    engine.set_precision(P.FP64_FFNT if path == "fp64" else P.INT8_EXACT)
+    engine.set_precision(P.FP64_FFNT if form == "fp64" else P.INT8_EXACT)
     level = 1
     words = P.TLWE1_WORDS
     B = gates.size
@@ -404,12 +449,12 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
 
     engine.cleanup()
 
-    br = "br_fp64" if path == "fp64" else "br_int8"
+    br = "br_fp64" if form == "fp64" else "br_int8"
     rl = None
     if br in kern:
         ms, n = kern[br]
         per_launch_s = ms * 1e-3 / n
-        if path == "fp64":
+        if form == "fp64":
             work = FLOP_FP64[bool(kb)] * nb
             peak = engine_peak_fp64(engine)
             rl = {"bound": "fp64", "achieved": work / per_launch_s / 1e12, "peak": peak,
@@ -420,12 +465,13 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
                   "peak_source": "measured FP64 FMA probe on this GPU "
                                  "(cufhe_measure_fp64_peak; the peaks file has no FP64 figure)"}
         else:
-            work = OPS_INT8[False] * nb
+            work = OPS_INT8[bool(kb)] * nb
             peak = engine_peak_int8(engine)
             rl = {"bound": "tensor", "achieved": work / per_launch_s / 1e12, "peak": peak,
                   "unit": "TOP/s", "frac": work / per_launch_s / 1e12 / peak,
-                  "traffic": ncu_traffic("br_int8"),
-                  "kernel": "INT8 blind rotation (decompose + tcgen05 Toeplitz GEMM per step)",
+                  "traffic": ncu_traffic("br_int8_kb" if kb else "br_int8"),
+                  "kernel": ("INT8 blind rotation (decompose + tcgen05 Toeplitz GEMM per " +
+                             ("KeyBundle pair, three keys)" if kb else "CMUX step)")),
                   "work_per_launch": work,
                   "peak_source": "measured tcgen05.mma.kind::i8 M128 N256 K32 probe on this GPU "
                                  "(cufhe_measure_int8_peak, random operands; the peaks file has "
@@ -443,6 +489,138 @@ def run_path(args, path, torch, engine, client, P, sk, ek, workload, rank, ws, f
         "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()},
         "roofline": rl, "clocks": clocks, "bootstraps_per_step": nb, "keybundle": bool(kb),
     }
+    return res
+
+
+def run_nand1000(args, torch, engine, client, P, sk, rank, ws, flush):
+    """configs: plain lvl1 NAND gate bootstrapping, FP64 FFNT, no KeyBundle:
+    1000 uniform random bit pairs encrypted at +-1/8 (Ctxt<lvl1>, key
+    switching then blind rotation), as one batch per step: device-resident
+    inputs, CUDA events per step, L2 flushed between steps; the same through
+    host buffers (e2e); a single NAND on the idle GPU; and the CPU port of the
+    reference's gate timed on the same 1000 pairs."""
+    from oracle import oracle as O
+    ek = client.EvalKey.generate(sk, keybundle=False)
+    engine.initialize(ek)
+    engine.set_precision(P.FP64_FFNT)
+    rng = np.random.default_rng(args.seed + 1000 + rank)
+    n = NAND_PAIRS
+    a, b = (rng.integers(0, 2, n).astype(np.uint8) for _ in range(2))
+    cts = [client.encrypt_bits(sk, x, 1, seed=args.seed + 1100 + i) for i, x in enumerate((a, b))]
+    din = [engine.to_device(x) for x in cts]
+    dout = engine.DeviceBuffer(n * P.TLWE1_WORDS * 4)
+    gates = np.zeros(n, np.int32)
+
+    def step():
+        engine.gate_batch(None, n, 1, dout, *din, uniform=P.NAND)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    fails = int(np.count_nonzero(
+        client.decrypt_bits(sk, engine.from_device(dout, (n, P.TLWE1_WORDS)), 1) != 1 - (a & b)))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        ev[k][0].record()
+        step()
+        ev[k][1].record()
+        flush.zero_()
+    torch.cuda.synchronize()
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    total = max_over_ranks(torch, sum(step_ms), "cuda")
+    # e2e: host buffers, H2D and D2H inside each timed step
+    host_out = np.empty((n, P.TLWE1_WORDS), np.uint32)
+    e2e = []
+    for k in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        engine.gate_batch_host(gates, 1, cts[0], cts[1], cts[1], out=host_out)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e.append(e0.elapsed_time(e1))
+        flush.zero_()
+    fails += int(np.count_nonzero(client.decrypt_bits(sk, host_out, 1) != 1 - (a & b)))
+    e2e_total = max_over_ranks(torch, sum(e2e), "cuda")
+    lat = []
+    L = engine.load()
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        engine.check(L.cufhe_gate(P.NAND, 1, engine.dptr(dout), engine.dptr(din[0]),
+                                  engine.dptr(din[1]), None, None), "gate")
+        e1.record()
+        torch.cuda.synchronize()
+        lat.append(e0.elapsed_time(e1))
+    engine.cleanup()
+    out = {"metric": "lvl1 NAND bootstraps/s (1000 random pairs per batch)", "unit": UNIT,
+           "workload": (f"{n} uniform random NAND bit pairs at +-1/8, Ctxt<lvl1> I/O, FP64 FFNT, "
+                        "plain bootstrapping key (no KeyBundle), one batch per step"),
+           "value": whole_job_rate(n, ws, args.steps, total), "ms_per_step": total / args.steps,
+           "p50_batch_latency_ms": statistics.median(step_ms),
+           "single_gate_latency_ms": statistics.median(lat),
+           "e2e": {"value": whole_job_rate(n, ws, args.steps, e2e_total), "unit": UNIT,
+                   "h2d_bytes_per_step": int(cts[0].nbytes + cts[1].nbytes),
+                   "d2h_bytes_per_step": int(host_out.nbytes)},
+           "decrypt_failures": fails, "gates_checked": 2 * n, "dtype": "f64"}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        fft = O.FFT()
+        bkf = O.bk_to_fft(fft, ek.bk)
+        O.gate_batch(gates[:16], 1, cts[0][:16], cts[1][:16], None, bkf, ek.ksk, False, O.FP64,
+                     fft)
+        t0 = time.perf_counter()
+        ref = O.gate_batch(gates, 1, cts[0], cts[1], None, bkf, ek.ksk, False, O.FP64, fft)
+        el = time.perf_counter() - t0
+        cpu_fails = int(np.count_nonzero(client.decrypt_bits(sk, ref, 1) != 1 - (a & b)))
+        out["cpu_baseline"] = {"value": n / el, "unit": UNIT, "cores": os.cpu_count() or 1,
+                               "kind": "port", "cpu_model": cpu_model(),
+                               "sample": f"the same {n} NAND pairs, once ({el:.2f} s), FP64 FFNT, "
+                                         "plain key, OpenMP over gates",
+                               "decrypt_failures": cpu_fails}
+    return out
+
+
+def fp64_error_lvl1(args, engine, client, P, sk, count=64):
+    """The FP64 form's rounding against the exact product at lvl1, per key
+    form: both forms rotate the same `count` lvl0 inputs (the exact INT8 form
+    is bit-identical to the schoolbook oracle); reported are the largest
+    coefficient difference after one step (CMUX step or KeyBundle pair), and
+    after the full rotation the largest coefficient difference and the
+    largest phase difference (Torus32 units).  Over a full rotation the two
+    ciphertexts part ways once a +-1 difference changes a gadget digit, so
+    there only the phase is a rounding figure."""
+    rng = np.random.default_rng(args.seed + 2000)
+    bits = rng.integers(0, 2, count).astype(np.uint8)
+    x = client.encrypt_bits(sk, bits, 0, seed=args.seed + 2001)
+    d_x = engine.to_device(x)
+    d_acc = engine.DeviceBuffer(count * P.TRLWE1_WORDS * 4)
+    res = {"inputs": count, "unit": "Torus32 units (2^-32)"}
+    for kb in (True, False):
+        engine.initialize(client.EvalKey.generate(sk, keybundle=kb))
+        accs = {}
+        try:
+            for form, prec in (("exact", P.INT8_EXACT), ("fp64", P.FP64_FFNT)):
+                engine.set_precision(prec)
+                for steps in (1, -1):
+                    engine.blind_rotate(d_x, count, P.MU32, steps, acc_out=d_acc)
+                    accs[form, steps] = engine.from_device(d_acc, (count, P.TRLWE1_WORDS)).copy()
+        finally:
+            engine.set_precision(P.FP64_FFNT)
+            engine.cleanup()
+
+        def coef(a_, b_):
+            return int(np.abs((a_ - b_).astype(np.uint32).view(np.int32).astype(np.int64)).max())
+        ph = max(int(np.abs((client.trlwe_phase(sk, accs["fp64", -1][i]) -
+                             client.trlwe_phase(sk, accs["exact", -1][i])).astype(np.uint32)
+                            .view(np.int32).astype(np.int64)).max()) for i in range(count))
+        res["kb" if kb else "plain"] = {
+            "one_step_max_coef_diff": coef(accs["fp64", 1], accs["exact", 1]),
+            "full_rotation_max_coef_diff": coef(accs["fp64", -1], accs["exact", -1]),
+            "full_rotation_max_phase_diff": ph,
+            "full_rotation_max_phase_diff_log2": float(np.log2(max(ph, 1)))}
     return res
 
 
@@ -785,7 +963,7 @@ def run_ours(args):
     rng = np.random.default_rng(args.seed + rank)
     workload = make_workload(rng, args.batch)
     sk = client.SecretKey.generate(args.seed)
-    paths = ["fp64", "int8"] if args.path == "both" else [args.path]
+    paths = list(PATHS) if args.path == "all" else [args.path]
     tuned = None
     if not args.no_autotune:
         ek_t = client.EvalKey.generate(sk, keybundle=True)
@@ -794,18 +972,23 @@ def run_ours(args):
         engine.cleanup()
     results = {}
     for p in paths:
-        ek = client.EvalKey.generate(sk, keybundle=(p == "fp64"))
-        results[p] = run_path(args, p, torch, engine, client, P, sk, ek, workload, rank, ws, flush)
-    primary = results[paths[0]]
-    # the sub-workloads (uneven circuits, circuit bootstrapping, lvl02) are
-    # measured by a single process (N = 1); under torchrun every rank runs the
-    # headline batch only
+        results[p] = run_path(args, p, torch, engine, client, P, sk, workload, rank, ws, flush)
+    primary_name = paths[0]
+    primary = results[primary_name]
+    # the sub-workloads are measured by a single process (N = 1); under
+    # torchrun every rank runs the headline batch only
     single = ws == 1
+    nand = None
+    if not args.no_nand1000 and single:
+        nand = run_nand1000(args, torch, engine, client, P, sk, rank, ws, flush)
+    err = None
+    if not args.no_error and single:
+        err = fp64_error_lvl1(args, engine, client, P, sk)
     uneven = None
     if not args.no_uneven and single:
         ek_u = client.EvalKey.generate(sk, keybundle=True)
         uneven = run_uneven(args, torch, engine, client, P, sk, ek_u, rank, ws, flush,
-                            results["fp64"]["value"] if "fp64" in results else None)
+                            results["fp64_kb"]["value"] if "fp64_kb" in results else None)
     cb = None
     if not args.no_cb and single:
         cb = run_cb(args, torch, engine, client, P, sk, client.EvalKey.generate(sk, keybundle=True),
@@ -815,23 +998,23 @@ def run_ours(args):
         lvl02 = run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_gate_rate(args.cpu_seconds, args.seed)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        v, cores, sample = cpu_gate_rate(args.seed, args.batch, keybundle=PATHS[primary_name][1])
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+               "cpu_model": cpu_model()}
         if lvl02 is not None:
             lvl02["cpu_baseline"] = cpu_gate2_rate(min(args.cpu_seconds, 8.0), args.seed)
     if rank == 0:
+        form, kb = PATHS[primary_name]
         line = {
             "metric": METRIC, "value": primary["value"], "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": primary["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if paths[0] == "fp64" else "int8",
+            "dtype": "f64" if form == "fp64" else "int8",
             "data": "synthetic: seeded keys, random bits",
-            "config": {"workload": WORKLOAD, "gates_per_step": args.batch,
-                       "bootstraps_per_step": primary["bootstraps_per_step"],
-                       "keybundle": primary["keybundle"],
-                       "path": {"fp64": "FP64 FFNT", "int8": "INT8 exact (tcgen05)"}[paths[0]],
-                       "l2": "flushed between timed steps (256 MiB write)",
-                       "parallelism": f"{ws} replica(s): independent gate batch per GPU"},
+            "config": common_config(args.batch, primary["bootstraps_per_step"]),
+            "headline_path": {"name": primary_name,
+                              "form": {"fp64": "FP64 FFNT", "int8": "INT8 exact (tcgen05)"}[form],
+                              "keybundle": kb},
             "p50_gate_latency_ms": primary["p50_gate_latency_ms"],
             "p99_gate_latency_ms": primary["p99_gate_latency_ms"],
             "single_gate_latency_ms": primary["single_gate_latency_ms"],
@@ -841,6 +1024,22 @@ def run_ours(args):
             "kernel_ms_per_step": primary["kernel_ms_per_step"],
             "vs_reference_a100_published": primary["value"] / A100_PUBLISHED,
         }
+        line["config"]["keybundle"] = kb
+        if len(paths) > 1:
+            line["paths"] = {p: {k: results[p][k] for k in
+                                 ("value", "ms_per_step", "p50_gate_latency_ms",
+                                  "single_gate_latency_ms", "decrypt_failures", "roofline",
+                                  "kernel_ms_per_step", "keybundle", "e2e", "gpu_launches")}
+                             for p in paths}
+            ratio = {}
+            for tag in ("kb", "plain"):
+                if f"int8_{tag}" in results and f"fp64_{tag}" in results:
+                    ratio[tag] = results[f"int8_{tag}"]["value"] / results[f"fp64_{tag}"]["value"]
+            line["int8_vs_fp64"] = ratio
+        if nand is not None:
+            line["nand1000"] = nand
+        if err is not None:
+            line["fp64_error_lvl1"] = err
         if lvl02 is not None:
             line["lvl02"] = lvl02
         if uneven is not None:
@@ -848,16 +1047,11 @@ def run_ours(args):
         if cb is not None:
             line["cb_lut"] = cb
         if not single:
-            line["sub_workloads"] = "measured at N = 1 only (uneven, cb_lut, lvl02)"
-        line["config"]["br_lanes_per_cta"] = (
+            line["sub_workloads"] = ("measured at N = 1 only (nand1000, fp64_error_lvl1, uneven, "
+                                     "cb_lut, lvl02)")
+        line["br_lanes_per_cta"] = (
             {"source": "autotuner (cufhe_autotune)", "table": tuned} if tuned
             else {"source": "built-in rule"})
-        if len(paths) > 1:
-            line["paths"] = {p: {k: results[p][k] for k in
-                                 ("value", "ms_per_step", "p50_gate_latency_ms",
-                                  "single_gate_latency_ms", "decrypt_failures", "roofline",
-                                  "kernel_ms_per_step", "keybundle", "e2e", "gpu_launches")}
-                             for p in paths}
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.barrier()

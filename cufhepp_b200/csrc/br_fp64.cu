@@ -281,14 +281,10 @@ cudaError_t launch_g(const uint32_t* lane_in, int lanes, uint32_t mu, const doub
                      cudaStream_t st)
 {
     constexpr size_t smem = br_smem_bytes<G>();
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr[64] = {};
-    if (!attr[dev & 63]) {
-        cudaError_t e = cudaFuncSetAttribute(k_br_fp64<KB, G>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static DeviceAttrFlags attr;
+    {
+        const cudaError_t e = set_smem_attr_once(attr, k_br_fp64<KB, G>, smem);
         if (e != cudaSuccess) return e;
-        attr[dev & 63] = true;
     }
     const int blocks = (lanes + G - 1) / G;
     k_br_fp64<KB, G><<<blocks, G * 128, smem, st>>>(lane_in, lanes, mu, bkf, t.psi, t.tw512, steps,
@@ -490,14 +486,10 @@ cudaError_t launch_clu(const uint32_t* lane_in, int lanes, uint32_t mu, const do
                        const Fp64Tables& t, int steps, uint32_t* acc_out, uint32_t* lane_out,
                        cudaStream_t st)
 {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr[64] = {};
-    if (!attr[dev & 63]) {
-        cudaError_t e = cudaFuncSetAttribute(k_br_fp64_clu<KB>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCluSmem);
+    static DeviceAttrFlags attr;
+    {
+        const cudaError_t e = set_smem_attr_once(attr, k_br_fp64_clu<KB>, kCluSmem);
         if (e != cudaSuccess) return e;
-        attr[dev & 63] = true;
     }
     k_br_fp64_clu<KB><<<lanes * kCluRanks, 128, kCluSmem, st>>>(lane_in, lanes, mu, bkf, t.psi, steps,
                                                               acc_out, lane_out);

@@ -344,14 +344,10 @@ cudaError_t launch2_g(const uint32_t* lane_in, int lanes, uint64_t mu, const dou
                       int in_count, int mu_shift, cudaStream_t st)
 {
     constexpr size_t smem = br2_smem_bytes<G>() < kSmemOneCta ? kSmemOneCta : br2_smem_bytes<G>();
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr[64] = {};
-    if (!attr[dev & 63]) {
-        cudaError_t e = cudaFuncSetAttribute(k_br2_fp64<KB, G>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static DeviceAttrFlags attr;
+    {
+        const cudaError_t e = set_smem_attr_once(attr, k_br2_fp64<KB, G>, smem);
         if (e != cudaSuccess) return e;
-        attr[dev & 63] = true;
     }
     const int blocks = (lanes + G - 1) / G;
     k_br2_fp64<KB, G><<<blocks, G * 256, smem, st>>>(lane_in, lanes, mu, bkf, psi2, steps, acc_out,
@@ -575,14 +571,10 @@ cudaError_t launch2_clu(const uint32_t* lane_in, int lanes, uint64_t mu, const d
                         const double2* psi2, int steps, uint64_t* acc_out, uint64_t* lane_out,
                         int in_count, int mu_shift, cudaStream_t st)
 {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr[64] = {};
-    if (!attr[dev & 63]) {
-        const cudaError_t e = cudaFuncSetAttribute(
-            k_br2_fp64_clu<KB, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClu2Smem);
+    static DeviceAttrFlags attr;
+    {
+        const cudaError_t e = set_smem_attr_once(attr, k_br2_fp64_clu<KB, R>, kClu2Smem);
         if (e != cudaSuccess) return e;
-        attr[dev & 63] = true;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(lanes * R);

@@ -63,11 +63,12 @@ constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kGr
 
 // ------------------------------------------------------------ kernels ----
 
-// key table: out[i][j][r][c][t], t < 2N (4 bytes per thread)
-__global__ void k_i8_key(const uint32_t* __restrict__ bk, int8_t* __restrict__ out)
+// key table: out[i][j][r][c][t], t < 2N (4 bytes per thread), i over the
+// key's ntrgsw TRGSWs (636 plain, 318 x 3 KeyBundle)
+__global__ void k_i8_key(const uint32_t* __restrict__ bk, int ntrgsw, int8_t* __restrict__ out)
 {
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // 4-byte unit
-    const size_t total = (size_t)kN0 * kVBytesStep / 4;
+    const size_t total = (size_t)ntrgsw * kVBytesStep / 4;
     if (q >= total) return;
     const size_t byte = q * 4;
     const int t0 = (int)(byte % (2 * kN));
@@ -106,10 +107,18 @@ __global__ void k_i8_init(const uint32_t* __restrict__ lane_in, int lanes, uint3
     }
 }
 
-// digits of X^abar acc - acc for step `step`, written as swizzled tiles
+// Digits of the step's external-product input, written as swizzled tiles
 // tiles[group][chunk][32 KB]; one CTA (256 threads) per lane, 4 coefficients
-// per thread and polynomial
-__global__ void __launch_bounds__(256) k_i8_decompose(const uint32_t* __restrict__ acc,
+// per thread and polynomial.
+//  * plain CMUX step `step`: digits of X^abar acc - acc (acc is only read);
+//  * KeyBundle pair (KB): digits of acc itself, and acc is overwritten in
+//    place with their gadget recomposition sum_d dec_d 2^(32 - 8 (d + 1)) =
+//    (acc + 2^15) & 0xFFFF0000 -- the H term of the combined key
+//    H + sum_j bk_j (X^(e_j) - 1), to which the pair's GEMM then adds the
+//    rotated products (include/gatebootstrapping_gpu.cuh:928-948, :966-994).
+//    Each thread reads and rewrites only its own coefficients.
+template <bool KB>
+__global__ void __launch_bounds__(256) k_i8_decompose(uint32_t* __restrict__ acc,
                                                       const uint16_t* __restrict__ abar, int lanes,
                                                       int step, uint8_t* __restrict__ tiles)
 {
@@ -118,30 +127,49 @@ __global__ void __launch_bounds__(256) k_i8_decompose(const uint32_t* __restrict
     asm volatile("griddepcontrol.wait;" ::: "memory");
     const int l = blockIdx.x;
     if (l >= lanes) return;
-    const uint32_t ab = abar[(size_t)l * 640 + step];
-    const uint32_t abm = ab & (kN - 1), abn = ab >> 10;
     const uint32_t row = (uint32_t)(l % kGroup);
     uint8_t* gtile = tiles + (size_t)(l / kGroup) * kChunks * kTileBytes;
     const int m = threadIdx.x * 4;
     constexpr uint32_t kOff = (128u << 24) + (128u << 16) + (1u << 15);
-    // the rotated window a[(m - ab) ..  + 4) from two aligned 16-byte loads
-    const uint32_t base = ((uint32_t)m - ab) & (kN - 1), q0 = base & ~3u, off = base & 3u;
+    uint32_t ab = 0, abm = 0, abn = 0, base = 0, q0 = 0, off = 0;
+    if (!KB) {
+        ab = abar[(size_t)l * 640 + step];
+        abm = ab & (kN - 1);
+        abn = ab >> 10;
+        // the rotated window a[(m - ab) ..  + 4) from two aligned 16-byte loads
+        base = ((uint32_t)m - ab) & (kN - 1);
+        q0 = base & ~3u;
+        off = base & 3u;
+    }
 #pragma unroll
     for (int j = 0; j < 2; j++) {
-        const uint32_t* a = acc + (size_t)l * kTrlwe + j * kN;
+        uint32_t* a = acc + (size_t)l * kTrlwe + j * kN;
         const uint4 cur = *reinterpret_cast<const uint4*>(a + m);
-        const uint4 w0 = *reinterpret_cast<const uint4*>(a + q0);
-        const uint4 w1 = *reinterpret_cast<const uint4*>(a + ((q0 + 4) & (kN - 1)));
-        const uint32_t win[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
         const uint32_t cv[4] = {cur.x, cur.y, cur.z, cur.w};
+        uint32_t x[4];
+        if (KB) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) x[e] = cv[e];
+            *reinterpret_cast<uint4*>(a + m) =
+                make_uint4((cv[0] + (1u << 15)) & 0xFFFF0000u, (cv[1] + (1u << 15)) & 0xFFFF0000u,
+                           (cv[2] + (1u << 15)) & 0xFFFF0000u, (cv[3] + (1u << 15)) & 0xFFFF0000u);
+        } else {
+            const uint4 w0 = *reinterpret_cast<const uint4*>(a + q0);
+            const uint4 w1 = *reinterpret_cast<const uint4*>(a + ((q0 + 4) & (kN - 1)));
+            const uint32_t win[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const uint32_t n = (uint32_t)(m + e);
+                // win[off + e] without a dynamic register index
+                uint32_t rv = off == 0 ? win[e] : off == 1 ? win[e + 1] : off == 2 ? win[e + 2] : win[e + 3];
+                rv = ((n < abm) ^ abn) ? 0u - rv : rv;
+                x[e] = rv - cv[e];
+            }
+        }
         uint32_t d0 = 0, d1 = 0;
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-            const uint32_t n = (uint32_t)(m + e);
-            // win[off + e] without a dynamic register index
-            uint32_t rv = off == 0 ? win[e] : off == 1 ? win[e + 1] : off == 2 ? win[e + 2] : win[e + 3];
-            rv = ((n < abm) ^ abn) ? 0u - rv : rv;
-            const uint32_t t = rv - cv[e] + kOff;
+            const uint32_t t = x[e] + kOff;
             d0 |= (uint32_t)(uint8_t)((int)((t >> 24) & 255u) - 128) << (8 * e);
             d1 |= (uint32_t)(uint8_t)((int)((t >> 16) & 255u) - 128) << (8 * e);
         }
@@ -221,11 +249,13 @@ __device__ __forceinline__ void unit_of(int it, const int* geo, int& t, int& k0,
     }
 }
 
+template <bool KB>
 __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __restrict__ vkey,
                                                                 const uint8_t* __restrict__ tiles,
                                                                 uint32_t* __restrict__ acc,
                                                                 int lanes, int tiles_j, int split,
-                                                                int* __restrict__ err)
+                                                                const uint16_t* __restrict__ abar,
+                                                                int pair, int* __restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t raw_addr = smem_u32(smem_raw);
@@ -243,10 +273,14 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
     uint64_t* red_clear = red_full + 1;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(red_clear + 1);
     __shared__ volatile int s_fail;
-    __shared__ int s_geo[4];
+    __shared__ int s_geo[5];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int j_out = blockIdx.x & 1, cb = blockIdx.x >> 1, ncj = gridDim.x >> 1;
+    // combo = key * 2 + j_out: the plain form has one key per step, the
+    // KeyBundle form three (bk0, bk1, bk2 of the pair)
+    constexpr int kCombos = KB ? 6 : 2;
+    const int combo = (int)(blockIdx.x % kCombos), j_out = combo & 1;
+    const int cb = (int)(blockIdx.x / kCombos), ncj = (int)(gridDim.x / kCombos);
     const int R = tiles_j / ncj, NU = (tiles_j - R * ncj) * split;
     const int T = R + (cb < NU ? (NU - 1 - cb) / ncj + 1 : 0);
 
@@ -262,6 +296,7 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
         s_geo[1] = cb;
         s_geo[2] = ncj;
         s_geo[3] = split;
+        s_geo[4] = combo;
         for (int s = 0; s < kPStages; s++) {
             mbar_init(&full[s], 128 + 1);
             mbar_init(&empty[s], 1);
@@ -284,7 +319,7 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
         if (lane == 0) {
             if (par == 0) {
                 mbar_expect_tx(bar_v, (uint32_t)kSmemPV);
-                bulk_g2s(vs, vkey + (size_t)j_out * kVBytesJ, (uint32_t)kSmemPV, bar_v);
+                bulk_g2s(vs, vkey + (size_t)combo * kVBytesJ, (uint32_t)kSmemPV, bar_v);
             }
             // the key window above is constant; the digit tiles are the
             // previous kernel's output (programmatic dependent launch)
@@ -426,14 +461,39 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
             const int group = t / (kN / kRowsCoef);
             const int n0 = (t % (kN / kRowsCoef)) * kRowsCoef;
             constexpr int kW = kGroup / kDrainWarps;
-            // a tile split along K is added by several CTAs: atomic adds
-            // (mod 2^32, so their order does not matter)
+            // a tile split along K is added by several CTAs, and in the
+            // KeyBundle form three keys add into every word: atomic adds (mod
+            // 2^32, so their order does not matter)
+            if (KB) {
+                // P = Dec(acc) . bk_key enters as (X^e - 1) P, with
+                // e = a0 + a1, a0, a1 for bk0, bk1, bk2
+                const int key = s_geo[4] >> 1;
+                const uint32_t n = (uint32_t)(n0 + lane);
+#pragma unroll 1
+                for (int i = 0; i < kW; i++) {
+                    const int gl = d + kDrainWarps * i, l = group * kGroup + gl;
+                    const uint32_t v = red[(size_t)gl * kRowsCoef + lane];
+                    red[(size_t)gl * kRowsCoef + lane] = 0u;
+                    if (l < lanes) {
+                        // both rotation amounts of the pair in one 32-bit load
+                        const uint32_t a01 = *reinterpret_cast<const uint32_t*>(
+                            abar + (size_t)l * 640 + 2 * pair);
+                        const uint32_t a0 = a01 & 0xFFFFu, a1 = a01 >> 16;
+                        const uint32_t e = key == 0 ? (a0 + a1) & (2 * kN - 1) : key == 1 ? a0 : a1;
+                        const uint32_t pos = (n + e) & (2 * kN - 1);
+                        uint32_t* out = acc + (size_t)l * kTrlwe + j_out * kN;
+                        atomicAdd(&out[pos & (kN - 1)], pos < (uint32_t)kN ? v : 0u - v);
+                        atomicAdd(&out[n], 0u - v);
+                    }
+                }
+            } else {
 #pragma unroll
-            for (int i = 0; i < kW; i++) {
-                const int gl = d + kDrainWarps * i, l = group * kGroup + gl;
-                const uint32_t v = red[(size_t)gl * kRowsCoef + lane];
-                red[(size_t)gl * kRowsCoef + lane] = 0u;
-                if (l < lanes) atomicAdd(&acc[(size_t)l * kTrlwe + j_out * kN + n0 + lane], v);
+                for (int i = 0; i < kW; i++) {
+                    const int gl = d + kDrainWarps * i, l = group * kGroup + gl;
+                    const uint32_t v = red[(size_t)gl * kRowsCoef + lane];
+                    red[(size_t)gl * kRowsCoef + lane] = 0u;
+                    if (l < lanes) atomicAdd(&acc[(size_t)l * kTrlwe + j_out * kN + n0 + lane], v);
+                }
             }
             __threadfence_block();  // the zeroed buffer before the next tile's adds
             __syncwarp();
@@ -490,28 +550,25 @@ cudaError_t ensure_ws(Int8Workspace& w, int lanes)
 
 cudaError_t set_gemm_attr()
 {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr[64] = {};
-    if (attr[dev & 63]) return cudaSuccess;
-    const cudaError_t e = cudaFuncSetAttribute(k_i8_gemm_p, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)kSmemGemmP);
-    if (e == cudaSuccess) attr[dev & 63] = true;
-    return e;
+    static DeviceAttrFlags attr_plain, attr_kb;
+    const cudaError_t e = set_smem_attr_once(attr_plain, k_i8_gemm_p<false>, kSmemGemmP);
+    return e != cudaSuccess ? e : set_smem_attr_once(attr_kb, k_i8_gemm_p<true>, kSmemGemmP);
 }
 
 }  // namespace
 
-cudaError_t int8_key_build(Int8Key& k, const uint32_t* bk_dev, cudaStream_t st)
+cudaError_t int8_key_build(Int8Key& k, const uint32_t* bk_dev, bool kb, cudaStream_t st)
 {
     int8_key_free(k);
-    k.bytes = (size_t)kN0 * kVBytesStep;
+    const int ntrgsw = kb ? 3 * (kN0 / 2) : kN0;
+    k.bytes = (size_t)ntrgsw * kVBytesStep;
     cudaError_t e = cudaMalloc(&k.limbs, k.bytes);
     if (e != cudaSuccess) return e;
     const size_t units = k.bytes / 4;
-    k_i8_key<<<(unsigned)((units + 255) / 256), 256, 0, st>>>(bk_dev, (int8_t*)k.limbs);
+    k_i8_key<<<(unsigned)((units + 255) / 256), 256, 0, st>>>(bk_dev, ntrgsw, (int8_t*)k.limbs);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    k.kb = kb;
     k.ready = true;
     return cudaSuccess;
 }
@@ -547,10 +604,23 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int nsteps = (steps < 0 || steps > kN0) ? kN0 : steps;
+    // plain key: one GEMM step per CMUX step (636); KeyBundle key: one per
+    // pair (318), over the pair's three keys
+    const int total = k.kb ? kN0 / 2 : kN0;
+    const int nsteps = (steps < 0 || steps > total) ? total : steps;
+    const int combos = k.kb ? 6 : 2;
+    const size_t key_step = (size_t)(k.kb ? 3 : 1) * kVBytesStep;
     const int groups = (lanes + kGroup - 1) / kGroup;
     k_i8_init<<<lanes, 256, 0, st>>>(lane_in, lanes, mu, w.abar, w.acc);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int n = 1;
+    // tiles per combo; the tiles of the last, partial round are split along
+    // K so that the round's units fit one per CTA (split = 1, 2, 4 or 8)
+    const int tiles_j = groups * (kN / kRowsCoef);
+    const int ncj = sms / combos, rem = tiles_j % ncj;
+    int split = 1;
+    while (rem && split < 8 && rem * split * 2 <= ncj) split *= 2;
+    const int units = tiles_j < ncj ? tiles_j * split : ncj;
     for (int i = 0; i < nsteps; i++) {
         // both kernels are programmatic dependents of the one before: each
         // starts (TMEM, barriers, key window) while the previous one drains
@@ -564,28 +634,28 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
             cfg.stream = st;
             cfg.attrs = pdl;
             cfg.numAttrs = 1;
-            cudaLaunchKernelEx(&cfg, k_i8_decompose, (const uint32_t*)w.acc, (const uint16_t*)w.abar,
-                               lanes, i, (uint8_t*)w.digits);
+            e = k.kb ? cudaLaunchKernelEx(&cfg, k_i8_decompose<true>, w.acc, (const uint16_t*)w.abar,
+                                          lanes, i, (uint8_t*)w.digits)
+                     : cudaLaunchKernelEx(&cfg, k_i8_decompose<false>, w.acc,
+                                          (const uint16_t*)w.abar, lanes, i, (uint8_t*)w.digits);
+            if (e != cudaSuccess) return e;
         }
-        const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * kVBytesStep;
-        // even grid: CTA b serves output polynomial b & 1
-        const int tiles_j = groups * (kN / kRowsCoef);
-        // tiles of the last, partial round are split along K so that the
-        // round's units fit one per CTA pair (split = 1, 2, 4 or 8)
-        const int ncj = sms / 2, rem = tiles_j % ncj;
-        int split = 1;
-        while (rem && split < 8 && rem * split * 2 <= ncj) split *= 2;
-        const int units = tiles_j < ncj ? tiles_j * split : ncj;
+        const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * key_step;
         {
             cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(2 * units);
+            cfg.gridDim = dim3(combos * units);
             cfg.blockDim = dim3(kGemmPThreads);
             cfg.dynamicSmemBytes = kSmemGemmP;
             cfg.stream = st;
             cfg.attrs = pdl;
             cfg.numAttrs = 1;
-            cudaLaunchKernelEx(&cfg, k_i8_gemm_p, vk, (const uint8_t*)w.digits, w.acc, lanes, tiles_j,
-                               split, err);
+            e = k.kb ? cudaLaunchKernelEx(&cfg, k_i8_gemm_p<true>, vk, (const uint8_t*)w.digits,
+                                          w.acc, lanes, tiles_j, split, (const uint16_t*)w.abar, i,
+                                          err)
+                     : cudaLaunchKernelEx(&cfg, k_i8_gemm_p<false>, vk, (const uint8_t*)w.digits,
+                                          w.acc, lanes, tiles_j, split, (const uint16_t*)w.abar, i,
+                                          err);
+            if (e != cudaSuccess) return e;
         }
         n += 2;
     }

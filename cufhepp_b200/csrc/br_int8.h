@@ -8,7 +8,8 @@ namespace cufhe {
 
 struct Int8Key {
     bool ready = false;
-    uint8_t* limbs = nullptr;  // per CMUX step: Toeplitz source rows of the key limbs
+    bool kb = false;           // KeyBundle key: TRGSW[n0 / 2][3], one step per pair
+    uint8_t* limbs = nullptr;  // per TRGSW: Toeplitz source rows of the key limbs
     size_t bytes = 0;
 };
 
@@ -28,7 +29,9 @@ struct Int8Workspace2 {
     uint16_t* abar = nullptr;
 };
 
-cudaError_t int8_key_build(Int8Key& k, const uint32_t* bk_dev, cudaStream_t st);
+// bk_dev: BootstrappingKey<lvl01> in the TFHEpp layout, plain TRGSW[636] or
+// (kb) KeyBundle TRGSW[318][3]
+cudaError_t int8_key_build(Int8Key& k, const uint32_t* bk_dev, bool kb, cudaStream_t st);
 void int8_key_free(Int8Key& k);
 void int8_workspace_free(Int8Workspace& w);
 // The launchers are asynchronous (stream-ordered, capturable into a CUDA
@@ -36,6 +39,8 @@ void int8_workspace_free(Int8Workspace& w);
 // up sets *err, which the caller reads at synchronisation.
 // int8_reserve*: size the workspace for `lanes` and set the kernels'
 // attributes; call before a graph capture.
+// launch_br_int8: `steps` counts CMUX steps of a plain key, pairs of a
+// KeyBundle key (all of them when steps < 0).
 cudaError_t int8_reserve(Int8Workspace& w, int lanes);
 cudaError_t int8_reserve2(Int8Workspace2& w, int lanes);
 cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* lane_in, int lanes,

@@ -520,14 +520,8 @@ cudaError_t ensure_ws2(Int8Workspace2& w, int lanes)
 
 cudaError_t set_gemm2_attr()
 {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr[64] = {};
-    if (attr[dev & 63]) return cudaSuccess;
-    const cudaError_t e = cudaFuncSetAttribute(k_i82_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)kSmemGemm);
-    if (e == cudaSuccess) attr[dev & 63] = true;
-    return e;
+    static DeviceAttrFlags attr;
+    return set_smem_attr_once(attr, k_i82_gemm, kSmemGemm);
 }
 
 }  // namespace
@@ -577,6 +571,7 @@ cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t*
     const int blocks_j = groups * kNBlocks;
     const int grid = 2 * (blocks_j < sms / 2 ? blocks_j : sms / 2);
     k_i82_init<<<lanes, 256, 0, st>>>(lane_in, lanes, mu, w.abar, w.acc);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int n = 1;
     for (int i = 0; i < nsteps; i++) {
         // both kernels are programmatic dependents of the one before: each
@@ -590,14 +585,16 @@ cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t*
         cfg.stream = st;
         cfg.attrs = pdl;
         cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, k_i82_decompose, (const uint64_t*)w.acc, (const uint16_t*)w.abar,
-                           lanes, i, (uint8_t*)w.digits);
+        e = cudaLaunchKernelEx(&cfg, k_i82_decompose, (const uint64_t*)w.acc,
+                               (const uint16_t*)w.abar, lanes, i, (uint8_t*)w.digits);
+        if (e != cudaSuccess) return e;
         const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * kVStep;
         cfg.gridDim = dim3(grid);
         cfg.blockDim = dim3(kGemmThreads);
         cfg.dynamicSmemBytes = kSmemGemm;
-        cudaLaunchKernelEx(&cfg, k_i82_gemm, vk, (const uint8_t*)w.digits, w.acc, lanes, blocks_j,
-                           err);
+        e = cudaLaunchKernelEx(&cfg, k_i82_gemm, vk, (const uint8_t*)w.digits, w.acc, lanes,
+                               blocks_j, err);
+        if (e != cudaSuccess) return e;
         n += 2;
     }
     k_i82_extract<<<lanes, 256, 0, st>>>(w.acc, lanes, acc_out, lane_out);

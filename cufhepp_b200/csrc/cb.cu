@@ -146,14 +146,10 @@ template <int L, int BGBIT>
 static cudaError_t launch_cmux_t(const CmuxPlan& p, const Fp64Tables& t, cudaStream_t st)
 {
     constexpr size_t smem = sizeof(double2) * 2 * L * kSlotStride;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr[64] = {};
-    if (!attr[dev & 63]) {
-        const cudaError_t e = cudaFuncSetAttribute(
-            k_cmux<L, BGBIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static DeviceAttrFlags attr;
+    {
+        const cudaError_t e = set_smem_attr_once(attr, k_cmux<L, BGBIT>, smem);
         if (e != cudaSuccess) return e;
-        attr[dev & 63] = true;
     }
     k_cmux<L, BGBIT><<<p.count, 64 * L, smem, st>>>(p, t.psi, t.tw512);
     return cudaGetLastError();

@@ -31,7 +31,7 @@ struct DeviceState {
     double2* bkf = nullptr;  // FP64 Fourier-domain bootstrapping key
     double2* psi = nullptr;
     double2* tw512 = nullptr;
-    Int8Key i8;              // INT8 exact-path key (non-KeyBundle only)
+    Int8Key i8;              // INT8 exact-path key (plain or KeyBundle, as the FP64 one)
     Int8Key i8_2;            // INT8 exact-path lvl02 key (non-KeyBundle only)
     uint8_t* iks_key = nullptr;  // KSK as signed byte-limb tiles (tensor-core IKS)
     int* err = nullptr;          // set by a device wait that timed out
@@ -331,8 +331,9 @@ int init_device(int d, const cufhe_keyview* ek)
     CK(cudaMalloc(&D.bkf, (size_t)npolys * 512 * sizeof(double2)));
     const Fp64Tables t = {D.psi, D.tw512};
     CKL(launch_bk_to_fft(raw, npolys, t, D.bkf, 0));
-    if (!ek->keybundle) {
-        cudaError_t e = int8_key_build(D.i8, raw, 0);
+    {
+        // INT8 Toeplitz limb windows of either key form (KeyBundle: 954 TRGSWs)
+        cudaError_t e = int8_key_build(D.i8, raw, ek->keybundle != 0, 0);
         if (e != cudaSuccess) {
             cudaFree(raw);
             return fail(CUFHE_ERR_CUDA, "INT8 key conversion: %s", cudaGetErrorString(e));
@@ -602,8 +603,7 @@ int run_br(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint32_t mu, i
 {
     DeviceState& D = g_dev[s->device];
     if (g_precision == CUFHE_INT8_EXACT) {
-        if (D.kb || !D.i8.ready)
-            return fail(CUFHE_ERR_STATE, "INT8_EXACT needs a bootstrapping key without KeyBundle");
+        if (!D.i8.ready) return fail(CUFHE_ERR_STATE, "INT8_EXACT: no INT8 key on this device");
         int launches = 0;
         ProfRec pr;
         prof_begin(s->st, pr, CUFHE_K_BR_INT8);

@@ -16,9 +16,37 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "params.h"
 
 namespace cufhe {
+
+// "Function attribute already set on this device" flags of one kernel.
+// cudaFuncSetAttribute acts on the current device only, so each device needs
+// its own flag; the bits are atomic because several host threads may launch
+// on different devices at once (setting an attribute twice is harmless).
+class DeviceAttrFlags {
+  public:
+    bool test(int dev) const { return (bits_.load(std::memory_order_acquire) >> (dev & 63)) & 1u; }
+    void set(int dev) { bits_.fetch_or(uint64_t(1) << (dev & 63), std::memory_order_release); }
+
+  private:
+    std::atomic<uint64_t> bits_{0};
+};
+
+// Sets the dynamic shared-memory limit of `func` on the current device once.
+template <typename F>
+cudaError_t set_smem_attr_once(DeviceAttrFlags& flags, F* func, size_t bytes)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (flags.test(dev)) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) flags.set(dev);
+    return e;
+}
 
 constexpr int kN0 = CUFHE_LVL0_N;          // 636
 constexpr int kN = CUFHE_LVL1_N;           // 1024

@@ -439,15 +439,10 @@ void iks_tc_workspace_free(IksWorkspace& w)
 template <int CH, int NT, int OUTW>
 static cudaError_t gemm_attr()
 {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static bool attr[64] = {};
-    if (!attr[dev & 63]) {
-        cudaError_t e = cudaFuncSetAttribute(k_iks_gemm<CH, NT, OUTW>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kSmem);
+    static DeviceAttrFlags attr;
+    {
+        const cudaError_t e = set_smem_attr_once(attr, k_iks_gemm<CH, NT, OUTW>, kSmem);
         if (e != cudaSuccess) return e;
-        attr[dev & 63] = true;
     }
     return cudaSuccess;
 }

@@ -148,13 +148,9 @@ cudaError_t launch_iks(int mode, const Plan& plan, const uint32_t* in0, const ui
     if (total <= 0) return cudaSuccess;
     const int blocks = (total + kIksGates - 1) / kIksGates;
     const size_t smem = sizeof(uint16_t) * kN * kIksGates;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_iks<kIksGates>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static DeviceAttrFlags attr;
+    const cudaError_t e = set_smem_attr_once(attr, k_iks<kIksGates>, smem);
+    if (e != cudaSuccess) return e;
     k_iks<kIksGates><<<blocks, kIksThreads, smem, st>>>(mode, plan, in0, in1, in2, lane_out, ksk,
                                                      dst);
     return cudaGetLastError();

@@ -190,8 +190,10 @@ int cufhe_gate_batch_host(const int32_t* gates_host, int uniform_gate, size_t co
  * keeps its lane buffers in a fixed array compiled into the library (about
  * 1.7 MB on every GPU that loads it, held until exit) and therefore accepts
  * at most 256 blind rotations per call (256 binary gates or 128 Mux/NMux);
- * larger calls return CUFHE_ERR_ARG.  Always uses the FP64 FFNT form.
- * Arguments as cufhe_gate_batch with every gate equal to `gate`; the caller
+ * larger calls return CUFHE_ERR_ARG.  Only CUFHE_LVL0 and CUFHE_LVL1 are
+ * accepted (CUFHE_LVL02 returns CUFHE_ERR_ARG), and it always runs the FP64
+ * FFNT form, whatever cufhe_set_precision selected.  Otherwise the arguments
+ * are those of cufhe_gate_batch with every gate equal to `gate`; the caller
  * passes device inputs and outputs.  The first call on a device looks up the
  * array's device address, so make it before any stream capture.  All calls
  * share the array: calls whose work overlaps on the GPU race and corrupt

@@ -145,9 +145,10 @@ def test_slack_gates_fill_narrow_waves(lvl1_ctx):
     assert np.array_equal(wires, wave_by_wave(net, engine.LVL1, host))
 
 
-def test_circuit_int8_form(keys):
-    sk, _, ek = keys
-    engine.initialize(ek)
+@pytest.mark.parametrize("kb", [False, True], ids=["plain", "kb"])
+def test_circuit_int8_form(keys, kb):
+    sk, ek_kb, ek_nokb = keys
+    engine.initialize(ek_kb if kb else ek_nokb)
     engine.set_precision(P.INT8_EXACT)
     try:
         net = CI.uneven_workload(5, dags=2, adders=1, dag_gates=(50, 80), adder_width=(8, 8))

@@ -21,10 +21,10 @@ FULL = 300
 GATES = [P.NAND, P.AND, P.OR, P.XOR, P.XNOR, P.MUX, P.NOR, P.ANDNY, P.ORYN, P.NMUX]
 
 
-@pytest.fixture(scope="module", params=["fp64", "int8"])
+@pytest.fixture(scope="module", params=["fp64", "int8", "int8_kb"])
 def form(request, keys):
     sk, ek_kb, ek_nokb = keys
-    engine.initialize(ek_kb if request.param == "fp64" else ek_nokb)
+    engine.initialize(ek_nokb if request.param == "int8" else ek_kb)
     engine.set_precision(P.FP64_FFNT if request.param == "fp64" else P.INT8_EXACT)
     yield sk, request.param
     engine.set_precision(P.FP64_FFNT)

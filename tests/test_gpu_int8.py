@@ -2,7 +2,17 @@
 
 The external product runs as INT8 Toeplitz GEMMs on byte limbs with INT32
 accumulation, so the whole blind rotation -- and with the integer key switch,
-the whole gate -- must be bit-identical to the exact schoolbook oracle.
+the whole gate -- must be bit-identical to the exact schoolbook oracle.  Both
+bootstrapping-key forms are covered:
+
+* plain key (TRGSW[636]): one GEMM per CMUX step, acc += Dec(X^a acc - acc) BK_i;
+* KeyBundle key (TRGSW[318][3]): one step per pair, three GEMMs against
+  bk0, bk1, bk2 whose products enter as (X^e - 1) P with e = a0 + a1, a0, a1,
+  plus the gadget recomposition of the digits (the H term).  The oracle forms
+  the combined key H + sum_j bk_j (X^e_j - 1) first and multiplies once
+  (include/gatebootstrapping_gpu.cuh:895-1033); the GPU splits the product by
+  distributivity, which is exact in Z_2^32[X]/(X^N + 1), so the two agree bit
+  for bit.
 """
 import numpy as np
 import pytest
@@ -13,9 +23,10 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def ctx(keys):
-    sk, _, ek = keys  # INT8 exact form uses the plain (non-KeyBundle) key
+@pytest.fixture(scope="module", params=[False, True], ids=["plain", "kb"])
+def ctx(keys, request):
+    sk, ek_kb, ek_plain = keys
+    ek = ek_kb if request.param else ek_plain
     engine.initialize(ek)
     engine.set_precision(P.INT8_EXACT)
     yield sk, ek
@@ -38,10 +49,11 @@ def lvl0(sk, count, seed):
 
 @pytest.mark.parametrize("steps", [1, 2, 7])
 def test_int8_steps_bit_exact(ctx, steps):
+    """1, 2 and 7 CMUX steps (plain) or KeyBundle pairs (kb)."""
     sk, ek = ctx
     _, x = lvl0(sk, 8, 100 + steps)
     got = rotate(x, steps, 8)
-    ref = O.blind_rotate(x, P.MU32, ek.bk, False, O.EXACT, steps=steps)
+    ref = O.blind_rotate(x, P.MU32, ek.bk, ek.keybundle, O.EXACT, steps=steps)
     assert np.array_equal(got, ref)
 
 
@@ -50,7 +62,7 @@ def test_int8_two_lane_groups_bit_exact(ctx):
     # 300 lanes span two 256-lane MMA groups (the second one partial)
     _, x = lvl0(sk, 300, 7)
     got = rotate(x, 2, 300)
-    ref = O.blind_rotate(x, P.MU32, ek.bk, False, O.EXACT, steps=2)
+    ref = O.blind_rotate(x, P.MU32, ek.bk, ek.keybundle, O.EXACT, steps=2)
     assert np.array_equal(got, ref)
 
 
@@ -64,7 +76,7 @@ def test_int8_many_tiles_per_cta_bit_exact(ctx):
     _, x = lvl0(sk, count, 77)
     got = rotate(x, 2, count)
     pick = np.unique(np.concatenate([np.arange(0, count, 131), [255, 256, 2559, 2560, count - 1]]))
-    ref = O.blind_rotate(x[pick], P.MU32, ek.bk, False, O.EXACT, steps=2)
+    ref = O.blind_rotate(x[pick], P.MU32, ek.bk, ek.keybundle, O.EXACT, steps=2)
     assert np.array_equal(got[pick], ref)
 
 
@@ -79,7 +91,7 @@ def test_int8_full_rotation_bit_exact(ctx):
     sk, ek = ctx
     bits, x = lvl0(sk, 4, 8)
     got = rotate(x, -1, 4)
-    ref = O.blind_rotate(x, P.MU32, ek.bk, False, O.EXACT)
+    ref = O.blind_rotate(x, P.MU32, ek.bk, ek.keybundle, O.EXACT)
     assert np.array_equal(got, ref)
 
 
@@ -92,14 +104,16 @@ def test_int8_gates_bit_exact(ctx, level):
     cts = [client.encrypt_bits(sk, x, level, seed=60 + i) for i, x in enumerate((a, b, c))]
     out = engine.gate_batch_host(gates, level, *cts)
     engine.synchronize()
-    ref = O.gate_batch(gates, level, *cts, ek.bk, ek.ksk, False, O.EXACT)
+    ref = O.gate_batch(gates, level, *cts, ek.bk, ek.ksk, ek.keybundle, O.EXACT)
     assert np.array_equal(out, ref)
     exp = np.array([P.TRUTH[g](int(x), int(y), int(z)) for g, x, y, z in zip(gates, a, b, c)])
     assert np.array_equal(client.decrypt_bits(sk, out, level), exp)
 
 
 def test_int8_reproduces_golden_digests(ctx):
-    """The INT8 engine path matches the committed exact-oracle digests bit for bit."""
+    """The INT8 engine path matches the committed exact-oracle digests bit for
+    bit, for the key form of this parametrisation (tests/golden/gates_exact.json
+    holds both)."""
     import json
     import sys
     from pathlib import Path
@@ -107,18 +121,20 @@ def test_int8_reproduces_golden_digests(ctx):
     sys.path.insert(0, str(golden))
     import make_gate_golden as M
     want = json.loads((golden / "gates_exact.json").read_text())
+    kb = ctx[1].keybundle
+    tag = "kb" if kb else "plain"
     sk = client.SecretKey.generate(M.SEED)
-    ek = client.EvalKey.generate(sk, keybundle=False)
-    assert M.digest(ek.bk) == want["keys"]["plain"]["bk"]
+    ek = client.EvalKey.generate(sk, keybundle=kb)
+    assert M.digest(ek.bk) == want["keys"][tag]["bk"]
     engine.initialize(ek)  # golden keys (the module fixture's keys are reinstated below)
     try:
         for level in (1, 0):
             _, cts = M.inputs(sk, level)
             out = engine.gate_batch_host(np.array(M.GATES, np.int32), level, *cts)
             engine.synchronize()
-            assert M.digest(out) == want["cases"][f"plain_lvl{level}"]["outputs"]
+            assert M.digest(out) == want["cases"][f"{tag}_lvl{level}"]["outputs"]
         x = client.encrypt_bits(sk, np.array([0, 1, 1, 0], np.uint8), 0, seed=M.SEED + 99)
-        assert M.digest(rotate(x, 3, 4)) == want["cases"]["plain_br3"]["outputs"]
+        assert M.digest(rotate(x, 3, 4)) == want["cases"][f"{tag}_br3"]["outputs"]
         c1 = client.encrypt_bits(sk, np.arange(16, dtype=np.uint8) & 1, 1, seed=M.SEED + 7)
         d_in = engine.to_device(c1)
         d_out = engine.DeviceBuffer(16 * P.TLWE0_WORDS * 4)

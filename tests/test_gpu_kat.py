@@ -9,6 +9,7 @@ C-ABI in both precision forms (test/test_accumulate_diag.cu:369-605):
   form must give the exact answer as well, with the plain key and with the
   KeyBundle key (bk0 = TRGSW(s0 s1), bk1 = TRGSW(s0 (1 - s1)),
   bk2 = TRGSW((1 - s0) s1) at s0 = 1, s1 = 0: bk1 = TRGSW(1), bk0 = bk2 = 0).
+  The INT8 form runs every case with both key forms as well.
 """
 import numpy as np
 import pytest
@@ -34,6 +35,8 @@ def trgsw_one() -> np.ndarray:
 def bootstrapping_key(kind: str) -> np.ndarray:
     if kind == "zero":
         return np.zeros(P.BK_WORDS, np.uint32)
+    if kind == "zero_kb":
+        return np.zeros(P.BKKB_WORDS, np.uint32)
     if kind == "one":
         return np.broadcast_to(trgsw_one(), (P.LVL0_N,) + trgsw_one().shape).ravel().copy()
     # KeyBundle of noiseless keys at s0 = 1, s1 = 0: [pair][bk0, bk1, bk2]
@@ -59,7 +62,7 @@ def rotated_test_vector(k: int) -> np.ndarray:
 def run(kind: str, form: int, steps: int) -> np.ndarray:
     rng = np.random.default_rng(1)
     ksk = rng.integers(0, 2**32, P.KSK_WORDS, dtype=np.uint64).astype(np.uint32)
-    engine.initialize(client.EvalKey(bootstrapping_key(kind), ksk, kind == "one_kb"))
+    engine.initialize(client.EvalKey(bootstrapping_key(kind), ksk, kind.endswith("_kb")))
     try:
         engine.set_precision(form)
         x = inputs()
@@ -77,9 +80,14 @@ FORMS = [pytest.param(P.FP64_FFNT, id="fp64"), pytest.param(P.INT8_EXACT, id="in
 
 
 @pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("kind", ["zero", "zero_kb"], ids=["plain", "kb"])
 @pytest.mark.parametrize("steps", [1, 7, -1], ids=["1step", "7steps", "all"])
-def test_zero_key_leaves_the_accumulator_unchanged(form, steps):
-    acc = run("zero", form, steps)
+def test_zero_key_leaves_the_accumulator_unchanged(form, kind, steps):
+    """A zero key leaves the accumulator unchanged; with a KeyBundle key the
+    pair's result is the gadget recomposition of the digits (the H term),
+    which is exact for the test polynomial (mu = 2^29 has no bits below
+    2^16)."""
+    acc = run(kind, form, steps)
     for lane in range(len(SHIFTS)):
         assert not acc[lane, 0].any()
         assert np.array_equal(acc[lane, 1], rotated_test_vector(0))
@@ -93,8 +101,9 @@ def test_trgsw_one_rotates_by_x_to_the_abar(form):
         assert np.array_equal(acc[lane, 1], rotated_test_vector(k)), k
 
 
-def test_keybundle_of_noiseless_keys_rotates_by_x_to_the_abar():
-    acc = run("one_kb", P.FP64_FFNT, -1)
+@pytest.mark.parametrize("form", FORMS)
+def test_keybundle_of_noiseless_keys_rotates_by_x_to_the_abar(form):
+    acc = run("one_kb", form, -1)
     for lane, k in enumerate(SHIFTS):
         assert not acc[lane, 0].any(), k
         assert np.array_equal(acc[lane, 1], rotated_test_vector(k)), k

@@ -1,8 +1,10 @@
-"""Large-sample correctness of both precision forms, through the C-ABI.
+"""Large-sample correctness of every precision form, through the C-ABI.
 
-* >= 10^6 random gates (all 14 gate ids, both ciphertext levels) decrypt to
-  the truth tables of test/plain.h with zero failures, on the FP64-FFNT form
-  and on the INT8-exact form;
+* >= 10^6 random *bootstrapped* gates per form (gate ids drawn over all 14,
+  so NOT/COPY, which do not bootstrap, are drawn too but not counted; both
+  ciphertext levels) decrypt to the truth tables of test/plain.h with zero
+  failures: the FP64-FFNT form (KeyBundle key), the INT8-exact form with the
+  plain key and the INT8-exact form with the KeyBundle key;
 * a 1024-gate subset on the INT8 form is bit-identical to the exact
   schoolbook oracle (the whole gate is integer arithmetic there).
 """
@@ -15,15 +17,17 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 CHUNK = 1 << 16
-CHUNKS = 16  # 1,048,576 gates per form
+TARGET = 10 ** 6  # bootstrapped gates per form
 
 
 def run_million(sk, level_split=4):
-    """Returns (gates, failures, smallest |phase| margin in units of mu)."""
+    """Returns (gates, bootstrapped gates, failures, smallest |phase| margin
+    in units of mu); chunks are added until TARGET gates have bootstrapped."""
     rng = np.random.default_rng(2026)
-    total = fails = 0
+    total = boots = fails = 0
     margin = np.inf
-    for c in range(CHUNKS):
+    c = 0
+    while boots < TARGET:
         level = 0 if c % level_split == 0 else 1
         gates = rng.integers(0, 14, CHUNK).astype(np.int32)
         a, b, cc = (rng.integers(0, 2, CHUNK).astype(np.uint8) for _ in range(3))
@@ -40,19 +44,22 @@ def run_million(sk, level_split=4):
         ph = client.phase(sk, out, level).view(np.int32).astype(np.float64)
         margin = min(margin, float(np.abs(ph).min()) / P.MU32)
         total += CHUNK
-    return total, fails, margin
+        boots += int(np.count_nonzero((gates != P.NOT) & (gates != P.COPY)))
+        c += 1
+    return total, boots, fails, margin
 
 
-@pytest.mark.parametrize("form", ["fp64", "int8"])
+@pytest.mark.parametrize("form", ["fp64", "int8", "int8_kb"])
 def test_one_million_gates_zero_failures(keys, form):
     sk, ek_kb, ek_nokb = keys
-    ek = ek_kb if form == "fp64" else ek_nokb
+    ek = ek_nokb if form == "int8" else ek_kb
     engine.initialize(ek)
     try:
         engine.set_precision(P.FP64_FFNT if form == "fp64" else P.INT8_EXACT)
-        total, fails, margin = run_million(sk)
-        print(f"{form}: {total} gates, {fails} decryption failures, min |phase| = {margin:.3f} mu")
-        assert total >= 10 ** 6
+        total, boots, fails, margin = run_million(sk)
+        print(f"{form}: {total} gates ({boots} bootstrapped), {fails} decryption failures, "
+              f"min |phase| = {margin:.3f} mu")
+        assert boots >= TARGET
         assert fails == 0
         assert margin > 0.5  # outputs sit near +-mu, far from the decision boundary
     finally:
@@ -60,8 +67,10 @@ def test_one_million_gates_zero_failures(keys, form):
         engine.cleanup()
 
 
-def test_int8_1024_gates_bit_exact_vs_oracle(keys):
-    sk, _, ek = keys
+@pytest.mark.parametrize("kb", [False, True], ids=["plain", "kb"])
+def test_int8_1024_gates_bit_exact_vs_oracle(keys, kb):
+    sk, ek_kb, ek_nokb = keys
+    ek = ek_kb if kb else ek_nokb
     engine.initialize(ek)
     try:
         engine.set_precision(P.INT8_EXACT)
@@ -71,7 +80,7 @@ def test_int8_1024_gates_bit_exact_vs_oracle(keys):
         cts = [client.encrypt_bits(sk, x, 1, seed=90 + i) for i, x in enumerate((a, b, c))]
         out = engine.gate_batch_host(gates, 1, *cts)
         engine.synchronize()
-        ref = O.gate_batch(gates, 1, *cts, ek.bk, ek.ksk, False, O.EXACT)
+        ref = O.gate_batch(gates, 1, *cts, ek.bk, ek.ksk, ek.keybundle, O.EXACT)
         assert np.array_equal(out, ref)
     finally:
         engine.set_precision(P.FP64_FFNT)
