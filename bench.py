@@ -583,7 +583,7 @@ def run_nand1000(args, torch, engine, client, P, sk, rank, ws, flush):
     return out
 
 
-def fp64_error_lvl1(args, engine, client, P, sk, count=64):
+def fp64_error_lvl1(args, engine, client, P, sk, count=4096):
     """The FP64 form's rounding against the exact product at lvl1, per key
     form: both forms rotate the same `count` lvl0 inputs (the exact INT8 form
     is bit-identical to the schoolbook oracle); reported are the largest
@@ -611,14 +611,19 @@ def fp64_error_lvl1(args, engine, client, P, sk, count=64):
             engine.set_precision(P.FP64_FFNT)
             engine.cleanup()
 
-        def coef(a_, b_):
-            return int(np.abs((a_ - b_).astype(np.uint32).view(np.int32).astype(np.int64)).max())
-        ph = max(int(np.abs((client.trlwe_phase(sk, accs["fp64", -1][i]) -
-                             client.trlwe_phase(sk, accs["exact", -1][i])).astype(np.uint32)
-                            .view(np.int32).astype(np.int64)).max()) for i in range(count))
+        def diff(a_, b_):
+            return np.abs((a_ - b_).astype(np.uint32).view(np.int32).astype(np.int64))
+        d1, dn = diff(accs["fp64", 1], accs["exact", 1]), diff(accs["fp64", -1], accs["exact", -1])
+        ph = 0
+        for i in np.flatnonzero(dn.any(axis=1)):  # identical rotations have identical phases
+            ph = max(ph, int(diff(client.trlwe_phase(sk, accs["fp64", -1][i]),
+                                  client.trlwe_phase(sk, accs["exact", -1][i])).max()))
         res["kb" if kb else "plain"] = {
-            "one_step_max_coef_diff": coef(accs["fp64", 1], accs["exact", 1]),
-            "full_rotation_max_coef_diff": coef(accs["fp64", -1], accs["exact", -1]),
+            "one_step_max_coef_diff": int(d1.max()),
+            "one_step_coefs_differing": int(np.count_nonzero(d1)),
+            "full_rotation_max_coef_diff": int(dn.max()),
+            "full_rotation_coefs_differing": int(np.count_nonzero(dn)),
+            "full_rotations_differing": int(np.count_nonzero(dn.any(axis=1))),
             "full_rotation_max_phase_diff": ph,
             "full_rotation_max_phase_diff_log2": float(np.log2(max(ph, 1)))}
     return res

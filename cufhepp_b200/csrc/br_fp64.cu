@@ -129,77 +129,84 @@ __global__ void __launch_bounds__(G * 128, G == 1 ? 3 : (G == 2 ? 2 : 1)) k_br_f
         }
         __syncthreads();
 
-        // ---- phase 2: key multiply-accumulate, thread f = frequency bin
+        // ---- phase 2: key multiply-accumulate, thread f = frequency bin.
+        // Rows outermost: each digit spectrum D[g][r] is read from shared
+        // memory once for both output polynomials, and the KeyBundle factors
+        // once per lane; per bin and output the additions run in the same
+        // order as in k_br_fp64_clu (rows 0..3, then H, x01, x0, x1), so the
+        // two kernels agree bit for bit.
         if (KB) {
             const double2* bk = bkf + (size_t)p * 3 * kTrgswF;
             for (int f = tid; f < kHalfN; f += blockDim.x) {
-                const uint32_t ef = 1u + 4u * (uint32_t)f;
-                double2 out0[G];
+                double2 s[G][2][3], h[G][2];
 #pragma unroll
-                for (int j = 0; j < 2; j++) {
-                    double2 b[3][4];
+                for (int r = 0; r < 4; r++) {
+                    double2 b[3][2];
 #pragma unroll
                     for (int e = 0; e < 3; e++)
 #pragma unroll
-                        for (int r = 0; r < 4; r++)
-                            b[e][r] = __ldg(&bk[((e * 4 + r) * 2 + j) * kHalfN + f]);
+                        for (int j = 0; j < 2; j++)
+                            b[e][j] = __ldg(&bk[((e * 4 + r) * 2 + j) * kHalfN + f]);
 #pragma unroll
                     for (int g = 0; g < G; g++) {
-                        double2 D[4];
+                        const double2 D = spec[(g * 4 + r) * kSlotStride + f];
 #pragma unroll
-                        for (int r = 0; r < 4; r++) D[r] = spec[(g * 4 + r) * kSlotStride + f];
-                        const uint32_t a0 = abar[g * kAbarStride + 2 * p];
-                        const uint32_t a1 = abar[g * kAbarStride + 2 * p + 1];
-                        double2 x0 = psi_at(psi_s, ef * a0);
-                        double2 x1 = psi_at(psi_s, ef * a1);
-                        double2 x01 = psi_at(psi_s, ef * (a0 + a1));
-                        x0.x -= 1.0;
-                        x1.x -= 1.0;
-                        x01.x -= 1.0;
-                        double2 s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0;
+                        for (int j = 0; j < 2; j++)
 #pragma unroll
-                        for (int r = 0; r < 4; r++) {
-                            s0 = cfma(s0, D[r], b[0][r]);
-                            s1 = cfma(s1, D[r], b[1][r]);
-                            s2 = cfma(s2, D[r], b[2][r]);
-                        }
-                        // FFNT(H 2^-32) = 2^-8 (d = 0), 2^-16 (d = 1) on poly j
-                        double2 o = make_double2(fma(D[2 * j].x, 0x1p-8, D[2 * j + 1].x * 0x1p-16),
-                                                 fma(D[2 * j].y, 0x1p-8, D[2 * j + 1].y * 0x1p-16));
-                        o = cfma(o, x01, s0);
-                        o = cfma(o, x0, s1);
-                        o = cfma(o, x1, s2);
-                        if (j == 0) {
-                            out0[g] = o;
-                        } else {
-                            spec[(g * 4 + 0) * kSlotStride + f] = out0[g];
-                            spec[(g * 4 + 1) * kSlotStride + f] = o;
-                        }
+                            for (int e = 0; e < 3; e++)
+                                s[g][j][e] = r == 0 ? cfma(make_double2(0.0, 0.0), D, b[e][j])
+                                                    : cfma(s[g][j][e], D, b[e][j]);
+                        // FFNT(H 2^-32) = 2^-8 (d = 0), 2^-16 (d = 1) on poly j = r / 2
+                        if ((r & 1) == 0)
+                            h[g][r >> 1] = D;
+                        else
+                            h[g][r >> 1] = make_double2(fma(h[g][r >> 1].x, 0x1p-8, D.x * 0x1p-16),
+                                                        fma(h[g][r >> 1].y, 0x1p-8, D.y * 0x1p-16));
+                    }
+                }
+                const uint32_t ef = 1u + 4u * (uint32_t)f;
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const uint32_t a0 = abar[g * kAbarStride + 2 * p];
+                    const uint32_t a1 = abar[g * kAbarStride + 2 * p + 1];
+                    double2 x0 = psi_at(psi_s, ef * a0);
+                    double2 x1 = psi_at(psi_s, ef * a1);
+                    double2 x01 = psi_at(psi_s, ef * (a0 + a1));
+                    x0.x -= 1.0;
+                    x1.x -= 1.0;
+                    x01.x -= 1.0;
+#pragma unroll
+                    for (int j = 0; j < 2; j++) {
+                        double2 o = h[g][j];
+                        o = cfma(o, x01, s[g][j][0]);
+                        o = cfma(o, x0, s[g][j][1]);
+                        o = cfma(o, x1, s[g][j][2]);
+                        spec[(g * 4 + j) * kSlotStride + f] = o;
                     }
                 }
             }
         } else {
             const double2* bk = bkf + (size_t)p * kTrgswF;
             for (int f = tid; f < kHalfN; f += blockDim.x) {
-                double2 out0[G];
+                double2 o[G][2];
 #pragma unroll
-                for (int j = 0; j < 2; j++) {
-                    double2 b[4];
+                for (int r = 0; r < 4; r++) {
+                    double2 b[2];
 #pragma unroll
-                    for (int r = 0; r < 4; r++) b[r] = __ldg(&bk[(r * 2 + j) * kHalfN + f]);
+                    for (int j = 0; j < 2; j++) b[j] = __ldg(&bk[(r * 2 + j) * kHalfN + f]);
 #pragma unroll
                     for (int g = 0; g < G; g++) {
-                        double2 o = make_double2(0.0, 0.0);
+                        const double2 D = spec[(g * 4 + r) * kSlotStride + f];
 #pragma unroll
-                        for (int r = 0; r < 4; r++)
-                            o = cfma(o, spec[(g * 4 + r) * kSlotStride + f], b[r]);
-                        if (j == 0) {
-                            out0[g] = o;
-                        } else {
-                            spec[(g * 4 + 0) * kSlotStride + f] = out0[g];
-                            spec[(g * 4 + 1) * kSlotStride + f] = o;
-                        }
+                        for (int j = 0; j < 2; j++)
+                            o[g][j] = r == 0 ? cfma(make_double2(0.0, 0.0), D, b[j])
+                                             : cfma(o[g][j], D, b[j]);
                     }
+                }
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    spec[(g * 4 + 0) * kSlotStride + f] = o[g][0];
+                    spec[(g * 4 + 1) * kSlotStride + f] = o[g][1];
                 }
             }
         }

@@ -1,7 +1,9 @@
 """Runs one engine stage on seeded synthetic inputs, for profilers.
 
     python -m cufhepp_b200.kernel_driver br_fp64 LANES [REPS]   # FP64 blind rotation (KeyBundle)
+    python -m cufhepp_b200.kernel_driver br_fp64_plain LANES [REPS]  # the same, plain key
     python -m cufhepp_b200.kernel_driver br_int8 LANES [REPS] [STEPS]  # INT8 exact rotation
+    python -m cufhepp_b200.kernel_driver br_int8_kb LANES [REPS] [STEPS]  # the same, KeyBundle key
     python -m cufhepp_b200.kernel_driver iks LANES [REPS]       # identity key switching
     python -m cufhepp_b200.kernel_driver gates LANES [REPS]     # full mixed-gate batch (lvl1)
     python -m cufhepp_b200.kernel_driver br2_fp64 LANES [REPS] [STEPS]  # lvl0 -> lvl2 rotation
@@ -36,7 +38,8 @@ def main(argv: list[str]) -> None:
     elif lvl02:
         engine.initialize_lvl02(client.EvalKey02.generate(sk, keybundle=(stage != "br2_int8")))
     else:
-        engine.initialize(client.EvalKey.generate(sk, keybundle=(stage != "br_int8")))
+        engine.initialize(client.EvalKey.generate(
+            sk, keybundle=stage not in ("br_int8", "br_fp64_plain")))
     rng = np.random.default_rng(1)
     bits = rng.integers(0, 2, lanes).astype(np.uint8)
     t0 = None
@@ -75,8 +78,8 @@ def main(argv: list[str]) -> None:
         for i in range(reps):
             engine.gate_batch(gates, lanes, engine.LVL02, d_out, *cts)
             tick(i)
-    elif stage in ("br_fp64", "br_int8"):
-        engine.set_precision(P.FP64_FFNT if stage == "br_fp64" else P.INT8_EXACT)
+    elif stage in ("br_fp64", "br_fp64_plain", "br_int8", "br_int8_kb"):
+        engine.set_precision(P.FP64_FFNT if stage.startswith("br_fp64") else P.INT8_EXACT)
         steps = int(argv[3]) if len(argv) > 3 else -1
         x = client.encrypt_bits(sk, bits, 0, seed=3)
         d_in = engine.to_device(x)
