@@ -11,6 +11,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <vector>
 
@@ -900,8 +901,18 @@ int cufhe_initialize(const cufhe_keyview* ek)
     return CUFHE_OK;
 }
 
+// engine streams of cufhe_gate_batch_sharded_host, one per shard
+static std::vector<cufhe_stream_t> g_shard_st;
+
+static void release_shard_streams()
+{
+    for (cufhe_stream_t st : g_shard_st) cufhe_stream_destroy(st);
+    g_shard_st.clear();
+}
+
 int cufhe_cleanup(void)
 {
+    release_shard_streams();
     for (int d = 0; d < kMaxDev; d++)
         if (g_dev[d].ready) release_device(d);
     cudaSetDevice(0);
@@ -1306,33 +1317,15 @@ int cufhe_circuit_plan(int level, size_t num_wires, size_t num_gates, const int3
     return CUFHE_OK;
 }
 
-int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, size_t num_gates,
+// Device form of a planned circuit: one Plan per wave over the gates
+// members[w], packed into one device buffer, and a private workspace for the
+// widest wave.  Waves may be empty (a shard of a sharded circuit).
+static int build_circuit(cufhe_circuit_t* out_c, int level, size_t num_wires, size_t num_gates,
                          const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
-                         const int32_t* in2, const int32_t* out, int device)
+                         const int32_t* in2, const int32_t* out, int device,
+                         const std::vector<std::vector<int32_t>>& members)
 {
-    if (!out_c) return fail(CUFHE_ERR_ARG, "null circuit handle");
-    *out_c = nullptr;
-    if (level != CUFHE_LVL0 && level != CUFHE_LVL1 && level != CUFHE_LVL02)
-        return fail(CUFHE_ERR_ARG, "bad level %d", level);
-    if (device < 0) device = 0;
-    if (device >= g_gpu_num) return fail(CUFHE_ERR_ARG, "device %d >= gpu num", device);
-    int sms = 148;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
-        cudaGetLastError();
-        sms = 148;
-    }
-    std::vector<int32_t> wave;
-    int nwaves = 0;
-    const int prc = plan_waves(level, num_wires, num_gates, gate_ops, in0, in1, in2, out, sms, wave,
-                               nwaves);
-    if (prc != CUFHE_OK) return prc;
-    const DeviceState& D = g_dev[device];
-    if (level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
-        return fail(CUFHE_ERR_STATE, level == CUFHE_LVL02 ? "cufhe_initialize_lvl02() not called"
-                                                         : "cufhe_initialize() not called");
-    std::vector<std::vector<int32_t>> members(nwaves);
-    for (size_t g = 0; g < num_gates; g++) members[wave[g]].push_back((int32_t)g);
-
+    const int nwaves = (int)members.size();
     // ---- per-wave plan arrays, packed into one buffer (16-byte aligned)
     auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
     std::vector<size_t> off(nwaves);
@@ -1347,6 +1340,7 @@ int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, si
         max_lanes = (int)lanes > max_lanes ? (int)lanes : max_lanes;
         max_gates = (int)n > max_gates ? (int)n : max_gates;
     }
+    if (total == 0) total = 16;
     std::vector<unsigned char> host(total, 0);
     cufhe_circuit_s* c = new cufhe_circuit_s();
     c->device = device;
@@ -1356,7 +1350,6 @@ int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, si
     c->max_lanes = max_lanes;
     c->max_gates = max_gates;
     c->exec.device = device;
-    int rc = CUFHE_OK;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaMalloc(&c->dbuf, total);
     if (e != cudaSuccess) {
@@ -1437,9 +1430,43 @@ int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, si
         circuit_free(c);
         return fail(CUFHE_ERR_NOMEM, "circuit buffers: %s", cudaGetErrorString(e));
     }
-    (void)rc;
     *out_c = c;
     return CUFHE_OK;
+}
+
+static int sms_of(int device)
+{
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 148;
+    }
+    return sms;
+}
+
+int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, size_t num_gates,
+                         const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
+                         const int32_t* in2, const int32_t* out, int device)
+{
+    if (!out_c) return fail(CUFHE_ERR_ARG, "null circuit handle");
+    *out_c = nullptr;
+    if (level != CUFHE_LVL0 && level != CUFHE_LVL1 && level != CUFHE_LVL02)
+        return fail(CUFHE_ERR_ARG, "bad level %d", level);
+    if (device < 0) device = 0;
+    if (device >= g_gpu_num) return fail(CUFHE_ERR_ARG, "device %d >= gpu num", device);
+    std::vector<int32_t> wave;
+    int nwaves = 0;
+    const int prc = plan_waves(level, num_wires, num_gates, gate_ops, in0, in1, in2, out,
+                               sms_of(device), wave, nwaves);
+    if (prc != CUFHE_OK) return prc;
+    const DeviceState& D = g_dev[device];
+    if (level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
+        return fail(CUFHE_ERR_STATE, level == CUFHE_LVL02 ? "cufhe_initialize_lvl02() not called"
+                                                         : "cufhe_initialize() not called");
+    std::vector<std::vector<int32_t>> members(nwaves);
+    for (size_t g = 0; g < num_gates; g++) members[wave[g]].push_back((int32_t)g);
+    return build_circuit(out_c, level, num_wires, num_gates, gate_ops, in0, in1, in2, out, device,
+                         members);
 }
 
 int cufhe_circuit_info(cufhe_circuit_t c, int* waves, int* max_wave_gates, int* max_wave_lanes)
@@ -1495,6 +1522,432 @@ int cufhe_circuit_destroy(cufhe_circuit_t c)
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
     circuit_free(c);
+    return CUFHE_OK;
+}
+
+// ---- sharding over devices --------------------------------------------------
+// The reference spreads gates over GPUs by giving each Stream a device in
+// turn, with every key replicated per device (include/cufhe_gpu.cuh:164-175,
+// src/cufhe_gates_gpu.cu:38-61).  Here one batch or one circuit is split over
+// `shards` shards, shard s running on device s % cufhe_set_gpu_num.  A batch
+// splits into contiguous gate ranges of balanced blind-rotation lanes; a
+// circuit splits every wave, and the wires one shard writes and another reads
+// later are copied into the reader's own wire table right after the wave
+// that writes them (stores from the writer's device into the peer's memory
+// over NVLink; no multicast).  The planners are host functions and need no
+// GPU.
+
+namespace cufhe {
+namespace {
+
+constexpr int kMaxShards = 64;
+
+static int ninputs(int op) { return (op == kNot || op == kCopy) ? 1 : ((op == kMux || op == kNMux) ? 3 : 2); }
+
+// Contiguous gate ranges [bounds[k], bounds[k + 1]) with balanced lanes (by
+// count when no gate bootstraps).
+static void plan_batch_shards(const int32_t* gates, int uniform, size_t count, int shards,
+                              std::vector<size_t>& bounds)
+{
+    bounds.assign((size_t)shards + 1, count);
+    bounds[0] = 0;
+    size_t total = 0;
+    for (size_t b = 0; b < count; b++) total += lanes_of_gate(gates ? gates[b] : uniform);
+    if (total == 0) {
+        for (int k = 1; k < shards; k++) bounds[k] = count * (size_t)k / (size_t)shards;
+        return;
+    }
+    size_t acc = 0;
+    int k = 1;
+    for (size_t b = 0; b < count && k < shards; b++) {
+        acc += lanes_of_gate(gates ? gates[b] : uniform);
+        while (k < shards && acc * (size_t)shards >= total * (size_t)k) bounds[k++] = b + 1;
+    }
+}
+
+// Waves (plan_waves) and a shard per gate: within a wave the lanes are
+// balanced (at most ceil(lanes / shards) per shard unless a gate does not
+// fit anywhere else), and a gate goes to the shard that wrote most of its
+// operands when that shard has room, which keeps chains of gates on one
+// shard and the copies few.  copies = wires that must move between shards.
+static int plan_shards(int level, size_t num_wires, size_t num_gates, const int32_t* gate_ops,
+                       const int32_t* in0, const int32_t* in1, const int32_t* in2,
+                       const int32_t* out, int sms, int shards, std::vector<int32_t>& wave,
+                       int& nwaves, std::vector<int32_t>& shard, std::vector<uint64_t>& copies)
+{
+    if (shards < 1 || shards > kMaxShards)
+        return fail(CUFHE_ERR_ARG, "shards %d outside [1, %d]", shards, kMaxShards);
+    const int rc = plan_waves(level, num_wires, num_gates, gate_ops, in0, in1, in2, out, sms, wave,
+                              nwaves);
+    if (rc != CUFHE_OK) return rc;
+    std::vector<int32_t> producer(num_wires, -1);
+    for (size_t g = 0; g < num_gates; g++) producer[out[g]] = (int32_t)g;
+    std::vector<std::vector<int32_t>> members(nwaves);
+    for (size_t g = 0; g < num_gates; g++) members[wave[g]].push_back((int32_t)g);
+    shard.assign(num_gates, 0);
+    const int32_t* ins[3] = {in0, in1, in2};
+    for (int w = 0; w < nwaves; w++) {
+        long lanes = 0;
+        for (int32_t g : members[w]) lanes += lanes_of_gate(gate_ops[g]);
+        const long target = (lanes + shards - 1) / shards;
+        std::vector<long> load(shards, 0), light(shards, 0);
+        for (int32_t g : members[w]) {
+            const int op = gate_ops[g];
+            int votes[3] = {-1, -1, -1}, pref = -1, best = 0;
+            for (int k = 0; k < ninputs(op); k++) {
+                const int32_t pg = producer[ins[k][g]];
+                votes[k] = pg >= 0 ? shard[pg] : -1;
+            }
+            for (int k = 0; k < 3; k++) {
+                if (votes[k] < 0) continue;
+                int n = 0;
+                for (int q = 0; q < 3; q++) n += votes[q] == votes[k];
+                if (n > best) best = n, pref = votes[k];
+            }
+            const long lg = lanes_of_gate(op);
+            int sh;
+            if (lg == 0) {  // Not / Copy: no rotation, stay with the operand
+                sh = pref;
+                if (sh < 0) {
+                    sh = 0;
+                    for (int q = 1; q < shards; q++) sh = light[q] < light[sh] ? q : sh;
+                }
+                light[sh]++;
+            } else if (pref >= 0 && load[pref] + lg <= target) {
+                sh = pref;
+            } else {
+                sh = 0;
+                for (int q = 1; q < shards; q++) sh = load[q] < load[sh] ? q : sh;
+            }
+            load[sh] += lg;
+            shard[g] = sh;
+        }
+    }
+    // wires to move: (wave of the writer, writer shard, reader shard, wire)
+    copies.clear();
+    for (size_t g = 0; g < num_gates; g++)
+        for (int k = 0; k < ninputs(gate_ops[g]); k++) {
+            const int32_t x = ins[k][g], pg = producer[x];
+            if (pg < 0 || shard[pg] == shard[g]) continue;
+            copies.push_back(((uint64_t)wave[pg] << 44) | ((uint64_t)shard[pg] << 38) |
+                             ((uint64_t)shard[g] << 32) | (uint32_t)x);
+        }
+    std::sort(copies.begin(), copies.end());
+    copies.erase(std::unique(copies.begin(), copies.end()), copies.end());
+    return CUFHE_OK;
+}
+
+}  // namespace
+}  // namespace cufhe
+
+// A circuit split over shards: one sub-circuit per shard (its gates of every
+// wave; waves may be empty) and, per wave, the wires each shard sends to
+// each other shard.
+struct cufhe_sharded_s {
+    int level = 0, shards = 0, nwaves = 0, words = 0;
+    size_t wires = 0, ncopies = 0;
+    std::vector<cufhe_circuit_s*> sub;
+    std::vector<int> device;
+    struct Copy {
+        int wave, from, to;
+        const int32_t* rows;  // on the sending shard's device
+        int n;
+    };
+    std::vector<Copy> copies;       // ordered by wave
+    std::vector<const int32_t*> outs;  // every wire a shard's gates write
+    std::vector<int> nouts;
+    std::vector<void*> rowbuf;
+    std::vector<cudaStream_t> st;
+    std::vector<cudaEvent_t> ev;
+};
+
+namespace cufhe {
+namespace {
+
+void sharded_free(cufhe_sharded_s* c)
+{
+    for (size_t s = 0; s < c->sub.size(); s++) {
+        cudaSetDevice(c->device[s]);
+        if (s < c->st.size() && c->st[s]) cudaStreamSynchronize(c->st[s]);
+        if (c->sub[s]) circuit_free(c->sub[s]);
+        if (s < c->rowbuf.size() && c->rowbuf[s]) cudaFree(c->rowbuf[s]);
+        if (s < c->ev.size() && c->ev[s]) cudaEventDestroy(c->ev[s]);
+        if (s < c->st.size() && c->st[s]) cudaStreamDestroy(c->st[s]);
+    }
+    delete c;
+}
+
+}  // namespace
+}  // namespace cufhe
+
+using namespace cufhe;
+
+int cufhe_batch_shard_plan(const int32_t* gates_host, int uniform_gate, size_t count, int shards,
+                           size_t* bounds)
+{
+    if (!bounds) return fail(CUFHE_ERR_ARG, "null bounds");
+    if (shards < 1 || shards > kMaxShards)
+        return fail(CUFHE_ERR_ARG, "shards %d outside [1, %d]", shards, kMaxShards);
+    std::vector<size_t> b;
+    plan_batch_shards(gates_host, uniform_gate, count, shards, b);
+    for (int k = 0; k <= shards; k++) bounds[k] = b[k];
+    return CUFHE_OK;
+}
+
+int cufhe_gate_batch_sharded_host(const int32_t* gates_host, int uniform_gate, size_t count,
+                                  int level, uint32_t* out_host, const uint32_t* in0_host,
+                                  const uint32_t* in1_host, const uint32_t* in2_host, int shards)
+{
+    if (shards <= 0) shards = g_gpu_num;
+    if (shards > kMaxShards) return fail(CUFHE_ERR_ARG, "shards %d > %d", shards, kMaxShards);
+    if (level != CUFHE_LVL0 && level != CUFHE_LVL1 && level != CUFHE_LVL02)
+        return fail(CUFHE_ERR_ARG, "bad level %d", level);
+    if (count == 0) return CUFHE_OK;
+    if (!out_host || !in0_host) return fail(CUFHE_ERR_ARG, "null ciphertext pointer");
+    const size_t words = level == CUFHE_LVL1 ? kTlwe1 : kTlwe0;
+    std::vector<size_t> bounds;
+    plan_batch_shards(gates_host, uniform_gate, count, shards, bounds);
+    // one engine stream per shard, on device shard % gpu num
+    for (int k = 0; k < shards; k++) {
+        const int dev = k % g_gpu_num;
+        if (k < (int)g_shard_st.size() && g_shard_st[k]->device != dev) {
+            cufhe_stream_destroy(g_shard_st[k]);
+            g_shard_st[k] = nullptr;
+        }
+        if (k >= (int)g_shard_st.size()) g_shard_st.push_back(nullptr);
+        if (!g_shard_st[k]) {
+            const int rc = cufhe_stream_create(&g_shard_st[k], dev);
+            if (rc) return rc;
+        }
+    }
+    for (int k = 0; k < shards; k++) {
+        const size_t b0 = bounds[k], n = bounds[k + 1] - b0;
+        if (!n) continue;
+        const int rc = cufhe_gate_batch_host(
+            gates_host ? gates_host + b0 : nullptr, uniform_gate, n, level, out_host + b0 * words,
+            in0_host + b0 * words, in1_host ? in1_host + b0 * words : nullptr,
+            in2_host ? in2_host + b0 * words : nullptr, g_shard_st[k]);
+        if (rc) return rc;
+    }
+    for (int k = 0; k < shards; k++) {
+        const int rc = cufhe_stream_synchronize(g_shard_st[k]);
+        if (rc) return rc;
+    }
+    return CUFHE_OK;
+}
+
+int cufhe_circuit_shard_plan(int level, size_t num_wires, size_t num_gates, const int32_t* gate_ops,
+                             const int32_t* in0, const int32_t* in1, const int32_t* in2,
+                             const int32_t* out, int sms, int shards, int32_t* wave_of_gate,
+                             int32_t* shard_of_gate, int* num_waves, size_t* num_copies)
+{
+    if (!wave_of_gate || !shard_of_gate || !num_waves) return fail(CUFHE_ERR_ARG, "null plan output");
+    std::vector<int32_t> wave, shard;
+    std::vector<uint64_t> copies;
+    int nwaves = 0;
+    const int rc = plan_shards(level, num_wires, num_gates, gate_ops, in0, in1, in2, out, sms,
+                               shards, wave, nwaves, shard, copies);
+    if (rc != CUFHE_OK) return rc;
+    for (size_t g = 0; g < num_gates; g++) {
+        wave_of_gate[g] = wave[g];
+        shard_of_gate[g] = shard[g];
+    }
+    *num_waves = nwaves;
+    if (num_copies) *num_copies = copies.size();
+    return CUFHE_OK;
+}
+
+int cufhe_sharded_create(cufhe_sharded_t* out_c, int level, size_t num_wires, size_t num_gates,
+                         const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
+                         const int32_t* in2, const int32_t* out, int shards)
+{
+    if (!out_c) return fail(CUFHE_ERR_ARG, "null circuit handle");
+    *out_c = nullptr;
+    if (shards <= 0) shards = g_gpu_num;
+    std::vector<int32_t> wave, shard;
+    std::vector<uint64_t> copies;
+    int nwaves = 0;
+    int rc = plan_shards(level, num_wires, num_gates, gate_ops, in0, in1, in2, out, sms_of(0),
+                         shards, wave, nwaves, shard, copies);
+    if (rc != CUFHE_OK) return rc;
+    for (int k = 0; k < shards && k < g_gpu_num; k++) {
+        const DeviceState& D = g_dev[k];
+        if (level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
+            return fail(CUFHE_ERR_STATE, "keys of the circuit's level are not initialised on "
+                                         "device %d", k);
+    }
+    cufhe_sharded_s* c = new cufhe_sharded_s();
+    c->level = level;
+    c->shards = shards;
+    c->nwaves = nwaves;
+    c->wires = num_wires;
+    c->words = level == CUFHE_LVL1 ? kTlwe1 : kTlwe0;
+    c->ncopies = copies.size();
+    c->sub.assign(shards, nullptr);
+    c->rowbuf.assign(shards, nullptr);
+    c->st.assign(shards, nullptr);
+    c->ev.assign(shards, nullptr);
+    c->outs.assign(shards, nullptr);
+    c->nouts.assign(shards, 0);
+    for (int k = 0; k < shards; k++) c->device.push_back(k % g_gpu_num);
+    // peer access between the devices in use (stores into a peer's table)
+    for (int a = 0; a < shards && a < g_gpu_num; a++)
+        for (int b = 0; b < shards && b < g_gpu_num; b++) {
+            if (a == b) continue;
+            int ok = 0;
+            cudaDeviceCanAccessPeer(&ok, a, b);
+            if (!ok) {
+                sharded_free(c);
+                return fail(CUFHE_ERR_STATE, "device %d cannot access device %d's memory", a, b);
+            }
+            cudaSetDevice(a);
+            const cudaError_t e = cudaDeviceEnablePeerAccess(b, 0);
+            if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled) {
+                sharded_free(c);
+                return fail(CUFHE_ERR_CUDA, "peer access %d -> %d: %s", a, b, cudaGetErrorString(e));
+            }
+            cudaGetLastError();
+        }
+    // per shard: the sub-circuit, and one device buffer with its outgoing
+    // copy rows (grouped by wave and reader) followed by its output rows
+    for (int k = 0; k < shards; k++) {
+        std::vector<std::vector<int32_t>> members(nwaves);
+        std::vector<int32_t> rows;
+        for (size_t g = 0; g < num_gates; g++)
+            if (shard[g] == k) members[wave[g]].push_back((int32_t)g);
+        rc = build_circuit(&c->sub[k], level, num_wires, num_gates, gate_ops, in0, in1, in2, out,
+                           c->device[k], members);
+        if (rc != CUFHE_OK) {
+            sharded_free(c);
+            return rc;
+        }
+        struct Pending { int wave, to; size_t off; int n; };
+        std::vector<Pending> mine;
+        for (size_t i = 0; i < copies.size();) {
+            const uint64_t key = copies[i] >> 32;
+            const int w = (int)(key >> 12), from = (int)((key >> 6) & 63), to = (int)(key & 63);
+            size_t j = i;
+            while (j < copies.size() && (copies[j] >> 32) == key) j++;
+            if (from == k) {
+                mine.push_back({w, to, rows.size(), (int)(j - i)});
+                for (size_t q = i; q < j; q++) rows.push_back((int32_t)(copies[q] & 0xFFFFFFFFu));
+            }
+            i = j;
+        }
+        const size_t out_off = rows.size();
+        for (size_t g = 0; g < num_gates; g++)
+            if (shard[g] == k) rows.push_back(out[g]);
+        cudaError_t e = cudaSetDevice(c->device[k]);
+        if (e == cudaSuccess && !rows.empty()) e = cudaMalloc(&c->rowbuf[k], rows.size() * 4);
+        if (e == cudaSuccess && !rows.empty())
+            e = cudaMemcpy(c->rowbuf[k], rows.data(), rows.size() * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            sharded_free(c);
+            return fail(CUFHE_ERR_NOMEM, "sharded circuit buffers: %s", cudaGetErrorString(e));
+        }
+        const int32_t* base = static_cast<const int32_t*>(c->rowbuf[k]);
+        for (const Pending& q : mine) c->copies.push_back({q.wave, k, q.to, base + q.off, q.n});
+        c->outs[k] = base + out_off;
+        c->nouts[k] = (int)(rows.size() - out_off);
+    }
+    std::stable_sort(c->copies.begin(), c->copies.end(),
+                     [](const cufhe_sharded_s::Copy& a, const cufhe_sharded_s::Copy& b) {
+                         return a.wave < b.wave;
+                     });
+    *out_c = c;
+    return CUFHE_OK;
+}
+
+int cufhe_sharded_info(cufhe_sharded_t c, int* waves, size_t* copies, int* shards)
+{
+    if (!c) return fail(CUFHE_ERR_ARG, "null circuit");
+    if (waves) *waves = c->nwaves;
+    if (copies) *copies = c->ncopies;
+    if (shards) *shards = c->shards;
+    return CUFHE_OK;
+}
+
+int cufhe_sharded_device(cufhe_sharded_t c, int shard)
+{
+    if (!c || shard < 0 || shard >= c->shards) return fail(CUFHE_ERR_ARG, "bad shard");
+    return c->device[shard];
+}
+
+int cufhe_sharded_run(cufhe_sharded_t c, uint32_t* const* wires)
+{
+    if (!c || !wires) return fail(CUFHE_ERR_ARG, "null circuit or wire tables");
+    for (int k = 0; k < c->shards; k++)
+        if (!wires[k]) return fail(CUFHE_ERR_ARG, "null wire table of shard %d", k);
+    for (int k = 0; k < c->shards && k < g_gpu_num; k++)
+        if (c->level == CUFHE_LVL02 ? !g_dev[k].ready2 : !g_dev[k].ready)
+            return fail(CUFHE_ERR_STATE, "keys of the circuit's level are not initialised");
+    size_t ci = 0;
+    std::vector<char> sent(c->shards);
+    for (int w = 0; w < c->nwaves; w++) {
+        for (int k = 0; k < c->shards; k++) {
+            CK(cudaSetDevice(c->device[k]));
+            c->sub[k]->exec.st = c->st[k];
+            const int rc = run_wave(c->sub[k], w, wires[k]);
+            if (rc) return rc;
+        }
+        // this wave's copies, on the writer's stream right after its gates;
+        // each reader waits for its writers before its next wave
+        const size_t c0 = ci;
+        std::fill(sent.begin(), sent.end(), 0);
+        for (; ci < c->copies.size() && c->copies[ci].wave == w; ci++) {
+            const cufhe_sharded_s::Copy& q = c->copies[ci];
+            CK(cudaSetDevice(c->device[q.from]));
+            LAUNCH(CUFHE_K_FINALIZE, c->st[q.from],
+                   launch_copy_rows(q.rows, q.n, c->words, wires[q.from], wires[q.to],
+                                    c->st[q.from]));
+            sent[q.from] = 1;
+        }
+        for (int k = 0; k < c->shards; k++)
+            if (sent[k]) {
+                CK(cudaSetDevice(c->device[k]));
+                CK(cudaEventRecord(c->ev[k], c->st[k]));
+            }
+        for (size_t q = c0; q < ci; q++) {
+            const cufhe_sharded_s::Copy& cp = c->copies[q];
+            CK(cudaSetDevice(c->device[cp.to]));
+            CK(cudaStreamWaitEvent(c->st[cp.to], c->ev[cp.from], 0));
+        }
+    }
+    return CUFHE_OK;
+}
+
+int cufhe_sharded_collect(cufhe_sharded_t c, uint32_t* const* wires, int dst)
+{
+    if (!c || !wires) return fail(CUFHE_ERR_ARG, "null circuit or wire tables");
+    if (dst < 0 || dst >= c->shards) return fail(CUFHE_ERR_ARG, "bad shard %d", dst);
+    for (int k = 0; k < c->shards; k++) {
+        if (k == dst || !c->nouts[k]) continue;
+        CK(cudaSetDevice(c->device[k]));
+        LAUNCH(CUFHE_K_FINALIZE, c->st[k],
+               launch_copy_rows(c->outs[k], c->nouts[k], c->words, wires[k], wires[dst], c->st[k]));
+        CK(cudaEventRecord(c->ev[k], c->st[k]));
+        CK(cudaSetDevice(c->device[dst]));
+        CK(cudaStreamWaitEvent(c->st[dst], c->ev[k], 0));
+    }
+    return CUFHE_OK;
+}
+
+int cufhe_sharded_synchronize(cufhe_sharded_t c)
+{
+    if (!c) return fail(CUFHE_ERR_ARG, "null circuit");
+    for (int k = 0; k < c->shards; k++) {
+        CK(cudaSetDevice(c->device[k]));
+        CK(cudaStreamSynchronize(c->st[k]));
+    }
+    return cufhe_synchronize();
+}
+
+int cufhe_sharded_destroy(cufhe_sharded_t c)
+{
+    if (!c) return CUFHE_OK;
+    sharded_free(c);
     return CUFHE_OK;
 }
 

@@ -200,6 +200,10 @@ cudaError_t launch_finalize_lvl1(const Plan& plan, const uint32_t* lane_out, uin
 
 cudaError_t launch_not_copy(const Plan& plan, int words, const uint32_t* in0, uint32_t* out,
                             cudaStream_t st);
+// rows[0..nrows) of the wire table src copied into dst (same rows); dst may
+// be a peer device's memory (peer access enabled)
+cudaError_t launch_copy_rows(const int32_t* rows, int nrows, int words, const uint32_t* src,
+                             uint32_t* dst, cudaStream_t st);
 
 // FP64 FFNT blind rotation + SampleExtract of `lanes` lvl0 TLWEs.
 // acc_out (optional) receives the TRLWE accumulators; lane_out (optional) the

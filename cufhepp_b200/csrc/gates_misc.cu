@@ -5,6 +5,10 @@
 //   k_finalize_lvl1 lane outputs -> gate outputs of the IKS->BR order
 //                   (Mux: + mu, NMux: negate - mu; src/bootstrap_gpu.cu:1557-1672)
 //   k_not_copy      Not / Copy (src/bootstrap_gpu.cu:2200-2222)
+//   k_copy_rows     wire rows of one shard's wire table into another shard's
+//                   table at the same rows (sharded circuits); the
+//                   destination may be a peer GPU's memory, written over
+//                   NVLink by this device's stores
 #include "engine.h"
 
 namespace cufhe {
@@ -58,7 +62,25 @@ __global__ void k_not_copy(Plan plan, int words, const uint32_t* __restrict__ in
     for (int i = threadIdx.x; i < words; i += blockDim.x) d[i] = op == kNot ? 0u - s[i] : s[i];
 }
 
+// one CTA per listed row; words are 4-byte aligned only (a lvl1 row is 4100 B)
+__global__ void k_copy_rows(const int32_t* __restrict__ rows, int nrows, int words,
+                            const uint32_t* __restrict__ src, uint32_t* __restrict__ dst)
+{
+    const int r = blockIdx.x;
+    if (r >= nrows) return;
+    const size_t base = (size_t)rows[r] * words;
+    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[base + i] = src[base + i];
+}
+
 }  // namespace
+
+cudaError_t launch_copy_rows(const int32_t* rows, int nrows, int words, const uint32_t* src,
+                             uint32_t* dst, cudaStream_t st)
+{
+    if (nrows <= 0) return cudaSuccess;
+    k_copy_rows<<<nrows, 256, 0, st>>>(rows, nrows, words, src, dst);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_preadd_lvl0(const Plan& plan, const uint32_t* in0, const uint32_t* in1,
                                const uint32_t* in2, uint32_t* lane_in, cudaStream_t st)

@@ -76,6 +76,17 @@ SIGNATURES = {
     "cufhe_cmux": ([_i, _vp, _vp, _vp, _vp, _sz, _vp], _i),
     "cufhe_lut_eval": ([_vp, _sz, _vp, _u32, _vp, _vp], _i),
     "cufhe_autotune_table": ([_vp, _vp, _i], _i),
+    "cufhe_batch_shard_plan": ([_vp, _i, _sz, _i, _vp], _i),
+    "cufhe_gate_batch_sharded_host": ([_vp, _i, _sz, _i, _vp, _vp, _vp, _vp, _i], _i),
+    "cufhe_circuit_shard_plan": ([_i, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp,
+                                  _vp], _i),
+    "cufhe_sharded_create": ([_vp, _i, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i], _i),
+    "cufhe_sharded_info": ([_vp, _vp, _vp, _vp], _i),
+    "cufhe_sharded_device": ([_vp, _i], _i),
+    "cufhe_sharded_run": ([_vp, _vp], _i),
+    "cufhe_sharded_collect": ([_vp, _vp, _i], _i),
+    "cufhe_sharded_synchronize": ([_vp], _i),
+    "cufhe_sharded_destroy": ([_vp], _i),
 }
 
 (K_IKS, K_PREADD, K_BR_FP64, K_BR_INT8, K_FINALIZE, K_BR_FP64_LVL02, K_IKS_LVL20, K_PRIVKS,
@@ -379,6 +390,105 @@ class Circuit:
     def destroy(self) -> None:
         if getattr(self, "h", None):
             load().cufhe_circuit_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def batch_shard_plan(gates, count: int, shards: int, uniform: int = 0) -> np.ndarray:
+    """cufhe_batch_shard_plan (host only): bounds[0..shards] of the contiguous
+    gate ranges of a batch split over `shards` shards with balanced lanes."""
+    g = None if gates is None else np.ascontiguousarray(gates, np.int32)
+    bounds = np.zeros(shards + 1, np.uint64)
+    check(load().cufhe_batch_shard_plan(_p(g), uniform, count, shards, _p(bounds)),
+          "batch_shard_plan")
+    return bounds.astype(np.int64)
+
+
+def gate_batch_sharded_host(gates, level: int, in0, in1=None, in2=None, shards: int = 0,
+                            uniform: int = 0) -> np.ndarray:
+    """cufhe_gate_batch_sharded_host: one host batch split over shards (shard s
+    on device s % gpu num); returns when every shard is done."""
+    words = P.TLWE1_WORDS if level == LVL1 else P.TLWE0_WORDS
+    in0 = np.ascontiguousarray(in0, np.uint32).reshape(-1, words)
+    count = in0.shape[0]
+    out = np.empty((count, words), np.uint32)
+    g = None if gates is None else np.ascontiguousarray(gates, np.int32)
+    i1 = None if in1 is None else np.ascontiguousarray(in1, np.uint32)
+    i2 = None if in2 is None else np.ascontiguousarray(in2, np.uint32)
+    check(load().cufhe_gate_batch_sharded_host(_p(g), uniform, count, level, _p(out), _p(in0),
+                                               _p(i1), _p(i2), shards), "gate_batch_sharded_host")
+    return out
+
+
+def circuit_shard_plan(level: int, num_wires: int, ops, in0, in1, in2, out, shards: int,
+                       sms: int = 0):
+    """cufhe_circuit_shard_plan (host only, no GPU or keys): returns (wave of
+    every gate, shard of every gate, number of waves, number of wire copies)."""
+    ops = np.ascontiguousarray(ops, np.int32)
+    arrs = [np.ascontiguousarray(x, np.int32) for x in (in0, in1, in2, out)]
+    wave = np.empty(ops.size, np.int32)
+    shard = np.empty(ops.size, np.int32)
+    n = C.c_int()
+    nc = C.c_size_t()
+    check(load().cufhe_circuit_shard_plan(level, num_wires, ops.size, _p(ops),
+                                          *(_p(a) for a in arrs), sms, shards, _p(wave),
+                                          _p(shard), C.byref(n), C.byref(nc)),
+          "circuit_shard_plan")
+    return wave, shard, n.value, nc.value
+
+
+class ShardedCircuit:
+    """One circuit split over shards (cufhe_sharded_create): every shard runs
+    its part of each wave on device shard % gpu num against its own wire
+    table, and wires cross between shards' tables after the wave that writes
+    them."""
+
+    def __init__(self, level: int, num_wires: int, ops, in0, in1, in2, out, shards: int = 0):
+        arr = lambda a: np.ascontiguousarray(a, np.int32)  # noqa: E731
+        self.ops, self.in0, self.in1, self.in2, self.out = (arr(x) for x in (ops, in0, in1, in2,
+                                                                            out))
+        self.level = level
+        self.num_wires = int(num_wires)
+        h = C.c_void_p()
+        check(load().cufhe_sharded_create(C.byref(h), level, self.num_wires, self.ops.size,
+                                          _p(self.ops), _p(self.in0), _p(self.in1),
+                                          _p(self.in2), _p(self.out), shards), "sharded_create")
+        self.h = h
+
+    def info(self) -> tuple[int, int, int]:
+        """(waves, wire copies, shards)"""
+        w, c, s = C.c_int(), C.c_size_t(), C.c_int()
+        check(load().cufhe_sharded_info(self.h, C.byref(w), C.byref(c), C.byref(s)),
+              "sharded_info")
+        return w.value, c.value, s.value
+
+    def device(self, shard: int) -> int:
+        d = load().cufhe_sharded_device(self.h, shard)
+        if d < 0:
+            check(d, "sharded_device")
+        return d
+
+    @staticmethod
+    def _tables(wires) -> C.Array:
+        return (C.c_void_p * len(wires))(*[dptr(w).value for w in wires])
+
+    def run(self, wires) -> None:
+        check(load().cufhe_sharded_run(self.h, self._tables(wires)), "sharded_run")
+
+    def collect(self, wires, dst: int = 0) -> None:
+        check(load().cufhe_sharded_collect(self.h, self._tables(wires), dst), "sharded_collect")
+
+    def synchronize(self) -> None:
+        check(load().cufhe_sharded_synchronize(self.h), "sharded_synchronize")
+
+    def destroy(self) -> None:
+        if getattr(self, "h", None):
+            load().cufhe_sharded_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -270,6 +270,57 @@ int cufhe_circuit_wave_sizes(cufhe_circuit_t c, int32_t* gates, int32_t* lanes, 
 int cufhe_circuit_run(cufhe_circuit_t c, uint32_t* wires, cufhe_stream_t st, int use_graph);
 int cufhe_circuit_destroy(cufhe_circuit_t c);
 
+/* ---- one batch or one circuit over several GPUs -------------------------
+ * The reference spreads work over GPUs only through the device each Stream
+ * is given in turn, with the keys replicated on every GPU
+ * (include/cufhe_gpu.cuh:164-175, src/cufhe_gates_gpu.cu:38-61); that stays
+ * available here (cufhe_stream_create with device -1).  These entry points
+ * split ONE batch or ONE circuit over `shards` shards (<= 0: the
+ * cufhe_set_gpu_num count, at most 64); shard s runs on device
+ * s % cufhe_set_gpu_num, each with its own key replica.  Gates are
+ * independent, so a batch needs no data exchange: it splits into contiguous
+ * gate ranges with balanced blind-rotation lanes.  A circuit splits every
+ * wave (lanes balanced per wave; a gate preferably joins the shard that wrote
+ * its operands), and each wire that one shard writes and another reads later
+ * is copied into the reader's own wire table right after the wave that
+ * writes it (the writer's device stores into the peer's memory; peer access
+ * is enabled between the devices in use).
+ *
+ * cufhe_batch_shard_plan: host only; bounds[0..shards] with shard k holding
+ * gates [bounds[k], bounds[k + 1]).
+ * cufhe_gate_batch_sharded_host: cufhe_gate_batch_host split that way, each
+ * shard on an engine stream of its device; returns when all shards are done.
+ * cufhe_circuit_shard_plan: host only (no GPU, no keys); the waves of
+ * cufhe_circuit_plan, a shard per gate, and the number of wire copies.
+ * cufhe_sharded_create: the same plan on the devices (keys initialised on
+ * each device in use).  cufhe_sharded_run(c, wires): wires[s] is shard s's
+ * wire table [num_wires][words] on its device (cufhe_sharded_device); the
+ * circuit's input wires must be in every shard's table before the call.  The
+ * run is asynchronous; after it each shard's table holds the wires its gates
+ * wrote and the wires it received.  cufhe_sharded_collect(c, wires, dst)
+ * copies every gate output into shard dst's table; cufhe_sharded_synchronize
+ * waits for both.  Runs of one sharded circuit must not overlap. */
+typedef struct cufhe_sharded_s* cufhe_sharded_t;
+int cufhe_batch_shard_plan(const int32_t* gates_host, int uniform_gate, size_t count, int shards,
+                           size_t* bounds);
+int cufhe_gate_batch_sharded_host(const int32_t* gates_host, int uniform_gate, size_t count,
+                                  int level, uint32_t* out_host, const uint32_t* in0_host,
+                                  const uint32_t* in1_host, const uint32_t* in2_host, int shards);
+int cufhe_circuit_shard_plan(int level, size_t num_wires, size_t num_gates, const int32_t* gate_ops,
+                             const int32_t* in0, const int32_t* in1, const int32_t* in2,
+                             const int32_t* out, int sms, int shards, int32_t* wave_of_gate,
+                             int32_t* shard_of_gate, int* num_waves, size_t* num_copies);
+int cufhe_sharded_create(cufhe_sharded_t* c, int level, size_t num_wires, size_t num_gates,
+                         const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
+                         const int32_t* in2, const int32_t* out, int shards);
+int cufhe_sharded_info(cufhe_sharded_t c, int* waves, size_t* copies, int* shards);
+/* device of a shard (or a negative error code) */
+int cufhe_sharded_device(cufhe_sharded_t c, int shard);
+int cufhe_sharded_run(cufhe_sharded_t c, uint32_t* const* wires);
+int cufhe_sharded_collect(cufhe_sharded_t c, uint32_t* const* wires, int dst);
+int cufhe_sharded_synchronize(cufhe_sharded_t c);
+int cufhe_sharded_destroy(cufhe_sharded_t c);
+
 /* ---- circuit bootstrapping, CMUX, lookup tables ----------------------- */
 /* Gadgets of TRGSW<lvl1> (N = 1024, Torus32): */
 #define CUFHE_GADGET_LVL1 0 /* l = 2, Bgbit = 8: the bootstrapping gadget (lvl1param) */
