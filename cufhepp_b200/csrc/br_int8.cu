@@ -37,6 +37,11 @@
 // accumulator.  Hand-offs go through mbarriers only; every wait is bounded
 // and reports a timeout through an error flag instead of hanging.
 #include <stdio.h>
+#include <stdlib.h>
+
+#include <atomic>
+
+#include <cuda.h>
 
 #include "br_int8.h"
 #include "engine.h"
@@ -520,6 +525,313 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
                      "r"(kTmemCols));
 }
 
+// ---- CTA-pair form of the step GEMM (tcgen05 cta_group::2) ----------------
+// A cluster of two CTAs on two SMs shares every digit tile: each CTA copies
+// its half of the tile's 256 lanes (16 KB per chunk instead of 32) and
+// generates the Toeplitz A rows of its own (key, output polynomial) combo,
+// and the even CTA issues M = 256 MMAs (128 rows in each CTA's TMEM, lanes
+// split between the two CTAs' shared memory) for both.  Each SM therefore
+// moves half the digit bytes and issues half the MMAs of k_i8_gemm_p for the
+// same work.  Rank r of a pair serves output polynomial r; pair type
+// (KeyBundle: the key of the pair) = cluster mod kPairTypes.
+//   warps 0-7   generators (own combo), as in k_i8_gemm_p
+//   warp 8      even CTA: MMA issue for the pair; its chunk barrier counts
+//               both CTAs' digit bytes (the odd CTA's tensor copies complete
+//               on it) and both CTAs' generators (the odd CTA's warps arrive
+//               remotely), and the odd CTA's drain warps release the
+//               accumulator remotely; every MMA batch commits to the
+//               barriers of both CTAs
+//   warps 9, 26 producers: own half of each digit chunk, own key window
+//   warps 10-25 drainers (own 128 rows of the accumulator), as in k_i8_gemm_p
+// Every wait is bounded; both CTAs always meet at the closing cluster barrier
+// before the pair releases its TMEM.
+constexpr int kHalfTile = kTileBytes / 2;                                  // 16 KB
+constexpr size_t kSmemPairB = (size_t)kPStages * kHalfTile;                // 80 KB
+constexpr size_t kSmemGemmPair = 1024 + kSmemPairB + kSmemPV + kSmemPRed + 512;
+constexpr uint32_t kIdescPair = idesc_i8(256, kGroup);
+
+template <bool KB>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmPThreads, 1)
+    k_i8_gemm_2sm(const __grid_constant__ CUtensorMap tmap, const int8_t* __restrict__ vkey,
+                  const uint8_t* __restrict__ tiles,
+                  uint32_t* __restrict__ acc, int lanes, int tiles_j, int split,
+                  const uint16_t* __restrict__ abar, int pair, int* __restrict__ err)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t raw_addr = smem_u32(smem_raw);
+    unsigned char* smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
+    unsigned char* bst = smem;
+    int8_t* vs = reinterpret_cast<int8_t*>(smem + kSmemPairB);
+    uint32_t* red = reinterpret_cast<uint32_t*>(smem + kSmemPairB + kSmemPV);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kSmemPairB + kSmemPV + kSmemPRed);
+    uint64_t* full = bars;                    // [kPStages]
+    uint64_t* empty = full + kPStages;        // [kPStages]
+    uint64_t* acc_full = empty + kPStages;
+    uint64_t* acc_empty = acc_full + 1;
+    uint64_t* bar_v = acc_empty + 1;
+    uint64_t* red_full = bar_v + 1;
+    uint64_t* red_clear = red_full + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(red_clear + 1);
+    __shared__ volatile int s_fail;
+    __shared__ int s_geo[5];
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t rank = cluster_rank();
+    constexpr int kPairTypes = KB ? 3 : 1;
+    const int q = (int)(blockIdx.x >> 1);
+    const int combo = (q % kPairTypes) * 2 + (int)rank, j_out = (int)rank;
+    const int cb = q / kPairTypes, ncj = (int)(gridDim.x >> 1) / kPairTypes;
+    const int R = tiles_j / ncj, NU = (tiles_j - R * ncj) * split;
+    const int T = R + (cb < NU ? (NU - 1 - cb) / ncj + 1 : 0);
+
+    for (size_t i = tid; i < kRedWords; i += blockDim.x) red[i] = 0u;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(tmem_slot)), "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    if (tid == 0) {
+        s_fail = 0;
+        s_geo[0] = R;
+        s_geo[1] = cb;
+        s_geo[2] = ncj;
+        s_geo[3] = split;
+        s_geo[4] = combo;
+        for (int s = 0; s < kPStages; s++) {
+            // (even CTA) 128 own generator threads, its producer, 4 odd generator warps
+            mbar_init(&full[s], 128 + 1 + 4);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        mbar_init(acc_empty, 2 * kDrainWarps);  // (even CTA) both CTAs' drain warps
+        mbar_init(bar_v, 1);
+        mbar_init(red_full, kDrainWarps);
+        mbar_init(red_clear, kDrainWarps);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();  // both CTAs' barriers exist before any remote arrival
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 9 || warp == 10 + kDrainWarps) {
+        // ---- producers: this CTA's half (lanes 128 r ..) of each digit chunk
+        const int par = warp == 9 ? 0 : 1;
+        if (lane == 0) {
+            if (par == 0) {
+                mbar_expect_tx(bar_v, (uint32_t)kSmemPV);
+                bulk_g2s(vs, vkey + (size_t)combo * kVBytesJ, (uint32_t)kSmemPV, bar_v);
+            }
+            asm volatile("griddepcontrol.wait;" ::: "memory");
+            int gbase = 0;
+            for (int it = 0; it < T && !s_fail; it++) {
+                int t, k0, nk;
+                unit_of(it, s_geo, t, k0, nk);
+                const int group = t / (kN / kRowsCoef);
+                const uint8_t* gt = tiles + (size_t)group * kChunks * kTileBytes;
+                for (int lk = par; lk < nk; lk += 2) {
+                    const int kc = k0 + lk, gc = gbase + lk, s = gc % kPStages;
+                    if (s_fail) break;
+                    if (gc >= kPStages &&
+                        !mbar_wait(&empty[s], (uint32_t)((gc / kPStages) - 1) & 1)) {
+                        s_fail = 1;
+                        break;
+                    }
+                    if (rank == 0) {
+                        // both halves' bytes land on this barrier
+                        mbar_expect_tx(&full[s], kTileBytes);
+                        bulk_g2s(bst + s * kHalfTile, gt + (size_t)kc * kTileBytes, kHalfTile,
+                                 &full[s]);
+                    } else {
+                        // rows 128..255 of chunk kc of the group, as 128 rows x 128 B
+                        tma2d_g2s_to_even(bst + s * kHalfTile, &tmap, 0,
+                                          (group * kChunks + kc) * kGroup + 128, &full[s]);
+                    }
+                }
+                gbase += nk;
+            }
+        }
+    } else if (warp == 8) {
+        if (lane == 0 && rank == 0) {
+            // ---- MMA issue for the pair
+            int gc = 0;
+            for (int it = 0; it < T && !s_fail; it++) {
+                int t, k0, nk;
+                unit_of(it, s_geo, t, k0, nk);
+                if (it >= 1 && !mbar_wait(acc_empty, (uint32_t)(it - 1) & 1)) {
+                    s_fail = 1;
+                    break;
+                }
+                tc_fence_after();
+                for (int lk = 0; lk < nk; lk++, gc++) {
+                    const int s = gc % kPStages;
+                    if (!mbar_wait(&full[s], (uint32_t)(gc / kPStages) & 1)) {
+                        s_fail = 1;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t bbase = smem_u32(bst + s * kHalfTile);
+#pragma unroll
+                    for (int k = 0; k < kChunkK / 32; k++)
+                        tc_mma_i8_pair(tmem + kAccCol, tmem + kACol + 32 * s + 8 * k,
+                                       desc_kmajor_sw128(bbase + 32 * k), kIdescPair, (lk | k) != 0);
+                    tc_commit_pair(&empty[s]);
+                }
+                if (s_fail) break;
+                tc_commit_pair(acc_full);
+            }
+        }
+    } else if (warp < 8) {
+        // ---- generators: this CTA's combo, chunks of parity wg
+        const int wg = warp >> 2, qd = warp & 3;
+        const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
+        bool ok = __all_sync(0xffffffffu, mbar_wait(bar_v, 0));
+        int gbase = 0;
+        for (int it = 0; it < T && ok; it++) {
+            int t, k0, nk;
+            unit_of(it, s_geo, t, k0, nk);
+            const int n = (t % (kN / kRowsCoef)) * kRowsCoef + lane;
+            for (int lk = wg; lk < nk; lk += 2) {
+                const int kc = k0 + lk, gc = gbase + lk, s = gc % kPStages;
+                if (__any_sync(0xffffffffu, s_fail != 0)) {
+                    ok = false;
+                    break;
+                }
+                if (gc >= kPStages &&
+                    !__all_sync(0xffffffffu,
+                                mbar_wait(&empty[s], (uint32_t)((gc / kPStages) - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const int r = kc / (kN / kChunkK), m0 = (kc % (kN / kChunkK)) * kChunkK;
+                const uint32_t* vw =
+                    reinterpret_cast<const uint32_t*>(vs + (size_t)(r * 4 + qd) * (2 * kN));
+                const int sst = kN - 1 - n + m0;
+                const int w0 = sst >> 2, sh = (sst & 3) * 8;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    uint32_t w[17];
+#pragma unroll
+                    for (int i = 0; i < 17; i++) w[i] = vw[w0 + 16 * h + i];
+                    uint32_t a[16];
+#pragma unroll
+                    for (int i = 0; i < 16; i++) a[i] = __funnelshift_r(w[i], w[i + 1], sh);
+                    tmem_st16(tmem + lane_base + kACol + 32 * s + 16 * h, a);
+                }
+                tmem_wait_st();
+                tc_fence_before();
+                if (rank == 0) {
+                    mbar_arrive(&full[s]);
+                } else {
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive_cluster(&full[s], 0);
+                }
+            }
+            gbase += nk;
+        }
+        if (!ok) s_fail = 1;
+    } else {
+        // ---- drainers: this CTA's 128 rows (its combo), all 256 lanes
+        const int d = warp - 10, qd = warp & 3, pq = d >> 2;
+        const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        bool ok = true;
+        for (int it = 0; it < T && ok; it++) {
+            if (__any_sync(0xffffffffu, s_fail != 0) ||
+                !__all_sync(0xffffffffu, mbar_wait(acc_full, (uint32_t)it & 1))) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            uint32_t v0[32], v1[32];
+            tmem_ld32(tmem + lane_base + kAccCol + 64 * pq, v0);
+            tmem_ld32(tmem + lane_base + kAccCol + 64 * pq + 32, v1);
+            tmem_wait_ld();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                if (rank == 0)
+                    mbar_arrive(acc_empty);
+                else
+                    mbar_arrive_cluster(acc_empty, 0);
+            }
+#pragma unroll
+            for (int i = 0; i < 32; i++)
+                atomicAdd(&red[(size_t)(64 * pq + i) * kRowsCoef + lane], v0[i] << (8 * qd));
+#pragma unroll
+            for (int i = 0; i < 32; i++)
+                atomicAdd(&red[(size_t)(64 * pq + 32 + i) * kRowsCoef + lane], v1[i] << (8 * qd));
+            __threadfence_block();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(red_full);
+            if (!__all_sync(0xffffffffu, mbar_wait(red_full, (uint32_t)it & 1))) {
+                ok = false;
+                break;
+            }
+            int t, k0, nk;
+            unit_of(it, s_geo, t, k0, nk);
+            const int group = t / (kN / kRowsCoef);
+            const int n0 = (t % (kN / kRowsCoef)) * kRowsCoef;
+            constexpr int kW = kGroup / kDrainWarps;
+            if (KB) {
+                const int key = s_geo[4] >> 1;
+                const uint32_t n = (uint32_t)(n0 + lane);
+#pragma unroll 1
+                for (int i = 0; i < kW; i++) {
+                    const int gl = d + kDrainWarps * i, l = group * kGroup + gl;
+                    const uint32_t v = red[(size_t)gl * kRowsCoef + lane];
+                    red[(size_t)gl * kRowsCoef + lane] = 0u;
+                    if (l < lanes) {
+                        const uint32_t a01 = *reinterpret_cast<const uint32_t*>(
+                            abar + (size_t)l * 640 + 2 * pair);
+                        const uint32_t a0 = a01 & 0xFFFFu, a1 = a01 >> 16;
+                        const uint32_t e = key == 0 ? (a0 + a1) & (2 * kN - 1) : key == 1 ? a0 : a1;
+                        const uint32_t pos = (n + e) & (2 * kN - 1);
+                        uint32_t* out = acc + (size_t)l * kTrlwe + j_out * kN;
+                        atomicAdd(&out[pos & (kN - 1)], pos < (uint32_t)kN ? v : 0u - v);
+                        atomicAdd(&out[n], 0u - v);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < kW; i++) {
+                    const int gl = d + kDrainWarps * i, l = group * kGroup + gl;
+                    const uint32_t v = red[(size_t)gl * kRowsCoef + lane];
+                    red[(size_t)gl * kRowsCoef + lane] = 0u;
+                    if (l < lanes) atomicAdd(&acc[(size_t)l * kTrlwe + j_out * kN + n0 + lane], v);
+                }
+            }
+            __threadfence_block();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(red_clear);
+            if (!__all_sync(0xffffffffu, mbar_wait(red_clear, (uint32_t)it & 1))) {
+                ok = false;
+                break;
+            }
+        }
+        if (!ok) s_fail = 1;
+    }
+
+    __syncthreads();
+    if (s_fail && tid == 0) {
+        atomicOr(err, 1);
+        // wait (bounded) for copies and MMA batches that may be in flight (the
+        // chunk barriers, which count both CTAs' copies, live in the even CTA)
+        if (rank == 0)
+            for (int s = 0; s < kPStages; s++) mbar_wait(&full[s], 0), mbar_wait(&full[s], 1);
+        mbar_wait(acc_full, 0), mbar_wait(acc_full, 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();  // the pair's MMAs and copies are done with both CTAs' TMEM and smem
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols));
+}
+
 // SampleExtract (index 0) and accumulator copy-out
 __global__ void k_i8_extract(const uint32_t* __restrict__ acc, int lanes,
                              uint32_t* __restrict__ acc_out, uint32_t* __restrict__ lane_out)
@@ -550,9 +862,69 @@ cudaError_t ensure_ws(Int8Workspace& w, int lanes)
 
 cudaError_t set_gemm_attr()
 {
-    static DeviceAttrFlags attr_plain, attr_kb;
-    const cudaError_t e = set_smem_attr_once(attr_plain, k_i8_gemm_p<false>, kSmemGemmP);
-    return e != cudaSuccess ? e : set_smem_attr_once(attr_kb, k_i8_gemm_p<true>, kSmemGemmP);
+    static DeviceAttrFlags attr_plain, attr_kb, attr_pair_plain, attr_pair_kb;
+    cudaError_t e = set_smem_attr_once(attr_plain, k_i8_gemm_p<false>, kSmemGemmP);
+    if (e == cudaSuccess) e = set_smem_attr_once(attr_kb, k_i8_gemm_p<true>, kSmemGemmP);
+    if (e == cudaSuccess) e = set_smem_attr_once(attr_pair_plain, k_i8_gemm_2sm<false>, kSmemGemmPair);
+    if (e == cudaSuccess) e = set_smem_attr_once(attr_pair_kb, k_i8_gemm_2sm<true>, kSmemGemmPair);
+    return e;
+}
+
+// CTA pairs of the pair GEMM that can be resident at once on this device
+// (SMs of a GPC pair up; an odd one is left out), cached per device
+int max_pairs(int dev, int sms)
+{
+    static std::atomic<int> cache[64];
+    const int c = cache[dev & 63].load();
+    if (c > 0) return c;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * (sms / 2));
+    cfg.blockDim = dim3(kGemmPThreads);
+    cfg.dynamicSmemBytes = kSmemGemmPair;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_i8_gemm_2sm<true>, &cfg) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        n = sms / 2;
+    }
+    if (n > sms / 2) n = sms / 2;
+    cache[dev & 63].store(n);
+    return n;
+}
+
+// Tensor map of a workspace's digit tiles for the odd CTA's copies: rows of
+// 128 bytes ([group][chunk][256 lanes] rows, already in the MMA's swizzled
+// order, copied as they are), boxes of 128 rows.  cuTensorMapEncodeTiled comes
+// from the driver through the runtime's entry-point query.
+cudaError_t digits_tensor_map(const Int8Workspace& w, int groups, CUtensorMap* map)
+{
+    typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                    const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                    const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static std::atomic<EncodeTiled> encode{nullptr};
+    EncodeTiled fn = encode.load();
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !f) return cudaErrorNotSupported;
+        fn = reinterpret_cast<EncodeTiled>(f);
+        encode.store(fn);
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)kChunkK, (cuuint64_t)groups * kChunks * kGroup};
+    const cuuint64_t strides[1] = {(cuuint64_t)kChunkK};
+    const cuuint32_t box[2] = {(cuuint32_t)kChunkK, 128u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, w.digits, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+bool use_pair_gemm()
+{
+    const char* e = getenv("CUFHE_I8_PAIR");
+    return !(e && e[0] == '0');
 }
 
 }  // namespace
@@ -615,9 +987,16 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int n = 1;
     // tiles per combo; the tiles of the last, partial round are split along
-    // K so that the round's units fit one per CTA (split = 1, 2, 4 or 8)
+    // K so that the round's units fit one per CTA (split = 1, 2, 4 or 8).
+    // Pair form: one unit per CTA pair (its two CTAs serve the two output
+    // polynomials of one key), so the units per combo are the pairs per key.
+    const bool pair_form = use_pair_gemm();
+    CUtensorMap tmap;
+    if (pair_form && (e = digits_tensor_map(w, groups, &tmap)) != cudaSuccess) return e;
     const int tiles_j = groups * (kN / kRowsCoef);
-    const int ncj = sms / combos, rem = tiles_j % ncj;
+    const int keys = k.kb ? 3 : 1;
+    const int ncj = pair_form ? max_pairs(dev, sms) / keys : sms / combos;
+    const int rem = tiles_j % ncj;
     int split = 1;
     while (rem && split < 8 && rem * split * 2 <= ncj) split *= 2;
     const int units = tiles_j < ncj ? tiles_j * split : ncj;
@@ -643,18 +1022,25 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
         const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * key_step;
         {
             cudaLaunchConfig_t cfg = {};
+            // both forms: combos x units CTAs (pair form: keys x units pairs)
             cfg.gridDim = dim3(combos * units);
             cfg.blockDim = dim3(kGemmPThreads);
-            cfg.dynamicSmemBytes = kSmemGemmP;
+            cfg.dynamicSmemBytes = pair_form ? kSmemGemmPair : kSmemGemmP;
             cfg.stream = st;
             cfg.attrs = pdl;
             cfg.numAttrs = 1;
-            e = k.kb ? cudaLaunchKernelEx(&cfg, k_i8_gemm_p<true>, vk, (const uint8_t*)w.digits,
-                                          w.acc, lanes, tiles_j, split, (const uint16_t*)w.abar, i,
-                                          err)
-                     : cudaLaunchKernelEx(&cfg, k_i8_gemm_p<false>, vk, (const uint8_t*)w.digits,
-                                          w.acc, lanes, tiles_j, split, (const uint16_t*)w.abar, i,
-                                          err);
+            const uint8_t* dg = (const uint8_t*)w.digits;
+            const uint16_t* ab = (const uint16_t*)w.abar;
+            if (pair_form)
+                e = k.kb ? cudaLaunchKernelEx(&cfg, k_i8_gemm_2sm<true>, tmap, vk, dg, w.acc, lanes,
+                                              tiles_j, split, ab, i, err)
+                         : cudaLaunchKernelEx(&cfg, k_i8_gemm_2sm<false>, tmap, vk, dg, w.acc,
+                                              lanes, tiles_j, split, ab, i, err);
+            else
+                e = k.kb ? cudaLaunchKernelEx(&cfg, k_i8_gemm_p<true>, vk, dg, w.acc, lanes,
+                                              tiles_j, split, ab, i, err)
+                         : cudaLaunchKernelEx(&cfg, k_i8_gemm_p<false>, vk, dg, w.acc, lanes,
+                                              tiles_j, split, ab, i, err);
             if (e != cudaSuccess) return e;
         }
         n += 2;

@@ -145,6 +145,73 @@ __device__ __forceinline__ void tc_mma_i8_ss(uint32_t d_tmem, uint64_t a_desc, u
         : "memory");
 }
 
+// ---- CTA pairs (cluster of two, tcgen05 cta_group::2) -----------------------
+// In a pair MMA (M = 256) each CTA holds 128 rows of A in its own TMEM (same
+// TMEM address in both), half of B's N columns in its own shared memory (same
+// shared-memory address in both) and its 128 rows of D in its own TMEM; one
+// thread of the even CTA issues the MMA for both.
+
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// every thread of both CTAs; orders barrier initialisation and TMEM use
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;"
+                 ::: "memory");
+}
+
+// arrive on the mbarrier at the same shared-memory offset in CTA `rank` of the cluster
+__device__ __forceinline__ void mbar_arrive_cluster(uint64_t* bar, uint32_t rank)
+{
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(bar)), "r"(rank));
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(remote) : "memory");
+}
+
+// 2-D tensor copy global -> this CTA's shared memory whose transaction bytes
+// complete on the mbarrier at the same offset in the pair's even CTA (the
+// tensor map is a __grid_constant__ kernel parameter; x must be a multiple of
+// 16 bytes, here always 0)
+__device__ __forceinline__ void tma2d_g2s_to_even(void* dst, const void* tmap, int x, int y,
+                                                  uint64_t* bar)
+{
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, 0;" : "=r"(remote) : "r"(smem_u32(bar)));
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)), "l"(tmap), "r"(remote), "r"(x), "r"(y)
+        : "memory");
+}
+
+// pair MMA: D (+)= A[tmem, 128 rows per CTA] * B[smem desc, N/2 columns per CTA]^T
+__device__ __forceinline__ void tc_mma_i8_pair(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc,
+                                               uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], [%1], %2, %3, {%5, %6, %7, %8, %9, %10, %11, "
+        "%12}, p;\n\t}"
+        ::"r"(d_tmem), "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u),
+          "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+// completion of the pair's earlier MMAs arrives on the mbarrier at this
+// offset in both CTAs of the pair
+__device__ __forceinline__ void tc_commit_pair(uint64_t* bar)
+{
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 "
+        "[%0], %1;" ::"r"(smem_u32(bar)), "h"((uint16_t)3)
+        : "memory");
+}
+
 // balanced signed byte limb c of a Torus32 word: v = sum_c s_c 2^(8c) mod 2^32
 __host__ __device__ __forceinline__ int8_t limb(uint32_t v, int c)
 {
