@@ -474,15 +474,22 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
                 // e = a0 + a1, a0, a1 for bk0, bk1, bk2
                 const int key = s_geo[4] >> 1;
                 const uint32_t n = (uint32_t)(n0 + lane);
+                // the kW gate lanes' rotation pairs (a0, a1 in one 32-bit word),
+                // loaded together and then broadcast, not one dependent load
+                // per iteration
+                uint32_t my_a01 = 0;
+                {
+                    const int l = group * kGroup + d + kDrainWarps * lane;
+                    if (lane < kW && l < lanes)
+                        my_a01 = *reinterpret_cast<const uint32_t*>(abar + (size_t)l * 640 + 2 * pair);
+                }
 #pragma unroll 1
                 for (int i = 0; i < kW; i++) {
                     const int gl = d + kDrainWarps * i, l = group * kGroup + gl;
                     const uint32_t v = red[(size_t)gl * kRowsCoef + lane];
                     red[(size_t)gl * kRowsCoef + lane] = 0u;
+                    const uint32_t a01 = __shfl_sync(0xffffffffu, my_a01, i);
                     if (l < lanes) {
-                        // both rotation amounts of the pair in one 32-bit load
-                        const uint32_t a01 = *reinterpret_cast<const uint32_t*>(
-                            abar + (size_t)l * 640 + 2 * pair);
                         const uint32_t a0 = a01 & 0xFFFFu, a1 = a01 >> 16;
                         const uint32_t e = key == 0 ? (a0 + a1) & (2 * kN - 1) : key == 1 ? a0 : a1;
                         const uint32_t pos = (n + e) & (2 * kN - 1);
@@ -778,14 +785,22 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmPThreads, 1)
             if (KB) {
                 const int key = s_geo[4] >> 1;
                 const uint32_t n = (uint32_t)(n0 + lane);
+                // the kW gate lanes' rotation pairs (a0, a1 in one 32-bit word),
+                // loaded together and then broadcast, not one dependent load
+                // per iteration
+                uint32_t my_a01 = 0;
+                {
+                    const int l = group * kGroup + d + kDrainWarps * lane;
+                    if (lane < kW && l < lanes)
+                        my_a01 = *reinterpret_cast<const uint32_t*>(abar + (size_t)l * 640 + 2 * pair);
+                }
 #pragma unroll 1
                 for (int i = 0; i < kW; i++) {
                     const int gl = d + kDrainWarps * i, l = group * kGroup + gl;
                     const uint32_t v = red[(size_t)gl * kRowsCoef + lane];
                     red[(size_t)gl * kRowsCoef + lane] = 0u;
+                    const uint32_t a01 = __shfl_sync(0xffffffffu, my_a01, i);
                     if (l < lanes) {
-                        const uint32_t a01 = *reinterpret_cast<const uint32_t*>(
-                            abar + (size_t)l * 640 + 2 * pair);
                         const uint32_t a0 = a01 & 0xFFFFu, a1 = a01 >> 16;
                         const uint32_t e = key == 0 ? (a0 + a1) & (2 * kN - 1) : key == 1 ? a0 : a1;
                         const uint32_t pos = (n + e) & (2 * kN - 1);
