@@ -54,6 +54,22 @@ __device__ __forceinline__ double2 mul_si(double2 a)
     return S > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
 }
 
+// Radix-2 butterfly across lanes l and l ^ 16 (h = l >> 4): lanes h = 0 hold
+// E0, lanes h = 1 hold E1; afterwards h = 0 holds E0 + w E1 and h = 1 holds
+// E0 - w E1.  Lanes h = 1 multiply by w, and every lane finishes with
+// o + sg * t as one FMA per component (sg = +-1) instead of computing both
+// the sum and the difference and selecting one; an FMA by +-1 rounds like
+// the add or subtract it replaces, so the results are the same bit for bit.
+__device__ __forceinline__ double2 radix2_xlane(double2 v, double2 w, int h)
+{
+    const double sg = h ? -1.0 : 1.0;
+    const double2 t = h ? cmul(v, w) : v;
+    double2 o;
+    o.x = __shfl_xor_sync(0xffffffffu, t.x, 16);
+    o.y = __shfl_xor_sync(0xffffffffu, t.y, 16);
+    return make_double2(fma(sg, t.x, o.x), fma(sg, t.y, o.y));
+}
+
 // In-place 4-point DFT with root S*i.
 template <int S>
 __device__ __forceinline__ void dft4(double2& u0, double2& u1, double2& u2, double2& u3)
@@ -144,11 +160,7 @@ __device__ __forceinline__ void fft512_warp(double2 (&v)[16], double2* tile,
     for (int m = 0; m < 16; m++) {
         double2 w = c_w32[m];
         if (S < 0) w.y = -w.y;
-        double2 t = h ? cmul(v[m], w) : v[m];
-        double2 o;
-        o.x = __shfl_xor_sync(0xffffffffu, t.x, 16);
-        o.y = __shfl_xor_sync(0xffffffffu, t.y, 16);
-        v[m] = h ? csub(o, t) : cadd(t, o);
+        v[m] = radix2_xlane(v[m], w, h);
     }
 }
 
@@ -204,11 +216,7 @@ __device__ __forceinline__ void ffnt_forward_warp(double2 (&v)[16], double2* til
 #pragma unroll
     for (int m = 0; m < 16; m++) {
         const double2 w = c_w32[m];
-        double2 tt = h ? cmul(v[m], w) : v[m];
-        double2 o;
-        o.x = __shfl_xor_sync(0xffffffffu, tt.x, 16);
-        o.y = __shfl_xor_sync(0xffffffffu, tt.y, 16);
-        v[m] = h ? csub(o, tt) : cadd(tt, o);
+        v[m] = radix2_xlane(v[m], w, h);
     }
 }
 
@@ -240,11 +248,7 @@ __device__ __forceinline__ void ffnt_inverse_warp(double2 (&v)[16], double2* til
     for (int m = 0; m < 16; m++) {
         double2 w = c_w32[m];
         w.y = -w.y;
-        double2 tt = h ? cmul(v[m], w) : v[m];
-        double2 o;
-        o.x = __shfl_xor_sync(0xffffffffu, tt.x, 16);
-        o.y = __shfl_xor_sync(0xffffffffu, tt.y, 16);
-        v[m] = h ? csub(o, tt) : cadd(tt, o);
+        v[m] = radix2_xlane(v[m], w, h);
     }
     // untwist conj(psi^{k2 + 256 h}) conj(psi^{16 m})
     const double2 u = psi_s[psi_pos((uint32_t)(k2 + 256 * h))];
@@ -281,11 +285,7 @@ __device__ __forceinline__ void dft512_fwd_post(double2 (&v)[16], double2* tile,
 #pragma unroll
     for (int m = 0; m < 16; m++) {
         const double2 w = c_w32[m];
-        double2 tt = h ? cmul(v[m], w) : v[m];
-        double2 o;
-        o.x = __shfl_xor_sync(0xffffffffu, tt.x, 16);
-        o.y = __shfl_xor_sync(0xffffffffu, tt.y, 16);
-        v[m] = h ? csub(o, tt) : cadd(tt, o);
+        v[m] = radix2_xlane(v[m], w, h);
     }
 }
 
@@ -314,11 +314,7 @@ __device__ __forceinline__ void dft512_inv_raw(double2 (&v)[16], double2* tile, 
     for (int m = 0; m < 16; m++) {
         double2 w = c_w32[m];
         w.y = -w.y;
-        double2 tt = h ? cmul(v[m], w) : v[m];
-        double2 o;
-        o.x = __shfl_xor_sync(0xffffffffu, tt.x, 16);
-        o.y = __shfl_xor_sync(0xffffffffu, tt.y, 16);
-        v[m] = h ? csub(o, tt) : cadd(tt, o);
+        v[m] = radix2_xlane(v[m], w, h);
     }
 }
 
