@@ -225,10 +225,10 @@ __global__ void __launch_bounds__(G * 128, G == 1 ? 3 : (G == 2 ? 2 : 1)) k_br_f
 #pragma unroll
             for (int m = 0; m < 16; m++) {
                 const int n = (lane & 15) + 16 * m + 256 * (lane >> 4);
-                // untwisted value / 512, then x 2^32  =>  x 2^23
+                // already untwisted and scaled to Torus32 units (x 2^23)
                 const double2 u = v[m];
-                const uint32_t lo = (uint32_t)__double2ll_rn(u.x * 0x1p23);
-                const uint32_t hi = (uint32_t)__double2ll_rn(u.y * 0x1p23);
+                const uint32_t lo = (uint32_t)__double2ll_rn(u.x);
+                const uint32_t hi = (uint32_t)__double2ll_rn(u.y);
                 if (KB) {
                     a[n] = lo;
                     a[n + kHalfN] = hi;
@@ -462,9 +462,9 @@ __global__ void __cluster_dims__(kCluRanks, 1, 1) __launch_bounds__(128, 1)
 #pragma unroll
             for (int m = 0; m < 16; m++) {
                 const int n = (lane & 15) + 16 * m + 256 * (lane >> 4);
-                const double2 u = v[m];
-                const uint32_t lo = (uint32_t)__double2ll_rn(u.x * 0x1p23);
-                const uint32_t hi = (uint32_t)__double2ll_rn(u.y * 0x1p23);
+                const double2 u = v[m];  // untwisted, in Torus32 units
+                const uint32_t lo = (uint32_t)__double2ll_rn(u.x);
+                const uint32_t hi = (uint32_t)__double2ll_rn(u.y);
                 if (KB) {
                     a[n] = lo;
                     a[n + kHalfN] = hi;
@@ -610,7 +610,7 @@ cudaError_t launch_bk_to_fft(const uint32_t* bk, int npolys, const Fp64Tables& t
 
 cudaError_t upload_fft_constants(void)
 {
-    double2 w[16], t32[16], u16[16];
+    double2 w[16], t32[16], u16[16], u23[16];
     const long double pi = 3.141592653589793238462643383279502884L;
     for (int k = 0; k < 16; k++) {
         const long double a = 2 * pi * k / 32;
@@ -619,10 +619,12 @@ cudaError_t upload_fft_constants(void)
         t32[k] = make_double2((double)cosl(b), (double)sinl(b));
         const long double c = -pi * k / 64;  // conj(psi^{16 k})
         u16[k] = make_double2((double)cosl(c), (double)sinl(c));
+        u23[k] = make_double2(u16[k].x * 0x1p23, u16[k].y * 0x1p23);
     }
     cudaError_t e = cudaMemcpyToSymbol(c_w32, w, sizeof(w));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tw32, t32, sizeof(t32));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_utw16, u16, sizeof(u16));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_utw16x23, u23, sizeof(u23));
     return e;
 }
 

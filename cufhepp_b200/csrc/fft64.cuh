@@ -183,9 +183,13 @@ __device__ __forceinline__ double2 psi_at(const double2* psi_s, uint32_t t)
     return v;
 }
 
-// e^{i pi n2 / 32} (= psi^{32 n2}) and e^{-i pi m / 64} (= psi^{-16 m})
+// e^{i pi n2 / 32} (= psi^{32 n2}) and e^{-i pi m / 64} (= psi^{-16 m});
+// c_utw16x23 = 2^23 c_utw16 (N = 1024 inverse: the 1/512 normalisation and
+// the 2^32 Torus32 scale folded in; power-of-two scaling is exact, so the
+// products are those of the unscaled constant times 2^23 bit for bit)
 static __constant__ double2 c_tw32[16];
 static __constant__ double2 c_utw16[16];
+static __constant__ double2 c_utw16x23[16];
 
 // Forward FFNT of one folded polynomial: in v[n2] = d[n] + i d[n + 512] for
 // n = lane + 32 n2; out as fft512_warp.  The twist psi^n = psi^lane psi^{32 n2}
@@ -221,8 +225,8 @@ __device__ __forceinline__ void ffnt_forward_warp(double2 (&v)[16], double2* til
 }
 
 // Inverse FFNT: in v[n2] = Z[lane + 32 n2] (natural bins); out v[m] holds
-// z'[n] * conj(psi^n) (untwisted, without the 1/512 scale) for
-// n = (lane & 15) + 16 m + 256 (lane >> 4).
+// z'[n] * conj(psi^n) * 2^23 (untwisted; 2^23 = 2^32 / 512: the value in
+// Torus32 units before rounding) for n = (lane & 15) + 16 m + 256 (lane >> 4).
 __device__ __forceinline__ void ffnt_inverse_warp(double2 (&v)[16], double2* tile,
                                                   const double2* psi_s, int lane)
 {
@@ -253,7 +257,7 @@ __device__ __forceinline__ void ffnt_inverse_warp(double2 (&v)[16], double2* til
     // untwist conj(psi^{k2 + 256 h}) conj(psi^{16 m})
     const double2 u = psi_s[psi_pos((uint32_t)(k2 + 256 * h))];
 #pragma unroll
-    for (int m = 0; m < 16; m++) v[m] = cmul(cmulc(v[m], u), c_utw16[m]);
+    for (int m = 0; m < 16; m++) v[m] = cmul(cmulc(v[m], u), c_utw16x23[m]);
 }
 
 // ---------------------------------------------------------------------------
