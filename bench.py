@@ -65,6 +65,7 @@ LVL02_BATCHES = (512, 2048, 8192)
 # exact INT8 form at lvl02: K = 8 digit rows x 2048, M = 2 polys x 2048
 # coefficients x 8 key limbs, 2 digit limbs, 636 steps (a MAC is 2 ops)
 OPS_INT8_LVL2 = 2 * 636 * (8 * 2048) * (2 * 2048 * 8) * 2
+OPS_INT8_LVL2_KB = 2 * 318 * 3 * (8 * 2048) * (2 * 2048 * 8) * 2  # KeyBundle: 3 keys per pair
 LVL02_INT8_BATCH = 2048
 WORKLOAD = ("lvl1 mixed-gate batch: 4096 independent gates uniform over "
             "NAND/AND/OR/XOR/XNOR/MUX, Ctxt<lvl1> I/O (IKS->BR->SampleExtract), "
@@ -709,12 +710,13 @@ def run_lvl02(args, torch, engine, client, P, sk, rank, ws, flush):
 
 
 def run_lvl02_int8(args, torch, engine, client, P, sk, rank, ws, flush):
-    """The exact INT8 form of the lvl02 gates (plain lvl02 key, eight key limbs
-    x two digit limbs, INT32 accumulation): NAND batch of LVL02_INT8_BATCH
-    gates timed like the FP64 form (3 warm-up, events, L2 flush, bounded to
-    a few steps: a batch takes about a second), and the FP64 form's phase
-    error against it after full rotations of the same 64 inputs."""
-    ek = client.EvalKey02.generate(sk, keybundle=False)
+    """The exact INT8 form of the lvl02 gates with the KeyBundle key, as the
+    FP64 leg (eight key limbs x two digit limbs, INT32 accumulation; three key
+    GEMMs per pair): NAND batch of LVL02_INT8_BATCH gates timed like the FP64
+    form (3 warm-up, events, L2 flush, bounded to a few steps: a batch takes
+    about a second), and the FP64 form's phase error against it after full
+    rotations of the same 64 inputs."""
+    ek = client.EvalKey02.generate(sk, keybundle=True)
     engine.initialize_lvl02(ek)
     engine.set_precision(P.INT8_EXACT)
     rng = np.random.default_rng(args.seed + 17 + rank)
@@ -764,7 +766,7 @@ def run_lvl02_int8(args, torch, engine, client, P, sk, rank, ws, flush):
     finally:
         engine.set_precision(P.FP64_FFNT)
         engine.cleanup_lvl02()
-    work = OPS_INT8_LVL2 * B
+    work = OPS_INT8_LVL2_KB * B
     peak = engine_peak_int8(engine)
     ach = work / (br_ms / steps * 1e-3) / 1e12 if br_ms else None
     return {"batch": B, "value": whole_job_rate(B, ws, steps, total), "steps": steps,
@@ -774,7 +776,8 @@ def run_lvl02_int8(args, torch, engine, client, P, sk, rank, ws, flush):
             "roofline": {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TOP/s",
                          "frac": ach / peak if ach else None,
                          "kernel": "INT8 blind rotation to lvl2 (decompose + tcgen05 Toeplitz "
-                                   "GEMM per step)",
+                                   "GEMMs per KeyBundle pair)",
+                         "keybundle": True,
                          "work_per_launch": work,
                          "peak_source": "measured tcgen05.mma.kind::i8 probe on this GPU"},
             "dtype": "int8 products, int32 accumulation, Torus64 recombination"}

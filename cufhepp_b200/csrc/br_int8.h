@@ -47,8 +47,9 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
                            uint32_t mu, int steps, uint32_t* acc_out, uint32_t* lane_out,
                            int* err, cudaStream_t st, int* launches);
 
-// bk2_dev: plain (non-KeyBundle) BootstrappingKey<lvl02>, TRGSW<lvl2>[636]
-cudaError_t int8_key2_build(Int8Key& k, const uint64_t* bk2_dev, cudaStream_t st);
+// bk2_dev: BootstrappingKey<lvl02>, plain TRGSW<lvl2>[636] or (kb) KeyBundle
+// TRGSW<lvl2>[318][3]; launch_br2_int8's `steps` counts CMUX steps or pairs
+cudaError_t int8_key2_build(Int8Key& k, const uint64_t* bk2_dev, bool kb, cudaStream_t st);
 void int8_workspace2_free(Int8Workspace2& w);
 cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t* lane_in, int lanes,
                             uint64_t mu, int steps, uint64_t* acc_out, uint64_t* lane_out,

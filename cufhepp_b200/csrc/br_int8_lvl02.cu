@@ -1,5 +1,7 @@
 // Exact INT8 tensor-core blind rotation lvl0 -> lvl2 (tcgen05, sm_100a),
-// plain CMUX form: the lvl02param instantiation of __BlindRotate__
+// plain CMUX form and KeyBundle form (one step per pair, three key GEMMs whose
+// products enter as (X^e - 1) P, plus the gadget recomposition of the digits,
+// as at lvl1 in br_int8.cu): the lvl02param instantiation of __BlindRotate__
 // (include/gatebootstrapping_gpu.cuh:801-884) that the *_lvl02 gates run
 // (src/cufhe_gates_gpu.cu:826-979), with N = 2048, l = 4, Bgbit = 10,
 // Torus64.
@@ -93,11 +95,12 @@ __device__ __forceinline__ int8_t limb64(uint64_t v, int c)
     return s;
 }
 
-// key table: out[i][j][r][c][t], t < 2N (4 bytes per thread)
-__global__ void k_i82_key(const uint64_t* __restrict__ bk, int8_t* __restrict__ out)
+// key table: out[i][j][r][c][t], t < 2N (4 bytes per thread), i over the
+// key's ntrgsw TRGSWs (636 plain, 318 x 3 KeyBundle)
+__global__ void k_i82_key(const uint64_t* __restrict__ bk, int ntrgsw, int8_t* __restrict__ out)
 {
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // 4-byte unit
-    const size_t total = (size_t)kN0 * kVStep / 4;
+    const size_t total = (size_t)ntrgsw * kVStep / 4;
     if (q >= total) return;
     const size_t byte = q * 4;
     const int t0 = (int)(byte % kVRow);
@@ -138,10 +141,16 @@ __global__ void k_i82_init(const uint32_t* __restrict__ lane_in, int lanes, uint
     }
 }
 
-// digit limbs of X^abar acc - acc for step `step`, written as swizzled tiles
-// tiles[group][chunk][32 KB]; one CTA (256 threads) per lane, 4 coefficients
-// per thread and pass
-__global__ void __launch_bounds__(256) k_i82_decompose(const uint64_t* __restrict__ acc,
+// Digit limbs of the step's external-product input, written as swizzled
+// tiles tiles[group][chunk][32 KB]; one CTA (256 threads) per lane, 4
+// coefficients per thread and pass.
+//  * plain CMUX step `step`: digits of X^abar acc - acc (acc is only read);
+//  * KeyBundle pair (KB): digits of acc itself, and acc is overwritten in
+//    place with their gadget recomposition sum_d dec_d 2^(64 - 10 (d + 1)) =
+//    (acc + 2^23) & ~(2^24 - 1), the H term to which the pair's GEMM adds the
+//    rotated products.  Each thread reads and rewrites only its own words.
+template <bool KB>
+__global__ void __launch_bounds__(256) k_i82_decompose(uint64_t* __restrict__ acc,
                                                        const uint16_t* __restrict__ abar,
                                                        int lanes, int step,
                                                        uint8_t* __restrict__ tiles)
@@ -151,13 +160,13 @@ __global__ void __launch_bounds__(256) k_i82_decompose(const uint64_t* __restric
     asm volatile("griddepcontrol.wait;" ::: "memory");
     const int l = blockIdx.x;
     if (l >= lanes) return;
-    const uint32_t ab = abar[(size_t)l * kAbarStride + step];
+    const uint32_t ab = KB ? 0u : abar[(size_t)l * kAbarStride + step];
     const uint32_t abm = ab & (kN2 - 1), abn = ab >> 11;
     const uint32_t row = (uint32_t)(l % kGroup2);
     uint8_t* gtile = tiles + (size_t)(l / kGroup2) * kChunks2 * kTileBytes;
 #pragma unroll 1
     for (int j = 0; j < 2; j++) {
-        const uint64_t* a = acc + (size_t)l * kTrlwe2 + j * kN2;
+        uint64_t* a = acc + (size_t)l * kTrlwe2 + j * kN2;
 #pragma unroll 1
         for (int pass = 0; pass < 2; pass++) {
             const int m = (threadIdx.x + 256 * pass) * 4;
@@ -165,9 +174,16 @@ __global__ void __launch_bounds__(256) k_i82_decompose(const uint64_t* __restric
 #pragma unroll
             for (int e4 = 0; e4 < 4; e4++) {
                 const uint32_t n = (uint32_t)(m + e4);
-                uint64_t rv = a[(n - ab) & (kN2 - 1)];
-                rv = ((n < abm) ^ abn) ? 0ull - rv : rv;
-                const uint64_t t = rv - a[n] + kDecOffset2;
+                uint64_t t;
+                if (KB) {
+                    const uint64_t x = a[n];
+                    a[n] = (x + (1ull << 23)) & ~((1ull << 24) - 1);
+                    t = x + kDecOffset2;
+                } else {
+                    uint64_t rv = a[(n - ab) & (kN2 - 1)];
+                    rv = ((n < abm) ^ abn) ? 0ull - rv : rv;
+                    t = rv - a[n] + kDecOffset2;
+                }
 #pragma unroll
                 for (int d = 0; d < 4; d++) {
                     const int dig = (int)((t >> (54 - 10 * d)) & 1023u) - 512;
@@ -214,12 +230,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16])
 
 // Roles: warps 0-7 generators (warpgroup wg writes the chunks of parity wg),
 // warp 8 MMA issue, warp 9 digit-chunk producer, warps 10-25 drainers, warp 26
-// key-window producer.
+// key-window producer.  KeyBundle form (KB): CTA b serves combo b mod 6 =
+// key * 2 + output polynomial of the pair's three keys, and the drain adds
+// each product word P[n] at n + e (negacyclic) and subtracts it at n
+// (e = a0 + a1, a0, a1 for bk0, bk1, bk2) with 64-bit atomic adds, since
+// three keys add into every accumulator word.
+template <bool KB>
 __global__ void __launch_bounds__(kGemmThreads, 1) k_i82_gemm(const int8_t* __restrict__ vkey,
                                                               const uint8_t* __restrict__ tiles,
                                                               uint64_t* __restrict__ acc,
                                                               int lanes, int blocks_j,
-                                                              int* __restrict__ err)
+                                                              const uint16_t* __restrict__ abar,
+                                                              int pair, int* __restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t raw_addr = smem_u32(smem_raw);
@@ -240,7 +262,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_i82_gemm(const int8_t* __re
     __shared__ volatile int s_fail;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int j_out = blockIdx.x & 1, cb = blockIdx.x >> 1, ncj = gridDim.x >> 1;
+    constexpr int kCombos = KB ? 6 : 2;
+    const int combo = (int)(blockIdx.x % kCombos), j_out = combo & 1;
+    const int cb = (int)(blockIdx.x / kCombos), ncj = (int)(gridDim.x / kCombos);
     // blocks = (group, coefficient block) pairs of this output poly; each is
     // two tiles (limb groups 0 and 1) in a row
     const int nblk = cb < blocks_j ? (blocks_j - 1 - cb) / ncj + 1 : 0;
@@ -313,7 +337,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_i82_gemm(const int8_t* __re
 #pragma unroll 1
                     for (int q = 0; q < 4; q++) {
                         const int c = 4 * lg + q;
-                        const int8_t* src = vkey + ((size_t)(j_out * 8 + r) * 8 + c) * kVRow +
+                        const int8_t* src = vkey + ((size_t)(combo * 8 + r) * 8 + c) * kVRow +
                                             (2016 - n0);
                         bulk_g2s(vbuf + vs * kVStage + q * kVWin, src, (uint32_t)kVWin, &vfull[vs]);
                     }
@@ -446,20 +470,50 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_i82_gemm(const int8_t* __re
                 ok = false;
                 break;
             }
-            // 8 lanes per warp, all loads in flight before the stores
-            constexpr int kW = kGroup2 / kDrainWarps;
-            uint64_t old[kW];
+            constexpr int kW = kGroup2 / kDrainWarps;  // 8 lanes per warp
+            if (KB) {
+                const int key = combo >> 1;
+                const uint32_t n = (uint32_t)(n0 + lane);
+                // the kW gate lanes' rotation pairs, loaded together
+                uint32_t my_a01 = 0;
+                {
+                    const int l = group * kGroup2 + d + kDrainWarps * lane;
+                    if (lane < kW && l < lanes)
+                        my_a01 = *reinterpret_cast<const uint32_t*>(abar + (size_t)l * kAbarStride +
+                                                                    2 * pair);
+                }
+#pragma unroll 1
+                for (int i = 0; i < kW; i++) {
+                    const int gl = d + kDrainWarps * i, l = group * kGroup2 + gl;
+                    const uint64_t v = red[(size_t)gl * kRowsCoef + lane];
+                    red[(size_t)gl * kRowsCoef + lane] = 0ull;
+                    const uint32_t a01 = __shfl_sync(0xffffffffu, my_a01, i);
+                    if (l < lanes) {
+                        const uint32_t a0 = a01 & 0xFFFFu, a1 = a01 >> 16;
+                        const uint32_t e = key == 0 ? (a0 + a1) & (2 * kN2 - 1) : key == 1 ? a0 : a1;
+                        const uint32_t pos = (n + e) & (2 * kN2 - 1);
+                        unsigned long long* out = reinterpret_cast<unsigned long long*>(
+                            acc + ((size_t)l * 2 + j_out) * kN2);
+                        atomicAdd(&out[pos & (kN2 - 1)],
+                                  (unsigned long long)(pos < (uint32_t)kN2 ? v : 0ull - v));
+                        atomicAdd(&out[n], (unsigned long long)(0ull - v));
+                    }
+                }
+            } else {
+                // all loads in flight before the stores (one writer per word)
+                uint64_t old[kW];
 #pragma unroll
-            for (int i = 0; i < kW; i++) {
-                const int l = group * kGroup2 + d + kDrainWarps * i;
-                old[i] = l < lanes ? acc[((size_t)l * 2 + j_out) * kN2 + n0 + lane] : 0ull;
-            }
+                for (int i = 0; i < kW; i++) {
+                    const int l = group * kGroup2 + d + kDrainWarps * i;
+                    old[i] = l < lanes ? acc[((size_t)l * 2 + j_out) * kN2 + n0 + lane] : 0ull;
+                }
 #pragma unroll
-            for (int i = 0; i < kW; i++) {
-                const int gl = d + kDrainWarps * i, l = group * kGroup2 + gl;
-                const uint64_t v = red[(size_t)gl * kRowsCoef + lane];
-                red[(size_t)gl * kRowsCoef + lane] = 0ull;
-                if (l < lanes) acc[((size_t)l * 2 + j_out) * kN2 + n0 + lane] = old[i] + v;
+                for (int i = 0; i < kW; i++) {
+                    const int gl = d + kDrainWarps * i, l = group * kGroup2 + gl;
+                    const uint64_t v = red[(size_t)gl * kRowsCoef + lane];
+                    red[(size_t)gl * kRowsCoef + lane] = 0ull;
+                    if (l < lanes) acc[((size_t)l * 2 + j_out) * kN2 + n0 + lane] = old[i] + v;
+                }
             }
             __threadfence_block();  // the zeroed buffer before the next tile's adds
             __syncwarp();
@@ -521,21 +575,25 @@ cudaError_t ensure_ws2(Int8Workspace2& w, int lanes)
 cudaError_t set_gemm2_attr()
 {
     static DeviceAttrFlags attr;
-    return set_smem_attr_once(attr, k_i82_gemm, kSmemGemm);
+    static DeviceAttrFlags attr_kb;
+    const cudaError_t e = set_smem_attr_once(attr, k_i82_gemm<false>, kSmemGemm);
+    return e != cudaSuccess ? e : set_smem_attr_once(attr_kb, k_i82_gemm<true>, kSmemGemm);
 }
 
 }  // namespace
 
-cudaError_t int8_key2_build(Int8Key& k, const uint64_t* bk2_dev, cudaStream_t st)
+cudaError_t int8_key2_build(Int8Key& k, const uint64_t* bk2_dev, bool kb, cudaStream_t st)
 {
     int8_key_free(k);
-    k.bytes = (size_t)kN0 * kVStep;
+    const int ntrgsw = kb ? 3 * (kN0 / 2) : kN0;
+    k.bytes = (size_t)ntrgsw * kVStep;
     cudaError_t e = cudaMalloc(&k.limbs, k.bytes);
     if (e != cudaSuccess) return e;
     const size_t units = k.bytes / 4;
-    k_i82_key<<<(unsigned)((units + 255) / 256), 256, 0, st>>>(bk2_dev, (int8_t*)k.limbs);
+    k_i82_key<<<(unsigned)((units + 255) / 256), 256, 0, st>>>(bk2_dev, ntrgsw, (int8_t*)k.limbs);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    k.kb = kb;
     k.ready = true;
     return cudaSuccess;
 }
@@ -565,11 +623,17 @@ cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t*
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int nsteps = (steps < 0 || steps > kN0) ? kN0 : steps;
+    // plain key: one GEMM step per CMUX step (636); KeyBundle key: one per
+    // pair (318) over the pair's three keys
+    const int total = k.kb ? kN0 / 2 : kN0;
+    const int nsteps = (steps < 0 || steps > total) ? total : steps;
     const int groups = (lanes + kGroup2 - 1) / kGroup2;
-    // even grid: CTA b serves output polynomial b & 1
+    // CTA b serves combo b mod combos (plain: the output polynomial; KeyBundle:
+    // key * 2 + output polynomial)
+    const int combos = k.kb ? 6 : 2;
+    const size_t key_step = (size_t)(k.kb ? 3 : 1) * kVStep;
     const int blocks_j = groups * kNBlocks;
-    const int grid = 2 * (blocks_j < sms / 2 ? blocks_j : sms / 2);
+    const int grid = combos * (blocks_j < sms / combos ? blocks_j : sms / combos);
     k_i82_init<<<lanes, 256, 0, st>>>(lane_in, lanes, mu, w.abar, w.acc);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int n = 1;
@@ -585,15 +649,21 @@ cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t*
         cfg.stream = st;
         cfg.attrs = pdl;
         cfg.numAttrs = 1;
-        e = cudaLaunchKernelEx(&cfg, k_i82_decompose, (const uint64_t*)w.acc,
-                               (const uint16_t*)w.abar, lanes, i, (uint8_t*)w.digits);
+        const uint16_t* ab = (const uint16_t*)w.abar;
+        e = k.kb ? cudaLaunchKernelEx(&cfg, k_i82_decompose<true>, w.acc, ab, lanes, i,
+                                      (uint8_t*)w.digits)
+                 : cudaLaunchKernelEx(&cfg, k_i82_decompose<false>, w.acc, ab, lanes, i,
+                                      (uint8_t*)w.digits);
         if (e != cudaSuccess) return e;
-        const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * kVStep;
+        const int8_t* vk = (const int8_t*)k.limbs + (size_t)i * key_step;
         cfg.gridDim = dim3(grid);
         cfg.blockDim = dim3(kGemmThreads);
         cfg.dynamicSmemBytes = kSmemGemm;
-        e = cudaLaunchKernelEx(&cfg, k_i82_gemm, vk, (const uint8_t*)w.digits, w.acc, lanes,
-                               blocks_j, err);
+        const uint8_t* dg = (const uint8_t*)w.digits;
+        e = k.kb ? cudaLaunchKernelEx(&cfg, k_i82_gemm<true>, vk, dg, w.acc, lanes, blocks_j, ab,
+                                      i, err)
+                 : cudaLaunchKernelEx(&cfg, k_i82_gemm<false>, vk, dg, w.acc, lanes, blocks_j, ab,
+                                      i, err);
         if (e != cudaSuccess) return e;
         n += 2;
     }

@@ -33,7 +33,7 @@ struct DeviceState {
     double2* psi = nullptr;
     double2* tw512 = nullptr;
     Int8Key i8;              // INT8 exact-path key (plain or KeyBundle, as the FP64 one)
-    Int8Key i8_2;            // INT8 exact-path lvl02 key (non-KeyBundle only)
+    Int8Key i8_2;            // INT8 exact-path lvl02 key (plain or KeyBundle)
     uint8_t* iks_key = nullptr;  // KSK as signed byte-limb tiles (tensor-core IKS)
     int* err = nullptr;          // set by a device wait that timed out
     // lvl0 -> lvl2 path (Initialize_lvl02)
@@ -377,8 +377,9 @@ int init_device02(int d, const cufhe_keyview02* ek)
     const int npolys = (int)(ek->bk_words / CUFHE_LVL2_N);
     CK(cudaMalloc(&D.bkf2, (size_t)npolys * 1024 * sizeof(double2)));
     CKL(launch_bk2_to_fft(raw, npolys, D.psi2, D.bkf2, 0));
-    if (!ek->keybundle) {
-        cudaError_t e = int8_key2_build(D.i8_2, raw, 0);
+    {
+        // INT8 Toeplitz limb windows of either key form (KeyBundle: 954 TRGSWs)
+        cudaError_t e = int8_key2_build(D.i8_2, raw, ek->keybundle != 0, 0);
         if (e != cudaSuccess) {
             cudaFree(raw);
             cudaFree(ksk);
@@ -564,9 +565,7 @@ int run_br2(cufhe_stream_s* s, const uint32_t* lane_in, int lanes, uint64_t mu, 
 {
     DeviceState& D = g_dev[s->device];
     if (g_precision == CUFHE_INT8_EXACT) {
-        if (D.kb2 || !D.i8_2.ready)
-            return fail(CUFHE_ERR_STATE,
-                        "INT8_EXACT at lvl02 needs a lvl02 bootstrapping key without KeyBundle");
+        if (!D.i8_2.ready) return fail(CUFHE_ERR_STATE, "INT8_EXACT: no lvl02 INT8 key on this device");
         int launches = 0;
         ProfRec pr;
         prof_begin(s->st, pr, CUFHE_K_BR_INT8_LVL02);

@@ -8,6 +8,7 @@
     python -m cufhepp_b200.kernel_driver gates LANES [REPS]     # full mixed-gate batch (lvl1)
     python -m cufhepp_b200.kernel_driver br2_fp64 LANES [REPS] [STEPS]  # lvl0 -> lvl2 rotation
     python -m cufhepp_b200.kernel_driver br2_int8 LANES [REPS] [STEPS]  # the same, INT8 exact
+    python -m cufhepp_b200.kernel_driver br2_int8_kb LANES [REPS] [STEPS]  # INT8, KeyBundle key
     python -m cufhepp_b200.kernel_driver gates02 LANES [REPS]   # mixed *_lvl02 gate batch
     python -m cufhepp_b200.kernel_driver cb BITS [REPS]   # circuit bootstrapping + BITS/8 lookup tables
 
@@ -30,7 +31,7 @@ def main(argv: list[str]) -> None:
     lanes = int(argv[1])
     reps = int(argv[2]) if len(argv) > 2 else 2
     sk = client.SecretKey.generate(5)
-    lvl02 = stage in ("br2_fp64", "br2_int8", "gates02", "cb")
+    lvl02 = stage in ("br2_fp64", "br2_int8", "br2_int8_kb", "gates02", "cb")
     if stage == "cb":
         cbk = client.CBKey.generate(sk)
         engine.initialize_lvl02(cbk.ek02)
@@ -63,7 +64,7 @@ def main(argv: list[str]) -> None:
             engine.trgsw_to_fft(engine.GADGET_CB, d_t, 8 * q, d_f)
             engine.lut_eval(luts, d_f, P.MU32, d_o)
             tick(i)
-    elif stage in ("br2_fp64", "br2_int8"):
+    elif stage in ("br2_fp64", "br2_int8", "br2_int8_kb"):
         engine.set_precision(P.FP64_FFNT if stage == "br2_fp64" else P.INT8_EXACT)
         steps = int(argv[3]) if len(argv) > 3 else -1
         d_in = engine.to_device(client.encrypt_bits(sk, bits, 0, seed=3))

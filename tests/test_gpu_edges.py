@@ -80,7 +80,7 @@ def test_lvl02_prefix_batches_reproduce_the_full_batch():
     as a 400-gate batch, and the full batch decrypts to its truth table."""
     sk = client.SecretKey.generate(0xED6E)
     prev = engine.get_precision()
-    engine.set_precision(P.FP64_FFNT)  # the KeyBundle key needs the FP64 form
+    engine.set_precision(P.FP64_FFNT)  # the cluster form's limits are those of the FP64 form
     engine.initialize_lvl02(client.EvalKey02.generate(sk, keybundle=True))
     try:
         rng = np.random.default_rng(7)

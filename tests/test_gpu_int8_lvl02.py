@@ -12,8 +12,12 @@ limbs), through the C-ABI.
   key switch is the integer one of the FP64 form);
 * the FP64 form's rounding error against the exact form is measured on the
   same inputs after a full rotation (the report of configs' lvl02 case) and
-  stays within the FP64 path's phase tolerance;
-* the INT8 form refuses a KeyBundle lvl02 key.
+  stays within the FP64 path's phase tolerance.
+
+Every case runs with the plain key (one GEMM per CMUX step) and with the
+KeyBundle key (one step per pair: three key GEMMs whose products enter as
+(X^e - 1) P, plus the gadget recomposition of the digits; `steps` counts
+pairs), against the oracle's Torus64 CMUX and KeyBundle steps.
 """
 import numpy as np
 import pytest
@@ -31,10 +35,10 @@ def signed64(x):
     return np.asarray(x, np.uint64).view(np.int64).astype(np.float64)
 
 
-@pytest.fixture(scope="module")
-def ctx():
+@pytest.fixture(scope="module", params=[False, True], ids=["plain", "kb"])
+def ctx(request):
     sk = client.SecretKey.generate(0x1802)
-    ek = client.EvalKey02.generate(sk, keybundle=False)
+    ek = client.EvalKey02.generate(sk, keybundle=request.param)
     engine.initialize_lvl02(ek)
     engine.set_precision(P.INT8_EXACT)
     yield sk, ek
@@ -63,7 +67,7 @@ def test_int8_lvl02_steps_bit_exact(ctx, steps):
     sk, ek = ctx
     _, x = lvl0(sk, 6, 200 + steps)
     acc, t2 = rotate(x, 6, steps)
-    ref = O.blind_rotate2(x, MU2, ek.bk, False, O.EXACT, steps=steps)
+    ref = O.blind_rotate2(x, MU2, ek.bk, ek.keybundle, O.EXACT, steps=steps)
     assert np.array_equal(acc, ref)
     for i in range(6):
         assert np.array_equal(t2[i], O.sample_extract2(ref[i]))
@@ -78,7 +82,7 @@ def test_int8_lvl02_many_tiles_per_cta_bit_exact(ctx):
     _, x = lvl0(sk, count, 77)
     acc, _ = rotate(x, count, 2)
     pick = np.array([0, 1, 63, 127, 128, 200, 255, 256, 280, 299])
-    ref = O.blind_rotate2(x[pick], MU2, ek.bk, False, O.EXACT, steps=2)
+    ref = O.blind_rotate2(x[pick], MU2, ek.bk, ek.keybundle, O.EXACT, steps=2)
     assert np.array_equal(acc[pick], ref)
 
 
@@ -144,16 +148,3 @@ def test_int8_lvl02_circuit_graph_matches_direct(ctx):
     plain = CI.evaluate(net, bits)
     got = client.decrypt_bits(sk, direct[net.out], 0)
     assert int(np.count_nonzero(got != plain[net.out])) == 0
-
-
-def test_int8_lvl02_refuses_keybundle_key():
-    sk = client.SecretKey.generate(0x1803)
-    engine.initialize_lvl02(client.EvalKey02.generate(sk, keybundle=True))
-    engine.set_precision(P.INT8_EXACT)
-    try:
-        _, x = lvl0(sk, 2, 3)
-        with pytest.raises(engine.CufheError):
-            rotate(x, 2, 1)
-    finally:
-        engine.set_precision(P.FP64_FFNT)
-        engine.cleanup_lvl02()
