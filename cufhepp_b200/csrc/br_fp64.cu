@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(G * 128, G == 1 ? 3 : (G == 2 ? 2 : 1)) k_br_f
             double2* slot = spec + (g * 4 + r) * kSlotStride;
             ffnt_forward_warp(v, slot, psi_s, lane);
 #pragma unroll
-            for (int m = 0; m < 16; m++) slot[(lane & 15) + 16 * m + 256 * (lane >> 4)] = v[m];
+            for (int q = 0; q < 16; q++) slot[ffnt_pos(lane, q)] = v[q];
         }
         __syncthreads();
 
@@ -223,10 +223,10 @@ __global__ void __launch_bounds__(G * 128, G == 1 ? 3 : (G == 2 ? 2 : 1)) k_br_f
             ffnt_inverse_warp(v, slot, psi_s, lane);
             uint32_t* a = acc + g * kTrlwe + j * kN;
 #pragma unroll
-            for (int m = 0; m < 16; m++) {
-                const int n = (lane & 15) + 16 * m + 256 * (lane >> 4);
+            for (int q = 0; q < 16; q++) {
+                const int n = ffnt_pos(lane, q);
                 // already untwisted and scaled to Torus32 units (x 2^23)
-                const double2 u = v[m];
+                const double2 u = v[q];
                 const uint32_t lo = (uint32_t)__double2ll_rn(u.x);
                 const uint32_t hi = (uint32_t)__double2ll_rn(u.y);
                 if (KB) {
@@ -382,7 +382,7 @@ __global__ void __cluster_dims__(kCluRanks, 1, 1) __launch_bounds__(128, 1)
             double2* slot = spec + r * kSlotStride;
             ffnt_forward_warp(v, slot, psi_s, lane);
 #pragma unroll
-            for (int m = 0; m < 16; m++) slot[(lane & 15) + 16 * m + 256 * (lane >> 4)] = v[m];
+            for (int q = 0; q < 16; q++) slot[ffnt_pos(lane, q)] = v[q];
         }
         __syncthreads();
 
@@ -460,9 +460,9 @@ __global__ void __cluster_dims__(kCluRanks, 1, 1) __launch_bounds__(128, 1)
             ffnt_inverse_warp(v, scratch, psi_s, lane);
             uint32_t* a = acc + j * kN;
 #pragma unroll
-            for (int m = 0; m < 16; m++) {
-                const int n = (lane & 15) + 16 * m + 256 * (lane >> 4);
-                const double2 u = v[m];  // untwisted, in Torus32 units
+            for (int q = 0; q < 16; q++) {
+                const int n = ffnt_pos(lane, q);
+                const double2 u = v[q];  // untwisted, in Torus32 units
                 const uint32_t lo = (uint32_t)__double2ll_rn(u.x);
                 const uint32_t hi = (uint32_t)__double2ll_rn(u.y);
                 if (KB) {
@@ -610,21 +610,20 @@ cudaError_t launch_bk_to_fft(const uint32_t* bk, int npolys, const Fp64Tables& t
 
 cudaError_t upload_fft_constants(void)
 {
-    double2 w[16], t32[16], u16[16], u23[16];
+    double2 w[16], t32[16], uq[16];
     const long double pi = 3.141592653589793238462643383279502884L;
     for (int k = 0; k < 16; k++) {
         const long double a = 2 * pi * k / 32;
         w[k] = make_double2((double)cosl(a), (double)sinl(a));
         const long double b = pi * k / 32;  // psi^{32 k}
         t32[k] = make_double2((double)cosl(b), (double)sinl(b));
-        const long double c = -pi * k / 64;  // conj(psi^{16 k})
-        u16[k] = make_double2((double)cosl(c), (double)sinl(c));
-        u23[k] = make_double2(u16[k].x * 0x1p23, u16[k].y * 0x1p23);
+        // conj(psi^{16 (k mod 8) + 256 (k / 8)}) 2^23
+        const long double c = -pi * (16 * (k & 7) + 256 * (k >> 3)) / 1024;
+        uq[k] = make_double2((double)(cosl(c) * 0x1p23L), (double)(sinl(c) * 0x1p23L));
     }
     cudaError_t e = cudaMemcpyToSymbol(c_w32, w, sizeof(w));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tw32, t32, sizeof(t32));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_utw16, u16, sizeof(u16));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_utw16x23, u23, sizeof(u23));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_utwq, uq, sizeof(uq));
     return e;
 }
 

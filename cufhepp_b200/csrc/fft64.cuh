@@ -165,11 +165,11 @@ __device__ __forceinline__ void fft512_warp(double2 (&v)[16], double2* tile,
 }
 
 // ---------------------------------------------------------------------------
-// Table-light transforms for the blind-rotation kernel.  The root table
-// psi^t (t < N, psi = e^{i pi / N}; psi^{t+N} = -psi^t) lives in shared
-// memory in the interleaved order pos(t) = (t mod 4) * 256 + t / 4, which
-// makes the KeyBundle gathers psi^{(1+4f) a} (stride 4a across lanes)
-// bank-conflict free for odd a.
+// Transforms of the lvl1 blind-rotation kernels.  The root table psi^t
+// (t < N, psi = e^{i pi / N}; psi^{t+N} = -psi^t) lives in shared memory in
+// the interleaved order pos(t) = (t mod 4) * 256 + t / 4, which makes the
+// KeyBundle gathers psi^{(1+4f) a} (stride 4a across lanes) bank-conflict
+// free for odd a.
 __device__ __forceinline__ int psi_pos(uint32_t t) { return (int)((t & 3u) * 256u + ((t >> 2) & 255u)); }
 
 // psi^t for any t (mod 2N)
@@ -183,26 +183,72 @@ __device__ __forceinline__ double2 psi_at(const double2* psi_s, uint32_t t)
     return v;
 }
 
-// e^{i pi n2 / 32} (= psi^{32 n2}) and e^{-i pi m / 64} (= psi^{-16 m});
-// c_utw16x23 = 2^23 c_utw16 (N = 1024 inverse: the 1/512 normalisation and
-// the 2^32 Torus32 scale folded in; power-of-two scaling is exact, so the
-// products are those of the unscaled constant times 2^23 bit for bit)
+// e^{i pi n2 / 32} (= psi^{32 n2}), e^{-i pi m / 64} (the N = 2048 untwist's
+// compile-time factor) and c_utwq[q] = conj(psi^{16 (q mod 8) + 256 (q / 8)})
+// 2^23 (N = 1024 inverse: the 1/512 normalisation and the 2^32 Torus32 scale
+// folded in; power-of-two scaling is exact)
 static __constant__ double2 c_tw32[16];
 static __constant__ double2 c_utw16[16];
-static __constant__ double2 c_utw16x23[16];
+static __constant__ double2 c_utwq[16];
+
+// Where register q of `lane` lands after the lvl1 transforms: frequency bin
+// (forward) or coefficient (inverse) k2 + 16 m + 256 b with k2 = lane & 15,
+// m = (q & 7) + 8 (lane >> 4), b = q >> 3.
+__device__ __forceinline__ int ffnt_pos(int lane, int q)
+{
+    return (lane & 15) + 16 * (q & 7) + 128 * (lane >> 4) + 256 * (q >> 3);
+}
+
+// -1 for first-stage lanes n1 = 3 (mod 4), else +1.  The second-stage lanes
+// of the upper half (h = 1) read the first-stage lanes n1 = 1 + 2m, so with
+// this sign folded into the first-stage twiddles their inputs arrive
+// modulated by (-1)^m and their 16-point DFT comes out rotated by 8 bins,
+// which lets both lanes of a radix-2 pair exchange the same registers.
+__device__ __forceinline__ double lane_sign(int lane) { return (lane & 3) == 3 ? -1.0 : 1.0; }
+
+// Radix-2 stage of the 32-point second stage across lanes l and l ^ 16, with
+// every lane doing useful work.  On entry lanes h = 0 hold E0[q] in v[q] and
+// lanes h = 1 hold E1[(q + 8) mod 16] (the lane_sign modulation).  Both send
+// v[8 + j] to the partner, so that lane h holds E0[m] and E1[m] for
+// m = j + 8 h; it writes E0 + w^m E1 to v[j] and E0 - w^m E1 to v[8 + j],
+// w = e^{S 2 pi i / 32}.  Each output is rounded as in the textbook
+// butterfly (t = w E1 rounded, then one add or subtract).
+template <int S>
+__device__ __forceinline__ void radix2_pair(double2 (&v)[16], int h)
+{
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        double2 r;
+        r.x = __shfl_xor_sync(0xffffffffu, v[8 + j].x, 16);
+        r.y = __shfl_xor_sync(0xffffffffu, v[8 + j].y, 16);
+        const double2 e0 = h ? r : v[j];
+        const double2 e1 = h ? v[j] : r;
+        double2 w = c_w32[j + 8 * h];
+        if (S < 0) w.y = -w.y;
+        const double2 t = cmul(e1, w);
+        v[j] = cadd(e0, t);
+        v[8 + j] = csub(e0, t);
+    }
+}
 
 // Forward FFNT of one folded polynomial: in v[n2] = d[n] + i d[n + 512] for
-// n = lane + 32 n2; out as fft512_warp.  The twist psi^n = psi^lane psi^{32 n2}
-// is split into a compile-time factor (before the 16-point DFT) and a per-lane
-// factor merged with the w512^{lane k2} twiddle: psi^{lane (1 + 4 k2)},
-// generated by recurrence from two table reads.
+// n = lane + 32 n2; out v[q] = bin ffnt_pos(lane, q).  (Storing the bins
+// from inside the radix-2 stage keeps fewer registers live but measured
+// slower.)  The twist
+// psi^n = psi^lane psi^{32 n2} is split into a compile-time factor (before
+// the 16-point DFT) and a per-lane factor merged with the w512^{lane k2}
+// twiddle: lane_sign psi^{lane (1 + 4 k2)}, generated by recurrence from two
+// table reads.
 __device__ __forceinline__ void ffnt_forward_warp(double2 (&v)[16], double2* tile,
                                                   const double2* psi_s, int lane)
 {
 #pragma unroll
     for (int n2 = 1; n2 < 16; n2++) v[n2] = cmul(v[n2], c_tw32[n2]);
     dft16<1>(v);
+    const double sg = lane_sign(lane);
     double2 t = psi_s[psi_pos((uint32_t)lane)];
+    t.x *= sg;
+    t.y *= sg;
     const double2 st = psi_s[psi_pos(4u * (uint32_t)lane)];
 #pragma unroll
     for (int k2 = 0; k2 < 16; k2++) {
@@ -217,23 +263,22 @@ __device__ __forceinline__ void ffnt_forward_warp(double2 (&v)[16], double2* til
     for (int m = 0; m < 16; m++) v[m] = tile[k2 * 33 + h + 2 * m];
     __syncwarp();
     dft16<1>(v);
-#pragma unroll
-    for (int m = 0; m < 16; m++) {
-        const double2 w = c_w32[m];
-        v[m] = radix2_xlane(v[m], w, h);
-    }
+    radix2_pair<1>(v, h);
 }
 
-// Inverse FFNT: in v[n2] = Z[lane + 32 n2] (natural bins); out v[m] holds
-// z'[n] * conj(psi^n) * 2^23 (untwisted; 2^23 = 2^32 / 512: the value in
-// Torus32 units before rounding) for n = (lane & 15) + 16 m + 256 (lane >> 4).
+// Inverse FFNT: in v[n2] = Z[lane + 32 n2] (natural bins); out v[q] holds
+// z'[n] conj(psi^n) 2^23 for n = ffnt_pos(lane, q): untwisted and in Torus32
+// units before rounding (2^23 = 2^32 / 512).
 __device__ __forceinline__ void ffnt_inverse_warp(double2 (&v)[16], double2* tile,
                                                   const double2* psi_s, int lane)
 {
     dft16<-1>(v);
     {
+        const double sg = lane_sign(lane);
         const double2 st = psi_s[psi_pos(4u * (uint32_t)lane)];  // w512^{lane} = psi^{4 lane}
-        double2 t = st;
+        double2 t = make_double2(st.x * sg, st.y * sg);
+        v[0].x *= sg;
+        v[0].y *= sg;
 #pragma unroll
         for (int k2 = 1; k2 < 16; k2++) {
             v[k2] = cmulc(v[k2], t);
@@ -248,16 +293,11 @@ __device__ __forceinline__ void ffnt_inverse_warp(double2 (&v)[16], double2* til
     for (int m = 0; m < 16; m++) v[m] = tile[k2 * 33 + h + 2 * m];
     __syncwarp();
     dft16<-1>(v);
+    radix2_pair<-1>(v, h);
+    // untwist conj(psi^{k2 + 128 h}) conj(psi^{16 (q mod 8) + 256 (q / 8)}) 2^23
+    const double2 u = psi_s[psi_pos((uint32_t)(k2 + 128 * h))];
 #pragma unroll
-    for (int m = 0; m < 16; m++) {
-        double2 w = c_w32[m];
-        w.y = -w.y;
-        v[m] = radix2_xlane(v[m], w, h);
-    }
-    // untwist conj(psi^{k2 + 256 h}) conj(psi^{16 m})
-    const double2 u = psi_s[psi_pos((uint32_t)(k2 + 256 * h))];
-#pragma unroll
-    for (int m = 0; m < 16; m++) v[m] = cmul(cmulc(v[m], u), c_utw16x23[m]);
+    for (int q = 0; q < 16; q++) v[q] = cmul(cmulc(v[q], u), c_utwq[q]);
 }
 
 // ---------------------------------------------------------------------------
