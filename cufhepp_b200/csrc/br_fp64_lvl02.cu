@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(G * 256, 1)
                 dft512_fwd_post(v, slot, lane, psi2_at(tab, 2u * lane + par),
                                 psi2_at(tab, 8u * lane));
 #pragma unroll
-                for (int m = 0; m < 16; m++) slot[(lane & 15) + 16 * m + 256 * (lane >> 4)] = v[m];
+                for (int q = 0; q < 16; q++) slot[ffnt_pos(lane, q)] = v[q];
             }
             __syncthreads();
 
@@ -269,15 +269,15 @@ __global__ void __launch_bounds__(G * 256, 1)
             __syncwarp();
             dft512_inv_raw(v, slot, lane, psi2_at(tab, 8u * lane));
             const int k2 = lane & 15, hh = lane >> 4;
-            const double2 u = psi2_at(tab, 2u * (uint32_t)(k2 + 256 * hh) + par);
+            const double2 u = psi2_at(tab, 2u * (uint32_t)(k2 + 128 * hh) + par);
             uint64_t* a = acc + g * kTrlwe2 + j * kN2;
 #pragma unroll
-            for (int m = 0; m < 16; m++) {
-                const int n = 2 * (k2 + 16 * m + 256 * hh) + par;
-                // untwisted value / 1024, then x 2^64  =>  x 2^54
-                const double2 z = cmul(cmulc(v[m], u), c_utw16[m]);
-                const uint64_t lo = to_torus64(z.x * 0x1p54);
-                const uint64_t hi = to_torus64(z.y * 0x1p54);
+            for (int q = 0; q < 16; q++) {
+                const int n = 2 * ffnt_pos(lane, q) + par;
+                // untwisted value / 1024, then x 2^64  =>  x 2^54 (in c_utwq)
+                const double2 z = cmul(cmulc(v[q], u), c_utwq[q]);
+                const uint64_t lo = to_torus64(z.x);
+                const uint64_t hi = to_torus64(z.y);
                 if (KB) {
                     a[n] = lo;
                     a[n + 1024] = hi;
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(64) k_bk2_to_fft(const uint64_t* __restrict__ 
     }
     dft512_fwd_post(v, slots[par], lane, psi2_at(psi2, 2u * lane + par), psi2_at(psi2, 8u * lane));
 #pragma unroll
-    for (int m = 0; m < 16; m++) slots[par][(lane & 15) + 16 * m + 256 * (lane >> 4)] = v[m];
+    for (int q = 0; q < 16; q++) slots[par][ffnt_pos(lane, q)] = v[q];
     __syncthreads();
     double2* dst = out + (size_t)poly * 1024;
     for (int k = threadIdx.x; k < 512; k += 64) {
@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(256, 1)
                 dft512_fwd_post(v, slot, lane, psi2_at(tab, 2u * lane + par),
                                 psi2_at(tab, 8u * lane));
 #pragma unroll
-                for (int m = 0; m < 16; m++) slot[(lane & 15) + 16 * m + 256 * (lane >> 4)] = v[m];
+                for (int q = 0; q < 16; q++) slot[ffnt_pos(lane, q)] = v[q];
             }
             __syncthreads();
 
@@ -535,14 +535,14 @@ __global__ void __launch_bounds__(256, 1)
             double2* scratch = spec + (4 + 2 * j + par) * kSlotStride;  // rows d = 2, 3 are free
             dft512_inv_raw(v, scratch, lane, psi2_at(tab, 8u * lane));
             const int k2 = lane & 15, hh = lane >> 4;
-            const double2 u = psi2_at(tab, 2u * (uint32_t)(k2 + 256 * hh) + par);
+            const double2 u = psi2_at(tab, 2u * (uint32_t)(k2 + 128 * hh) + par);
             uint64_t* a = acc + j * kN2;
 #pragma unroll
-            for (int m = 0; m < 16; m++) {
-                const int n = 2 * (k2 + 16 * m + 256 * hh) + par;
-                const double2 z = cmul(cmulc(v[m], u), c_utw16[m]);
-                const uint64_t lo = to_torus64(z.x * 0x1p54);
-                const uint64_t hi = to_torus64(z.y * 0x1p54);
+            for (int q = 0; q < 16; q++) {
+                const int n = 2 * ffnt_pos(lane, q) + par;
+                const double2 z = cmul(cmulc(v[q], u), c_utwq[q]);  // x 2^54 in c_utwq
+                const uint64_t lo = to_torus64(z.x);
+                const uint64_t hi = to_torus64(z.y);
                 if (KB) {
                     a[n] = lo;
                     a[n + 1024] = hi;
@@ -642,19 +642,21 @@ cudaError_t launch_bk2_to_fft(const uint64_t* bk, int npolys, const double2* psi
 // The FFT constants of this translation unit (fft64.cuh keeps them per file)
 cudaError_t upload_fft2_constants(void)
 {
-    double2 w[16], t32[16], u16[16];
+    double2 w[16], t32[16], uq[16];
     const long double pi = 3.141592653589793238462643383279502884L;
     for (int k = 0; k < 16; k++) {
         const long double a = 2 * pi * k / 32;
         w[k] = make_double2((double)cosl(a), (double)sinl(a));
         const long double b = pi * k / 32;   // psi2^{64 k}
         t32[k] = make_double2((double)cosl(b), (double)sinl(b));
-        const long double c = -pi * k / 64;  // conj(psi2^{32 k})
-        u16[k] = make_double2((double)cosl(c), (double)sinl(c));
+        // conj(psi2^{32 (k mod 8) + 512 (k / 8)}) 2^54: the untwist of register
+        // k, the 1/1024 normalisation and the 2^64 Torus64 scale
+        const long double c = -pi * ((k & 7) + 16 * (k >> 3)) / 64;
+        uq[k] = make_double2((double)(cosl(c) * 0x1p54L), (double)(sinl(c) * 0x1p54L));
     }
     cudaError_t e = cudaMemcpyToSymbol(c_w32, w, sizeof(w));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tw32, t32, sizeof(t32));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_utw16, u16, sizeof(u16));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_utwq, uq, sizeof(uq));
     return e;
 }
 

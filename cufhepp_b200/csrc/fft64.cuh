@@ -183,12 +183,13 @@ __device__ __forceinline__ double2 psi_at(const double2* psi_s, uint32_t t)
     return v;
 }
 
-// e^{i pi n2 / 32} (= psi^{32 n2}), e^{-i pi m / 64} (the N = 2048 untwist's
-// compile-time factor) and c_utwq[q] = conj(psi^{16 (q mod 8) + 256 (q / 8)})
-// 2^23 (N = 1024 inverse: the 1/512 normalisation and the 2^32 Torus32 scale
-// folded in; power-of-two scaling is exact)
+// e^{i pi n2 / 32} (= psi^{32 n2}, the compile-time part of the forward
+// twist) and c_utwq[q] = e^{-i pi ((q mod 8) + 16 (q / 8)) / 64} times a
+// power of two that each translation unit chooses (the compile-time part of
+// the untwist of register q, with the inverse's normalisation and Torus
+// scale folded in: 2^23 for N = 1024 Torus32, 2^54 for N = 2048 Torus64;
+// power-of-two scaling commutes with every rounding)
 static __constant__ double2 c_tw32[16];
-static __constant__ double2 c_utw16[16];
 static __constant__ double2 c_utwq[16];
 
 // Where register q of `lane` lands after the lvl1 transforms: frequency bin
@@ -306,13 +307,16 @@ __device__ __forceinline__ void ffnt_inverse_warp(double2 (&v)[16], double2* til
 // whose twist psi2^{2m (+1)} = psi2^{2 lane (+1)} psi2^{64 n2} has the same
 // compile-time factor c_tw32[n2] as the N = 1024 case; the per-lane factor
 // t0 and the 512-point twiddle w512^{lane k2} = psi2^{8 lane k2} are merged
-// into the geometric sequence t0 * step^k2.  In: v[n2] already multiplied by
-// c_tw32[n2].  Out: natural bins, lane (k2 + 16 h), register m -> bin
-// k2 + 16 m + 256 h.
+// into the geometric sequence t0 * step^k2 (with the lane_sign modulation of
+// radix2_pair).  In: v[n2] already multiplied by c_tw32[n2].  Out: v[q] =
+// bin ffnt_pos(lane, q) of the half.
 __device__ __forceinline__ void dft512_fwd_post(double2 (&v)[16], double2* tile, int lane,
                                                 double2 t, const double2 step)
 {
     dft16<1>(v);
+    const double sg = lane_sign(lane);
+    t.x *= sg;
+    t.y *= sg;
 #pragma unroll
     for (int k2 = 0; k2 < 16; k2++) {
         v[k2] = cmul(v[k2], t);
@@ -326,21 +330,19 @@ __device__ __forceinline__ void dft512_fwd_post(double2 (&v)[16], double2* tile,
     for (int m = 0; m < 16; m++) v[m] = tile[k2 * 33 + h + 2 * m];
     __syncwarp();
     dft16<1>(v);
-#pragma unroll
-    for (int m = 0; m < 16; m++) {
-        const double2 w = c_w32[m];
-        v[m] = radix2_xlane(v[m], w, h);
-    }
+    radix2_pair<1>(v, h);
 }
 
-// Unscaled inverse 512-point DFT: in v[n2] = X[lane + 32 n2]; out v[m] =
-// sum_k X[k] w512^{-n k} for n = (lane & 15) + 16 m + 256 (lane >> 4).
-// wl = w512^{lane}.
+// Unscaled inverse 512-point DFT: in v[n2] = X[lane + 32 n2]; out v[q] =
+// sum_k X[k] w512^{-n k} for n = ffnt_pos(lane, q).  wl = w512^{lane}.
 __device__ __forceinline__ void dft512_inv_raw(double2 (&v)[16], double2* tile, int lane,
                                                const double2 wl)
 {
     dft16<-1>(v);
-    double2 t = wl;
+    const double sg = lane_sign(lane);
+    double2 t = make_double2(wl.x * sg, wl.y * sg);
+    v[0].x *= sg;
+    v[0].y *= sg;
 #pragma unroll
     for (int k2 = 1; k2 < 16; k2++) {
         v[k2] = cmulc(v[k2], t);
@@ -354,12 +356,7 @@ __device__ __forceinline__ void dft512_inv_raw(double2 (&v)[16], double2* tile, 
     for (int m = 0; m < 16; m++) v[m] = tile[k2 * 33 + h + 2 * m];
     __syncwarp();
     dft16<-1>(v);
-#pragma unroll
-    for (int m = 0; m < 16; m++) {
-        double2 w = c_w32[m];
-        w.y = -w.y;
-        v[m] = radix2_xlane(v[m], w, h);
-    }
+    radix2_pair<-1>(v, h);
 }
 
 }  // namespace cufhe
