@@ -943,17 +943,42 @@ def run_cb(args, torch, engine, client, P, sk, ek1, rank, ws, flush, gates_wl):
 
 
 _PEAK = {}
+PROBES = {}
+
+
+def _probe(kind, fn, per_clk_name, per_clk_div):
+    """Best of three runs of a throughput probe, with the SM clock sampled
+    while the probes ran, so that the denominator can be checked against
+    clock x SMs x units: `per_clk_name` is the probe's rate per SM per clock
+    (FP64 FMAs, or INT8 multiply-adds counted as 2 ops: per_clk_div = 2)."""
+    import torch
+    clk = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clk.start()
+    t0 = time.perf_counter()
+    runs = [fn() for _ in range(3)]
+    while time.perf_counter() - t0 < 1.2:  # at least ~6 clock samples
+        runs.append(fn())
+    c = clk.stop()
+    best = max(runs)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    rec = {"value": best, "runs": len(runs), "sms": sms,
+           "sm_mhz_median": c["sm_mhz"] if c else None,
+           "clock_reasons": c["reasons"] if c else None}
+    if c and c["sm_mhz"]:
+        rec[per_clk_name] = best * 1e12 / per_clk_div / (sms * c["sm_mhz"] * 1e6)
+    PROBES[kind] = rec
+    return best
 
 
 def engine_peak_fp64(engine):
     if "fp64" not in _PEAK:
-        _PEAK["fp64"] = max(engine.measure_fp64_peak() for _ in range(3))
+        _PEAK["fp64"] = _probe("fp64_tflops", engine.measure_fp64_peak, "dfma_per_clk_per_sm", 2)
     return _PEAK["fp64"]
 
 
 def engine_peak_int8(engine):
     if "int8" not in _PEAK:
-        _PEAK["int8"] = max(engine.measure_int8_peak() for _ in range(3))
+        _PEAK["int8"] = _probe("int8_tops", engine.measure_int8_peak, "i8_macs_per_clk_per_sm", 2)
     return _PEAK["int8"]
 
 
@@ -1031,6 +1056,7 @@ def run_ours(args):
             "gpu_launches": primary["gpu_launches"], "clocks": primary["clocks"],
             "kernel_ms_per_step": primary["kernel_ms_per_step"],
             "vs_reference_a100_published": primary["value"] / A100_PUBLISHED,
+            "peak_probes": PROBES,
         }
         line["config"]["keybundle"] = kb
         if len(paths) > 1:

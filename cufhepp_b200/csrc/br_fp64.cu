@@ -49,6 +49,19 @@ constexpr size_t br_smem_bytes()
            sizeof(uint32_t) * G * kTrlwe + sizeof(uint16_t) * G * kAbarStride;
 }
 
+// Word of coefficient n (0 <= n < 2N) of a lane's accumulator in shared
+// memory.  The KeyBundle form flips bit 4 when bit 7 is set: the inverse
+// transforms store coefficients n and n + 128 from lanes l and l + 16 in one
+// instruction, which would otherwise fall in the same bank; the forward
+// transforms' reads of 32 consecutive coefficients stay conflict-free.  (The
+// plain form keeps the natural order: its rotated reads X^a acc start
+// anywhere.)
+template <bool KB>
+__device__ __forceinline__ int acc_ix(int n)
+{
+    return KB ? n ^ (((n >> 7) & 1) << 4) : n;
+}
+
 // signed digit d (0 = most significant) of an offset Torus32 value
 __device__ __forceinline__ double digit_of(uint32_t t, int d)
 {
@@ -83,13 +96,13 @@ __global__ void __launch_bounds__(G * 128, G == 1 ? 3 : (G == 2 ? 2 : 1)) k_br_f
             abar[g * kAbarStride + i] = ok ? (uint16_t)((x[i] + (1u << 20)) >> 21) : 0;
         const uint32_t bar = ok ? 2u * kN - (x[kN0] >> 21) : 2u * kN;
         for (int i = tid; i < kN; i += blockDim.x) {
-            acc[g * kTrlwe + i] = 0;
+            acc[g * kTrlwe + acc_ix<KB>(i)] = 0;
             uint32_t v;
             if (bar == 2u * kN)
                 v = mu;
             else
                 v = (((uint32_t)i < (bar & (kN - 1))) ^ (bar >> 10)) ? 0u - mu : mu;
-            acc[g * kTrlwe + kN + i] = v;
+            acc[g * kTrlwe + acc_ix<KB>(kN + i)] = v;
         }
     }
     __syncthreads();
@@ -110,7 +123,7 @@ __global__ void __launch_bounds__(G * 128, G == 1 ? 3 : (G == 2 ? 2 : 1)) k_br_f
 #pragma unroll
             for (int n2 = 0; n2 < 16; n2++) {
                 const int n = lane + 32 * n2;
-                uint32_t lo = a[n], hi = a[n + kHalfN];
+                uint32_t lo = a[acc_ix<KB>(n)], hi = a[acc_ix<KB>(n + kHalfN)];
                 if (!KB) {
                     // X^abar acc - acc (include/gatebootstrapping_gpu.cuh:114-138)
                     uint32_t rl = a[(n - ab) & (kN - 1)];
@@ -130,59 +143,98 @@ __global__ void __launch_bounds__(G * 128, G == 1 ? 3 : (G == 2 ? 2 : 1)) k_br_f
         __syncthreads();
 
         // ---- phase 2: key multiply-accumulate, thread f = frequency bin.
-        // Rows outermost: each digit spectrum D[g][r] is read from shared
-        // memory once for both output polynomials, and the KeyBundle factors
-        // once per lane; per bin and output the additions run in the same
-        // order as in k_br_fp64_clu (rows 0..3, then H, x01, x0, x1), so the
-        // two kernels agree bit for bit.
+        // One (bin, output polynomial) item at a time with all twelve key
+        // words of the item (rows x keys) loaded before any is used: the
+        // phase is bound by the latency of the key rows from L2, and this
+        // keeps 12 loads per thread in flight (a rows-outermost loop with both
+        // outputs' accumulators live leaves room for only one row's 6).  The
+        // output of polynomial 0 overwrites row 0's spectrum, which polynomial
+        // 1 still reads, so it is held in registers until both are done.  Per
+        // bin and output the additions run in the same order as in
+        // k_br_fp64_clu (rows 0..3, then H, x01, x0, x1): bit-identical.
         if (KB) {
             const double2* bk = bkf + (size_t)p * 3 * kTrgswF;
-            for (int f = tid; f < kHalfN; f += blockDim.x) {
-                double2 s[G][2][3], h[G][2];
-#pragma unroll
-                for (int r = 0; r < 4; r++) {
-                    double2 b[3][2];
-#pragma unroll
-                    for (int e = 0; e < 3; e++)
-#pragma unroll
-                        for (int j = 0; j < 2; j++)
-                            b[e][j] = __ldg(&bk[((e * 4 + r) * 2 + j) * kHalfN + f]);
-#pragma unroll
-                    for (int g = 0; g < G; g++) {
-                        const double2 D = spec[(g * 4 + r) * kSlotStride + f];
-#pragma unroll
-                        for (int j = 0; j < 2; j++)
-#pragma unroll
-                            for (int e = 0; e < 3; e++)
-                                s[g][j][e] = r == 0 ? cfma(make_double2(0.0, 0.0), D, b[e][j])
-                                                    : cfma(s[g][j][e], D, b[e][j]);
-                        // FFNT(H 2^-32) = 2^-8 (d = 0), 2^-16 (d = 1) on poly j = r / 2
-                        if ((r & 1) == 0)
-                            h[g][r >> 1] = D;
-                        else
-                            h[g][r >> 1] = make_double2(fma(h[g][r >> 1].x, 0x1p-8, D.x * 0x1p-16),
-                                                        fma(h[g][r >> 1].y, 0x1p-8, D.y * 0x1p-16));
-                    }
-                }
-                const uint32_t ef = 1u + 4u * (uint32_t)f;
+            // KeyBundle roots psi^{(1 + 4 f) a} (a = a0 + a1, a0, a1) of the
+            // thread's first bin.  With two lanes per CTA the thread's bins
+            // are f and f + 256, and psi^{(1 + 4 (f + 256)) a} = (-1)^a
+            // psi^{(1 + 4 f) a} exactly (a sign flip), so the roots are
+            // gathered once per step; the table gathers are bank-conflicted
+            // for even a.  Other lane counts gather per bin.
+            double2 root[G][3];
+            uint32_t odd[G];
+            if (G == 2) {
+                const uint32_t ef = 1u + 4u * (uint32_t)tid;
 #pragma unroll
                 for (int g = 0; g < G; g++) {
                     const uint32_t a0 = abar[g * kAbarStride + 2 * p];
                     const uint32_t a1 = abar[g * kAbarStride + 2 * p + 1];
-                    double2 x0 = psi_at(psi_s, ef * a0);
-                    double2 x1 = psi_at(psi_s, ef * a1);
-                    double2 x01 = psi_at(psi_s, ef * (a0 + a1));
-                    x0.x -= 1.0;
-                    x1.x -= 1.0;
-                    x01.x -= 1.0;
+                    root[g][0] = psi_at(psi_s, ef * (a0 + a1));
+                    root[g][1] = psi_at(psi_s, ef * a0);
+                    root[g][2] = psi_at(psi_s, ef * a1);
+                    odd[g] = (((a0 + a1) & 1u) << 0) | ((a0 & 1u) << 1) | ((a1 & 1u) << 2);
+                }
+            }
+#pragma unroll 1
+            for (int f = tid; f < kHalfN; f += blockDim.x) {
+                const uint32_t ef = 1u + 4u * (uint32_t)f;
+                double2 o0[G];
 #pragma unroll
-                    for (int j = 0; j < 2; j++) {
-                        double2 o = h[g][j];
-                        o = cfma(o, x01, s[g][j][0]);
-                        o = cfma(o, x0, s[g][j][1]);
-                        o = cfma(o, x1, s[g][j][2]);
-                        spec[(g * 4 + j) * kSlotStride + f] = o;
+                for (int j = 0; j < 2; j++) {
+                    double2 b[4][3];
+#pragma unroll
+                    for (int r = 0; r < 4; r++)
+#pragma unroll
+                        for (int e = 0; e < 3; e++)
+                            b[r][e] = __ldg(&bk[((e * 4 + r) * 2 + j) * kHalfN + f]);
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        double2 D[4], sum[3];
+#pragma unroll
+                        for (int r = 0; r < 4; r++) D[r] = spec[(g * 4 + r) * kSlotStride + f];
+#pragma unroll
+                        for (int r = 0; r < 4; r++)
+#pragma unroll
+                            for (int e = 0; e < 3; e++)
+                                sum[e] = r == 0 ? cfma(make_double2(0.0, 0.0), D[r], b[r][e])
+                                                : cfma(sum[e], D[r], b[r][e]);
+                        // FFNT(H 2^-32) = 2^-8 (d = 0), 2^-16 (d = 1) on poly j
+                        double2 o = make_double2(fma(D[2 * j].x, 0x1p-8, D[2 * j + 1].x * 0x1p-16),
+                                                 fma(D[2 * j].y, 0x1p-8, D[2 * j + 1].y * 0x1p-16));
+                        double2 x01, x0, x1;
+                        if (G == 2) {
+                            x01 = root[g][0];
+                            x0 = root[g][1];
+                            x1 = root[g][2];
+                        } else {
+                            const uint32_t a0 = abar[g * kAbarStride + 2 * p];
+                            const uint32_t a1 = abar[g * kAbarStride + 2 * p + 1];
+                            x01 = psi_at(psi_s, ef * (a0 + a1));
+                            x0 = psi_at(psi_s, ef * a0);
+                            x1 = psi_at(psi_s, ef * a1);
+                        }
+                        x0.x -= 1.0;
+                        x1.x -= 1.0;
+                        x01.x -= 1.0;
+                        o = cfma(o, x01, sum[0]);
+                        o = cfma(o, x0, sum[1]);
+                        o = cfma(o, x1, sum[2]);
+                        if (j == 0) {
+                            o0[g] = o;
+                        } else {
+                            spec[(g * 4 + 0) * kSlotStride + f] = o0[g];
+                            spec[(g * 4 + 1) * kSlotStride + f] = o;
+                        }
                     }
+                }
+                if (G == 2) {
+#pragma unroll
+                    for (int g = 0; g < G; g++)
+#pragma unroll
+                        for (int e = 0; e < 3; e++)
+                            if ((odd[g] >> e) & 1u) {
+                                root[g][e].x = -root[g][e].x;
+                                root[g][e].y = -root[g][e].y;
+                            }
                 }
             }
         } else {
@@ -230,8 +282,8 @@ __global__ void __launch_bounds__(G * 128, G == 1 ? 3 : (G == 2 ? 2 : 1)) k_br_f
                 const uint32_t lo = (uint32_t)__double2ll_rn(u.x);
                 const uint32_t hi = (uint32_t)__double2ll_rn(u.y);
                 if (KB) {
-                    a[n] = lo;
-                    a[n + kHalfN] = hi;
+                    a[acc_ix<KB>(n)] = lo;
+                    a[acc_ix<KB>(n + kHalfN)] = hi;
                 } else {
                     a[n] += lo;
                     a[n + kHalfN] += hi;
@@ -247,11 +299,12 @@ __global__ void __launch_bounds__(G * 128, G == 1 ? 3 : (G == 2 ? 2 : 1)) k_br_f
         if (l >= lanes) break;
         const uint32_t* a = acc + g * kTrlwe;
         if (acc_out)
-            for (int i = tid; i < kTrlwe; i += blockDim.x) acc_out[(size_t)l * kTrlwe + i] = a[i];
+            for (int i = tid; i < kTrlwe; i += blockDim.x)
+                acc_out[(size_t)l * kTrlwe + i] = a[acc_ix<KB>(i)];
         if (lane_out) {
             uint32_t* o = lane_out + (size_t)l * kTlwe1;
             for (int i = tid; i <= kN; i += blockDim.x)
-                o[i] = i == kN ? a[kN] : (i == 0 ? a[0] : 0u - a[kN - i]);
+                o[i] = i == kN ? a[acc_ix<KB>(kN)] : (i == 0 ? a[0] : 0u - a[acc_ix<KB>(kN - i)]);
         }
     }
 }
