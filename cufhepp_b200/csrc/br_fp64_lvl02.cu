@@ -68,6 +68,15 @@ __device__ __forceinline__ double2 psi2_at(const double2* tab, uint32_t t)
     return v;
 }
 
+// i^m v (exact: swaps and negations, as in psi2_at), so that
+// psi2_at(t + 1024 m) = mul_ipow(psi2_at(t), m)
+__device__ __forceinline__ double2 mul_ipow(double2 v, uint32_t m)
+{
+    if (m & 1u) v = make_double2(-v.y, v.x);
+    if (m & 2u) v = make_double2(-v.x, -v.y);
+    return v;
+}
+
 __device__ __forceinline__ double digit2_of(uint64_t t, int d)
 {
     return (double)((int32_t)((t >> (54 - 10 * d)) & 1023u) - 512);
@@ -186,17 +195,20 @@ __global__ void __launch_bounds__(G * 256, 1)
                 const double2* sl = spec + g * 8 * kSlotStride;
                 double2 fac[2][3];
                 if (KB) {
+                    // bin k + 512: the roots of bin k times i^{2 a} (exact)
                     const uint32_t a0 = abar[g * kAbarStride2 + 2 * p];
                     const uint32_t a1 = abar[g * kAbarStride2 + 2 * p + 1];
+                    const uint32_t am[3] = {a0 + a1, a0, a1};
+                    const uint32_t e = 1u + 4u * (uint32_t)k;
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const uint32_t e = 1u + 4u * (uint32_t)(k + 512 * h);
-                        fac[h][0] = psi2_at(tab, e * (a0 + a1));
-                        fac[h][1] = psi2_at(tab, e * a0);
-                        fac[h][2] = psi2_at(tab, e * a1);
+                    for (int f = 0; f < 3; f++) {
+                        fac[0][f] = psi2_at(tab, e * am[f]);
+                        fac[1][f] = mul_ipow(fac[0][f], 2u * am[f]);
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
 #pragma unroll
                         for (int f = 0; f < 3; f++) fac[h][f].x -= 1.0;
-                    }
                 }
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
@@ -456,17 +468,20 @@ __global__ void __launch_bounds__(256, 1)
                 const double2 w4 = psi2_at(tab, 4u * (uint32_t)k);
                 double2 fac[2][3];
                 if (KB) {
+                    // bin k + 512: the roots of bin k times i^{2 a} (exact)
                     const uint32_t a0 = abar[2 * p];
                     const uint32_t a1 = abar[2 * p + 1];
+                    const uint32_t am[3] = {a0 + a1, a0, a1};
+                    const uint32_t e = 1u + 4u * (uint32_t)k;
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const uint32_t e = 1u + 4u * (uint32_t)(k + 512 * h);
-                        fac[h][0] = psi2_at(tab, e * (a0 + a1));
-                        fac[h][1] = psi2_at(tab, e * a0);
-                        fac[h][2] = psi2_at(tab, e * a1);
+                    for (int f = 0; f < 3; f++) {
+                        fac[0][f] = psi2_at(tab, e * am[f]);
+                        fac[1][f] = mul_ipow(fac[0][f], 2u * am[f]);
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
 #pragma unroll
                         for (int f = 0; f < 3; f++) fac[h][f].x -= 1.0;
-                    }
                 }
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
