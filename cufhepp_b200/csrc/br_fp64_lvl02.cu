@@ -55,13 +55,23 @@ constexpr size_t br2_smem_bytes()
 // has an SM (and its whole register file) to itself
 constexpr size_t kSmemOneCta = 120 * 1024;
 
-// psi2^t for any t (mod 4096) from the table of s in [0, 512]
+// Shared-memory position of psi2^s (s in [0, 512]): the low 3 bits XORed
+// with the next 3, so that the kernels' strided gathers (psi2^{(1+4k) a},
+// psi2^{4 k}, psi2^{2 lane + p}, psi2^{8 lane}) spread over the banks: 2.3
+// wavefronts per 8 lanes on average for the KeyBundle roots (4.6 in natural
+// order), 1 to 1.5 for the others (2 to 8).
+__device__ __forceinline__ uint32_t psi2_pos(uint32_t s) { return s ^ ((s >> 3) & 7u); }
+
+// psi2^t for any t (mod 4096) from the table of s in [0, 512] (kSwz: the
+// shared-memory copy, in psi2_pos order; else the natural-order table)
+template <bool kSwz = true>
 __device__ __forceinline__ double2 psi2_at(const double2* tab, uint32_t t)
 {
     const uint32_t q = (t >> 10) & 3u;
     const uint32_t s = t & 1023u;
     const bool refl = s > 512u;
-    const double2 w = tab[refl ? 1024u - s : s];
+    const uint32_t i = refl ? 1024u - s : s;
+    const double2 w = tab[kSwz ? psi2_pos(i) : i];
     double2 v = refl ? make_double2(w.y, w.x) : w;
     if (q & 1u) v = make_double2(-v.y, v.x);
     if (q & 2u) v = make_double2(-v.x, -v.y);
@@ -119,7 +129,7 @@ __global__ void __launch_bounds__(G * 256, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int lane_base = blockIdx.x * G;
 
-    for (int t = tid; t < kPsi2Entries; t += blockDim.x) tab[t] = psi2[t];
+    for (int t = tid; t < kPsi2Entries; t += blockDim.x) tab[psi2_pos(t)] = psi2[t];
 #pragma unroll 1
     for (int g = 0; g < G; g++) {
         const int l = lane_base + g;
@@ -338,13 +348,14 @@ __global__ void __launch_bounds__(64) k_bk2_to_fft(const uint64_t* __restrict__ 
                              (double)(int64_t)src[n + 1024] * 0x1p-64);
         if (n2) v[n2] = cmul(v[n2], c_tw32[n2]);
     }
-    dft512_fwd_post(v, slots[par], lane, psi2_at(psi2, 2u * lane + par), psi2_at(psi2, 8u * lane));
+    dft512_fwd_post(v, slots[par], lane, psi2_at<false>(psi2, 2u * lane + par),
+                    psi2_at<false>(psi2, 8u * lane));
 #pragma unroll
     for (int q = 0; q < 16; q++) slots[par][ffnt_pos(lane, q)] = v[q];
     __syncthreads();
     double2* dst = out + (size_t)poly * 1024;
     for (int k = threadIdx.x; k < 512; k += 64) {
-        const double2 wo = cmul(slots[1][k], psi2_at(psi2, 4u * k));
+        const double2 wo = cmul(slots[1][k], psi2_at<false>(psi2, 4u * k));
         dst[k] = cadd(slots[0][k], wo);
         dst[k + 512] = csub(slots[0][k], wo);
     }
@@ -399,7 +410,7 @@ __global__ void __launch_bounds__(256, 1)
     const int l = blockIdx.x / R;
     const bool ok = l < lanes;
 
-    for (int t = tid; t < kPsi2Entries; t += blockDim.x) tab[t] = psi2[t];
+    for (int t = tid; t < kPsi2Entries; t += blockDim.x) tab[psi2_pos(t)] = psi2[t];
     {
         const int src = ok ? l % in_count : 0;
         const uint64_t mul = mu >> (mu_shift * (ok ? l / in_count : 0));
