@@ -477,6 +477,19 @@ def run_path(args, path, torch, engine, client, P, sk, workload, rank, ws, flush
                   "peak_source": "measured tcgen05.mma.kind::i8 M128 N256 K32 probe on this GPU "
                                  "(cufhe_measure_int8_peak, random operands; the peaks file has "
                                  "no INT8 figure)"}
+    if rl is not None:
+        # where the launch time comes from, and the same work over the
+        # throughput loop's own time per batch (which also holds the key
+        # switch, about 1 % of it)
+        rl["launch_time_source"] = (
+            "CUDA events on the launching stream around every launch of the kernel in the "
+            "one-batch-at-a-time timed loop (the p50 loop: batches back to back, L2 flushed "
+            "between them), each launch alone on the GPU; in the throughput loop consecutive "
+            "batches overlap on two streams, so per-launch event times there would include the "
+            "sharing")
+        rl["launches_timed"] = kern[br][1]
+        rl["frac_over_throughput_loop_step"] = rl["work_per_launch"] / (
+            total_ms / args.steps * 1e-3) / 1e12 / rl["peak"]
     res = {
         "value": value, "ms_per_step": total_ms / args.steps,
         "p50_gate_latency_ms": statistics.median(step_ms),
