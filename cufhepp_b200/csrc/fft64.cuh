@@ -13,7 +13,11 @@
 //   4. lane (k2 + 16 h) holds the n1 = h + 2m half of sequence k2; 16-point
 //      DFT over m in registers.
 //   5. one radix-2 stage across lanes l and l ^ 16 (warp shuffle).
-//   Output: lane (k2 + 16 h), register m holds bin k2 + 16 m + 256 h.
+//   Output: lane (k2 + 16 h), register m holds bin k2 + 16 m + 256 h
+//   (fft512_warp: key conversion, CMUX).  The blind-rotation transforms
+//   (ffnt_forward_warp / ffnt_inverse_warp and the N = 2048 halves) run step
+//   5 with both lanes of a pair busy (radix2_pair) and leave register q at
+//   ffnt_pos(lane, q) instead.
 //
 // The reference runs one 512-point FFT per CTA with 256 threads and
 // __syncthreads between stages; here a warp owns a whole transform and only
