@@ -553,7 +553,11 @@ __global__ void __launch_bounds__(kGemmPThreads, 1) k_i8_gemm_p(const int8_t* __
 // Every wait is bounded; both CTAs always meet at the closing cluster barrier
 // before the pair releases its TMEM.
 constexpr int kHalfTile = kTileBytes / 2;                                  // 16 KB
-constexpr size_t kSmemPairB = (size_t)kPStages * kHalfTile;                // 80 KB
+// digit ring depth of the pair form (half chunks; A slots: 32 TMEM columns
+// each from column 256).  Measured at 4789 lanes, KeyBundle: 5 stages
+// 116.5 ms per rotation, 6 stages 115.1 ms, 8 stages 116.5 ms.
+constexpr int kPairStages = 6;
+constexpr size_t kSmemPairB = (size_t)kPairStages * kHalfTile;
 constexpr size_t kSmemGemmPair = 1024 + kSmemPairB + kSmemPV + kSmemPRed + 512;
 constexpr uint32_t kIdescPair = idesc_i8(256, kGroup);
 
@@ -571,9 +575,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmPThreads, 1)
     int8_t* vs = reinterpret_cast<int8_t*>(smem + kSmemPairB);
     uint32_t* red = reinterpret_cast<uint32_t*>(smem + kSmemPairB + kSmemPV);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kSmemPairB + kSmemPV + kSmemPRed);
-    uint64_t* full = bars;                    // [kPStages]
-    uint64_t* empty = full + kPStages;        // [kPStages]
-    uint64_t* acc_full = empty + kPStages;
+    uint64_t* full = bars;                    // [kPairStages]
+    uint64_t* empty = full + kPairStages;        // [kPairStages]
+    uint64_t* acc_full = empty + kPairStages;
     uint64_t* acc_empty = acc_full + 1;
     uint64_t* bar_v = acc_empty + 1;
     uint64_t* red_full = bar_v + 1;
@@ -604,7 +608,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmPThreads, 1)
         s_geo[2] = ncj;
         s_geo[3] = split;
         s_geo[4] = combo;
-        for (int s = 0; s < kPStages; s++) {
+        for (int s = 0; s < kPairStages; s++) {
             // (even CTA) 128 own generator threads, its producer, 4 odd generator warps
             mbar_init(&full[s], 128 + 1 + 4);
             mbar_init(&empty[s], 1);
@@ -638,10 +642,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmPThreads, 1)
                 const int group = t / (kN / kRowsCoef);
                 const uint8_t* gt = tiles + (size_t)group * kChunks * kTileBytes;
                 for (int lk = par; lk < nk; lk += 2) {
-                    const int kc = k0 + lk, gc = gbase + lk, s = gc % kPStages;
+                    const int kc = k0 + lk, gc = gbase + lk, s = gc % kPairStages;
                     if (s_fail) break;
-                    if (gc >= kPStages &&
-                        !mbar_wait(&empty[s], (uint32_t)((gc / kPStages) - 1) & 1)) {
+                    if (gc >= kPairStages &&
+                        !mbar_wait(&empty[s], (uint32_t)((gc / kPairStages) - 1) & 1)) {
                         s_fail = 1;
                         break;
                     }
@@ -672,8 +676,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmPThreads, 1)
                 }
                 tc_fence_after();
                 for (int lk = 0; lk < nk; lk++, gc++) {
-                    const int s = gc % kPStages;
-                    if (!mbar_wait(&full[s], (uint32_t)(gc / kPStages) & 1)) {
+                    const int s = gc % kPairStages;
+                    if (!mbar_wait(&full[s], (uint32_t)(gc / kPairStages) & 1)) {
                         s_fail = 1;
                         break;
                     }
@@ -700,14 +704,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmPThreads, 1)
             unit_of(it, s_geo, t, k0, nk);
             const int n = (t % (kN / kRowsCoef)) * kRowsCoef + lane;
             for (int lk = wg; lk < nk; lk += 2) {
-                const int kc = k0 + lk, gc = gbase + lk, s = gc % kPStages;
+                const int kc = k0 + lk, gc = gbase + lk, s = gc % kPairStages;
                 if (__any_sync(0xffffffffu, s_fail != 0)) {
                     ok = false;
                     break;
                 }
-                if (gc >= kPStages &&
+                if (gc >= kPairStages &&
                     !__all_sync(0xffffffffu,
-                                mbar_wait(&empty[s], (uint32_t)((gc / kPStages) - 1) & 1))) {
+                                mbar_wait(&empty[s], (uint32_t)((gc / kPairStages) - 1) & 1))) {
                     ok = false;
                     break;
                 }
@@ -835,7 +839,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kGemmPThreads, 1)
         // wait (bounded) for copies and MMA batches that may be in flight (the
         // chunk barriers, which count both CTAs' copies, live in the even CTA)
         if (rank == 0)
-            for (int s = 0; s < kPStages; s++) mbar_wait(&full[s], 0), mbar_wait(&full[s], 1);
+            for (int s = 0; s < kPairStages; s++) mbar_wait(&full[s], 0), mbar_wait(&full[s], 1);
         mbar_wait(acc_full, 0), mbar_wait(acc_full, 1);
     }
     tc_fence_before();
