@@ -37,6 +37,14 @@ constexpr int kStages = 4;
 constexpr size_t kSmem = 1024 + (size_t)kStages * kStageBytes + 256;
 constexpr uint32_t kIdescIks = idesc_i8(kMGates, kNCols);
 constexpr uint32_t kTmemColsIks = 256;
+// MT unit tiles per CTA share every key chunk (MT accumulators of 256 TMEM
+// columns): a stage holds MT A tiles and one B tile.  MT = 2 halves the key
+// bytes streamed per unit, for keys far larger than L2 (private key
+// switching: 2.5 GB per function).
+template <int MT>
+constexpr int iks_stages() { return MT == 1 ? kStages : 3; }
+template <int MT>
+constexpr size_t iks_smem() { return 1024 + (size_t)iks_stages<MT>() * (MT * kATile + kBTile) + 256; }
 
 // K = (i, j, e) of an input with NIN mask coefficients: NIN * 7 * 2
 template <int NIN>
@@ -266,7 +274,7 @@ struct OutMap {
 };
 
 // xb (optional) is added to output word OUTW - 1; valid (optional) masks units.
-template <int CH, int NT, int OUTW>
+template <int CH, int NT, int OUTW, int MT = 1>
 __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__ atiles,
                                                      const uint8_t* __restrict__ btiles,
                                                      const uint32_t* __restrict__ xb,
@@ -274,29 +282,36 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
                                                      uint32_t* __restrict__ dst, OutMap om,
                                                      int* __restrict__ err)
 {
+    constexpr int S = iks_stages<MT>();
+    constexpr int SB = MT * kATile + kBTile;  // stage bytes: MT A tiles, then the B tile
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t raw_addr = smem_u32(smem_raw);
     unsigned char* smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)kStages * kStageBytes);
-    uint64_t* empty = full + kStages;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(empty + kStages);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)S * SB);
+    uint64_t* empty = full + S;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(empty + S);
     __shared__ int s_fail;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int gt = blockIdx.x / NT, nt = blockIdx.x % NT;
-    const uint8_t* ga = atiles + (size_t)gt * CH * kATile;
+    // this CTA's unit tiles: gt * MT + m for m < mc
+    const int gtiles = (units + kMGates - 1) / kMGates;
+    const int mc = gtiles - gt * MT < MT ? gtiles - gt * MT : MT;
+    const uint8_t* ga = atiles + (size_t)gt * MT * CH * kATile;
     const uint8_t* gb = btiles + (size_t)nt * CH * kBTile;
-    int pend[kStages] = {0, 0, 0, 0};  // thread 0: 1 + parity of an outstanding fill
+    int pend[S];  // thread 0: 1 + parity of an outstanding fill
+#pragma unroll
+    for (int s = 0; s < S; s++) pend[s] = 0;
     int last_commit = -1;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     ::"r"(smem_u32(tmem_slot)), "r"(kTmemColsIks));
+                     ::"r"(smem_u32(tmem_slot)), "r"(kTmemColsIks * MT));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
         s_fail = 0;
-        for (int s = 0; s < kStages; s++) {
+        for (int s = 0; s < S; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
@@ -309,53 +324,57 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
 
     if (tid == 0) {
         auto fill = [&](int s, int kc) {
-            unsigned char* st = smem + (size_t)s * kStageBytes;
-            mbar_expect_tx(&full[s], kStageBytes);
-            bulk_g2s(st, ga + (size_t)kc * kATile, kATile, &full[s]);
-            bulk_g2s(st + kATile, gb + (size_t)kc * kBTile, kBTile, &full[s]);
-            pend[s] = 1 + ((kc / kStages) & 1);
+            unsigned char* st = smem + (size_t)s * SB;
+            mbar_expect_tx(&full[s], (uint32_t)(mc * kATile + kBTile));
+            for (int m = 0; m < mc; m++)
+                bulk_g2s(st + m * kATile, ga + ((size_t)m * CH + kc) * kATile, kATile, &full[s]);
+            bulk_g2s(st + MT * kATile, gb + (size_t)kc * kBTile, kBTile, &full[s]);
+            pend[s] = 1 + ((kc / S) & 1);
         };
-        for (int s = 0; s < kStages; s++) fill(s, s);
+        for (int s = 0; s < S; s++) fill(s, s);
         for (int kc = 0; kc < CH; kc++) {
-            const int s = kc % kStages;
-            if (!mbar_wait(&full[s], (kc / kStages) & 1)) {
+            const int s = kc % S;
+            if (!mbar_wait(&full[s], (kc / S) & 1)) {
                 s_fail = 1;
                 break;
             }
             pend[s] = 0;
             tc_fence_after();
-            const uint32_t a0 = smem_u32(smem + (size_t)s * kStageBytes);
-            const uint32_t b0 = a0 + kATile;
+            const uint32_t a0 = smem_u32(smem + (size_t)s * SB);
+            const uint32_t b0 = a0 + MT * kATile;
+            for (int m = 0; m < mc; m++)
 #pragma unroll
-            for (int k = 0; k < kChunkK / 32; k++)
-                tc_mma_i8_ss(tmem, desc_kmajor_sw128(a0 + 32 * k), desc_kmajor_sw128(b0 + 32 * k),
-                             kIdescIks, (kc | k) != 0);
+                for (int k = 0; k < kChunkK / 32; k++)
+                    tc_mma_i8_ss(tmem + kTmemColsIks * m, desc_kmajor_sw128(a0 + m * kATile + 32 * k),
+                                 desc_kmajor_sw128(b0 + 32 * k), kIdescIks, (kc | k) != 0);
             tc_commit(&empty[s]);
             last_commit = kc;
-            // refill the stage of chunk kc-1 with chunk kc+3 once its MMAs are done
-            if (kc >= 1 && kc + kStages - 1 < CH) {
-                const int sp = (kc - 1) % kStages;
-                if (!mbar_wait(&empty[sp], ((kc - 1) / kStages) & 1)) {
+            // refill the stage of chunk kc-1 with chunk kc+S-1 once its MMAs are done
+            if (kc >= 1 && kc + S - 1 < CH) {
+                const int sp = (kc - 1) % S;
+                if (!mbar_wait(&empty[sp], ((kc - 1) / S) & 1)) {
                     s_fail = 1;
                     break;
                 }
-                fill(sp, kc + kStages - 1);
+                fill(sp, kc + S - 1);
             }
         }
-        if (!s_fail && !mbar_wait(&empty[(CH - 1) % kStages], ((CH - 1) / kStages) & 1))
+        if (!s_fail && !mbar_wait(&empty[(CH - 1) % S], ((CH - 1) / S) & 1))
             s_fail = 1;
         if (s_fail) {
             atomicOr(err, 1);
-            for (int s = 0; s < kStages; s++)
+            for (int s = 0; s < S; s++)
                 if (pend[s]) mbar_wait(&full[s], (uint32_t)(pend[s] - 1));
             if (last_commit >= 0)
-                mbar_wait(&empty[last_commit % kStages], (uint32_t)((last_commit / kStages) & 1));
+                mbar_wait(&empty[last_commit % S], (uint32_t)((last_commit / S) & 1));
         }
     }
     __syncthreads();
     tc_fence_after();
-    if (!s_fail) {
-        const int u = gt * kMGates + warp * 32 + lane;  // this thread's TMEM lane = gate row
+#pragma unroll 1
+    for (int m = 0; m < mc && !s_fail; m++) {
+        // this thread's TMEM lane = unit row of tile gt * MT + m
+        const int u = (gt * MT + m) * kMGates + warp * 32 + lane;
         const bool live = u < units && (!valid || valid[u]);
         uint32_t* rowp = dst;
         if (live)
@@ -365,7 +384,7 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
 #pragma unroll 1
         for (int cc = 0; cc < kNCols / 32; cc++) {
             uint32_t v[32];
-            tmem_ld32(tmem + lane_base + 32 * cc, v);
+            tmem_ld32(tmem + lane_base + kTmemColsIks * m + 32 * cc, v);
             tmem_wait_ld();
             if (live) {
 #pragma unroll
@@ -383,7 +402,7 @@ __global__ void __launch_bounds__(128, 1) k_iks_gemm(const uint8_t* __restrict__
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(kTmemColsIks));
+                     "r"(kTmemColsIks * MT));
 }
 
 }  // namespace
@@ -436,12 +455,12 @@ void iks_tc_workspace_free(IksWorkspace& w)
     w = IksWorkspace();
 }
 
-template <int CH, int NT, int OUTW>
+template <int CH, int NT, int OUTW, int MT = 1>
 static cudaError_t gemm_attr()
 {
     static DeviceAttrFlags attr;
     {
-        const cudaError_t e = set_smem_attr_once(attr, k_iks_gemm<CH, NT, OUTW>, kSmem);
+        const cudaError_t e = set_smem_attr_once(attr, k_iks_gemm<CH, NT, OUTW, MT>, iks_smem<MT>());
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -504,14 +523,16 @@ cudaError_t launch_privks_tc(const uint64_t* tlwe, int units, const uint8_t* key
     *launches = 0;
     if (units <= 0) return cudaSuccess;
     cudaError_t e = iks_tc_workspace(w, units, kPksChunks);
-    if (e == cudaSuccess) e = gemm_attr<kPksChunks, kPksNTiles, kPksWordsOut>();
+    constexpr int kMT = 2;  // two unit tiles per CTA share each 2.5 GB key's chunks
+    if (e == cudaSuccess) e = gemm_attr<kPksChunks, kPksNTiles, kPksWordsOut, kMT>();
     if (e != cudaSuccess) return e;
     if (prep) k_pks_prep<<<units, 256, 0, st>>>(tlwe, units, map, w.atiles);
     const int gtiles = (units + kMGates - 1) / kMGates;
+    const int ggroups = (gtiles + kMT - 1) / kMT;
     const OutMap om = {nullptr, map.per, map.stride_lo, map.stride_hi};
-    k_iks_gemm<kPksChunks, kPksNTiles, kPksWordsOut>
-        <<<gtiles * kPksNTiles, 128, kSmem, st>>>(w.atiles, key_tiles, nullptr, nullptr, units, out,
-                                                  om, err);
+    k_iks_gemm<kPksChunks, kPksNTiles, kPksWordsOut, kMT>
+        <<<ggroups * kPksNTiles, 128, iks_smem<kMT>(), st>>>(w.atiles, key_tiles, nullptr, nullptr,
+                                                             units, out, om, err);
     *launches = prep ? 2 : 1;
     return cudaGetLastError();
 }
