@@ -103,6 +103,13 @@ struct cufhe_circuit_s {
     uint32_t* graph_wires = nullptr;
     int graph_precision = -1;
     uint64_t graph_launches = 0;
+    // cufhe_circuit_create_split: groups of the circuit's connected components,
+    // each a circuit of its own (waves, workspace, graph) run on its own
+    // stream, all groups concurrently; the fields above are then unused
+    std::vector<cufhe_circuit_s*> parts;
+    std::vector<cudaStream_t> part_st;
+    std::vector<cudaEvent_t> part_done;
+    cudaEvent_t part_fork = nullptr;
 };
 
 namespace cufhe {
@@ -766,6 +773,10 @@ int circuit_capture(cufhe_circuit_s* c, uint32_t* wires)
 void circuit_free(cufhe_circuit_s* c)
 {
     cudaSetDevice(c->device);
+    for (cufhe_circuit_s* q : c->parts) circuit_free(q);
+    for (cudaStream_t st : c->part_st) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : c->part_done) cudaEventDestroy(ev);
+    if (c->part_fork) cudaEventDestroy(c->part_fork);
     circuit_drop_graph(c);
     cudaFree(c->dbuf);
     free_ws(c->exec.ws);
@@ -1316,6 +1327,80 @@ int cufhe_circuit_plan(int level, size_t num_wires, size_t num_gates, const int3
     return CUFHE_OK;
 }
 
+// Connected components of the gate graph (a gate is joined to the producers
+// of its operands), packed into at most `parts` groups with balanced blind
+// rotations: components by decreasing weight, each into the lightest group
+// (weight = 16 x lanes + gates, so that Not/Copy-only components count too).
+// Gates of different groups read no wire the other group writes, so the
+// groups can run concurrently.  The circuit must be valid (plan_waves).
+// Returns the number of non-empty groups, numbered 0 .. n-1.
+static int split_components(size_t num_wires, size_t num_gates, const int32_t* gate_ops,
+                            const int32_t* in0, const int32_t* in1, const int32_t* in2,
+                            const int32_t* out, int parts, std::vector<int32_t>& group)
+{
+    std::vector<int32_t> parent(num_gates), producer(num_wires, -1);
+    for (size_t g = 0; g < num_gates; g++) {
+        parent[g] = (int32_t)g;
+        producer[out[g]] = (int32_t)g;
+    }
+    auto find = [&](int32_t x) {
+        while (parent[x] != x) {
+            parent[x] = parent[parent[x]];
+            x = parent[x];
+        }
+        return x;
+    };
+    for (size_t g = 0; g < num_gates; g++) {
+        const int op = gate_ops[g];
+        const int nin = (op == kNot || op == kCopy) ? 1 : ((op == kMux || op == kNMux) ? 3 : 2);
+        const int32_t* ins[3] = {in0, in1, in2};
+        for (int k = 0; k < nin; k++) {
+            const int32_t q = producer[ins[k][g]];
+            if (q < 0) continue;
+            const int32_t a = find((int32_t)g), b = find(q);
+            if (a != b) parent[a] = b;
+        }
+    }
+    std::vector<int64_t> weight(num_gates, 0);
+    for (size_t g = 0; g < num_gates; g++)
+        weight[find((int32_t)g)] += 16 * lanes_of_gate(gate_ops[g]) + 1;
+    std::vector<int32_t> comps;
+    for (size_t g = 0; g < num_gates; g++)
+        if (parent[g] == (int32_t)g) comps.push_back((int32_t)g);
+    std::stable_sort(comps.begin(), comps.end(),
+                     [&](int32_t a, int32_t b) { return weight[a] > weight[b]; });
+    const int np = (int)std::min<size_t>((size_t)parts, comps.size());
+    std::vector<int64_t> load(np, 0);
+    std::vector<int32_t> group_of_root(num_gates, -1);
+    for (int32_t r : comps) {
+        int k = 0;
+        for (int i = 1; i < np; i++)
+            if (load[i] < load[k]) k = i;
+        group_of_root[r] = k;
+        load[k] += weight[r];
+    }
+    group.assign(num_gates, 0);
+    for (size_t g = 0; g < num_gates; g++) group[g] = group_of_root[find((int32_t)g)];
+    return np;
+}
+
+int cufhe_circuit_split_plan(int level, size_t num_wires, size_t num_gates,
+                             const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
+                             const int32_t* in2, const int32_t* out, int parts,
+                             int32_t* group_of_gate)
+{
+    if (!group_of_gate) return fail(CUFHE_ERR_ARG, "null plan output");
+    if (parts < 1 || parts > 64) return fail(CUFHE_ERR_ARG, "parts %d outside 1..64", parts);
+    std::vector<int32_t> wave;
+    int nwaves = 0;
+    int rc = plan_waves(level, num_wires, num_gates, gate_ops, in0, in1, in2, out, 0, wave, nwaves);
+    if (rc != CUFHE_OK) return rc;
+    std::vector<int32_t> group;
+    rc = split_components(num_wires, num_gates, gate_ops, in0, in1, in2, out, parts, group);
+    for (size_t g = 0; g < num_gates; g++) group_of_gate[g] = group[g];
+    return rc;
+}
+
 // Device form of a planned circuit: one Plan per wave over the gates
 // members[w], packed into one device buffer, and a private workspace for the
 // widest wave.  Waves may be empty (a shard of a sharded circuit).
@@ -1468,10 +1553,96 @@ int cufhe_circuit_create(cufhe_circuit_t* out_c, int level, size_t num_wires, si
                          members);
 }
 
+int cufhe_circuit_create_split(cufhe_circuit_t* out_c, int level, size_t num_wires,
+                               size_t num_gates, const int32_t* gate_ops, const int32_t* in0,
+                               const int32_t* in1, const int32_t* in2, const int32_t* out,
+                               int device, int parts)
+{
+    if (!out_c) return fail(CUFHE_ERR_ARG, "null circuit handle");
+    *out_c = nullptr;
+    if (parts < 1 || parts > 64) return fail(CUFHE_ERR_ARG, "parts %d outside 1..64", parts);
+    if (device < 0) device = 0;
+    if (device >= g_gpu_num) return fail(CUFHE_ERR_ARG, "device %d >= gpu num", device);
+    std::vector<int32_t> wave;
+    int nwaves = 0;
+    int rc = plan_waves(level, num_wires, num_gates, gate_ops, in0, in1, in2, out, sms_of(device),
+                        wave, nwaves);
+    if (rc != CUFHE_OK) return rc;
+    std::vector<int32_t> group;
+    const int ng = parts == 1 ? 1
+                              : split_components(num_wires, num_gates, gate_ops, in0, in1, in2,
+                                                 out, parts, group);
+    if (ng <= 1)
+        return cufhe_circuit_create(out_c, level, num_wires, num_gates, gate_ops, in0, in1, in2,
+                                    out, device);
+    const DeviceState& D = g_dev[device];
+    if (level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
+        return fail(CUFHE_ERR_STATE, level == CUFHE_LVL02 ? "cufhe_initialize_lvl02() not called"
+                                                         : "cufhe_initialize() not called");
+    cufhe_circuit_s* c = new cufhe_circuit_s();
+    c->device = device;
+    c->level = level;
+    c->wires = num_wires;
+    c->gates = num_gates;
+    c->exec.device = device;
+    CK(cudaSetDevice(device));
+    for (int k = 0; k < ng && rc == CUFHE_OK; k++) {
+        // the group's gates, in circuit order, as a circuit of its own over the
+        // same wire table
+        std::vector<int32_t> ops_k, i0_k, i1_k, i2_k, out_k;
+        for (size_t g = 0; g < num_gates; g++) {
+            if (group[g] != k) continue;
+            ops_k.push_back(gate_ops[g]);
+            i0_k.push_back(in0[g]);
+            i1_k.push_back(in1 ? in1[g] : -1);
+            i2_k.push_back(in2 ? in2[g] : -1);
+            out_k.push_back(out[g]);
+        }
+        std::vector<int32_t> wave_k;
+        int nw_k = 0;
+        rc = plan_waves(level, num_wires, ops_k.size(), ops_k.data(), i0_k.data(), i1_k.data(),
+                        i2_k.data(), out_k.data(), sms_of(device), wave_k, nw_k);
+        if (rc != CUFHE_OK) break;
+        std::vector<std::vector<int32_t>> members(nw_k);
+        for (size_t g = 0; g < ops_k.size(); g++) members[wave_k[g]].push_back((int32_t)g);
+        cufhe_circuit_t sub = nullptr;
+        rc = build_circuit(&sub, level, num_wires, ops_k.size(), ops_k.data(), i0_k.data(),
+                           i1_k.data(), i2_k.data(), out_k.data(), device, members);
+        if (rc != CUFHE_OK) break;
+        c->parts.push_back(sub);
+        c->max_lanes = std::max(c->max_lanes, sub->max_lanes);
+        c->max_gates = std::max(c->max_gates, sub->max_gates);
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) c->part_st.push_back(st);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) c->part_done.push_back(ev);
+        if (e != cudaSuccess) rc = fail(CUFHE_ERR_CUDA, "circuit part stream: %s", cudaGetErrorString(e));
+    }
+    if (rc == CUFHE_OK) {
+        const cudaError_t e = cudaEventCreateWithFlags(&c->part_fork, cudaEventDisableTiming);
+        if (e != cudaSuccess) rc = fail(CUFHE_ERR_CUDA, "circuit fork event: %s", cudaGetErrorString(e));
+    }
+    if (rc != CUFHE_OK) {
+        circuit_free(c);
+        return rc;
+    }
+    *out_c = c;
+    return CUFHE_OK;
+}
+
+static size_t circuit_waves(const cufhe_circuit_s* c)
+{
+    size_t n = c->waves.size();
+    for (const cufhe_circuit_s* q : c->parts) n = std::max(n, q->waves.size());
+    return n;
+}
+
 int cufhe_circuit_info(cufhe_circuit_t c, int* waves, int* max_wave_gates, int* max_wave_lanes)
 {
     if (!c) return fail(CUFHE_ERR_ARG, "null circuit");
-    if (waves) *waves = (int)c->waves.size();
+    if (waves) *waves = (int)circuit_waves(c);
     if (max_wave_gates) *max_wave_gates = c->max_gates;
     if (max_wave_lanes) *max_wave_lanes = c->max_lanes;
     return CUFHE_OK;
@@ -1480,11 +1651,53 @@ int cufhe_circuit_info(cufhe_circuit_t c, int* waves, int* max_wave_gates, int* 
 int cufhe_circuit_wave_sizes(cufhe_circuit_t c, int32_t* gates, int32_t* lanes, size_t cap)
 {
     if (!c) return fail(CUFHE_ERR_ARG, "null circuit");
-    for (size_t w = 0; w < c->waves.size() && w < cap; w++) {
-        if (gates) gates[w] = c->waves[w].count;
-        if (lanes) lanes[w] = c->waves[w].lanes;
+    const size_t n = circuit_waves(c);
+    for (size_t w = 0; w < n && w < cap; w++) {
+        if (gates) gates[w] = 0;
+        if (lanes) lanes[w] = 0;
     }
-    return (int)c->waves.size();
+    // a split circuit: wave w of every group runs at the same time; their sum
+    const size_t np = c->parts.empty() ? 1 : c->parts.size();
+    for (size_t i = 0; i < np; i++) {
+        const cufhe_circuit_s* q = c->parts.empty() ? c : c->parts[i];
+        for (size_t w = 0; w < q->waves.size() && w < cap; w++) {
+            if (gates) gates[w] += q->waves[w].count;
+            if (lanes) lanes[w] += q->waves[w].lanes;
+        }
+    }
+    return (int)n;
+}
+
+// Runs circuit c (or each group of a split circuit, on the group's own
+// stream, forked from and joined back into st) over `wires` on stream st.
+static int circuit_run_on(cufhe_circuit_s* c, uint32_t* wires, cudaStream_t st, bool graph)
+{
+    if (!c->parts.empty()) {
+        CK(cudaEventRecord(c->part_fork, st));
+        for (size_t i = 0; i < c->parts.size(); i++) {
+            CK(cudaStreamWaitEvent(c->part_st[i], c->part_fork, 0));
+            const int rc = circuit_run_on(c->parts[i], wires, c->part_st[i], graph);
+            if (rc) return rc;
+            CK(cudaEventRecord(c->part_done[i], c->part_st[i]));
+            CK(cudaStreamWaitEvent(st, c->part_done[i], 0));
+        }
+        return CUFHE_OK;
+    }
+    if (!graph) {
+        c->exec.st = st;
+        for (size_t w = 0; w < c->waves.size(); w++) {
+            const int rc = run_wave(c, w, wires);
+            if (rc) return rc;
+        }
+        return CUFHE_OK;
+    }
+    if (!c->gexec || c->graph_wires != wires || c->graph_precision != g_precision) {
+        const int rc = circuit_capture(c, wires);
+        if (rc) return rc;
+    }
+    CK(cudaGraphLaunch(c->gexec, st));
+    g_launches.fetch_add(c->graph_launches);
+    return CUFHE_OK;
 }
 
 int cufhe_circuit_run(cufhe_circuit_t c, uint32_t* wires, cufhe_stream_t st, int use_graph)
@@ -1497,22 +1710,7 @@ int cufhe_circuit_run(cufhe_circuit_t c, uint32_t* wires, cufhe_stream_t st, int
     if (c->level == CUFHE_LVL02 ? !D.ready2 : !D.ready)
         return fail(CUFHE_ERR_STATE, "keys of the circuit's level are not initialised");
     CK(cudaSetDevice(c->device));
-    const bool graph = use_graph != 0;
-    if (!graph) {
-        c->exec.st = s->st;
-        for (size_t w = 0; w < c->waves.size(); w++) {
-            const int rc = run_wave(c, w, wires);
-            if (rc) return rc;
-        }
-        return CUFHE_OK;
-    }
-    if (!c->gexec || c->graph_wires != wires || c->graph_precision != g_precision) {
-        const int rc = circuit_capture(c, wires);
-        if (rc) return rc;
-    }
-    CK(cudaGraphLaunch(c->gexec, s->st));
-    g_launches.fetch_add(c->graph_launches);
-    return CUFHE_OK;
+    return circuit_run_on(c, wires, s->st, use_graph != 0);
 }
 
 int cufhe_circuit_destroy(cufhe_circuit_t c)

@@ -67,6 +67,8 @@ SIGNATURES = {
     "cufhe_circuit_wave_sizes": ([_vp, _vp, _vp, _sz], _i),
     "cufhe_circuit_run": ([_vp, _vp, _vp, _i], _i),
     "cufhe_circuit_destroy": ([_vp], _i),
+    "cufhe_circuit_create_split": ([_vp, _i, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i, _i], _i),
+    "cufhe_circuit_split_plan": ([_i, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i, _vp], _i),
     "cufhe_autotune": ([], _i),
     "cufhe_initialize_cb": ([_vp], _i),
     "cufhe_cleanup_cb": ([], _i),
@@ -354,12 +356,28 @@ def circuit_plan(level: int, num_wires: int, ops, in0, in1, in2, out, sms: int =
     return wave, n.value
 
 
+def circuit_split_plan(level: int, num_wires: int, ops, in0, in1, in2, out, parts: int):
+    """cufhe_circuit_split_plan: the group of every gate when the circuit's
+    connected components are packed into up to `parts` groups (host only).
+    Returns (group of every gate, number of groups)."""
+    ops = np.ascontiguousarray(ops, np.int32)
+    arrs = [np.ascontiguousarray(x, np.int32) for x in (in0, in1, in2, out)]
+    group = np.empty(ops.size, np.int32)
+    n = load().cufhe_circuit_split_plan(level, num_wires, ops.size, _p(ops),
+                                        *(_p(a) for a in arrs), parts, _p(group))
+    check(min(n, 0), "circuit_split_plan")
+    return group, n
+
+
 class Circuit:
     """A DAG of gates over a wire table, levelised into waves by the engine
     (cufhe_circuit_create).  ops/in0/in1/in2/out are per-gate arrays of gate
-    ids and wire indices (-1 for an operand the gate does not take)."""
+    ids and wire indices (-1 for an operand the gate does not take).  With
+    parts > 1 its connected components are packed into up to `parts` groups
+    run concurrently on streams of their own (cufhe_circuit_create_split)."""
 
-    def __init__(self, level: int, num_wires: int, ops, in0, in1, in2, out, device: int = 0):
+    def __init__(self, level: int, num_wires: int, ops, in0, in1, in2, out, device: int = 0,
+                 parts: int = 1):
         arr = lambda a: np.ascontiguousarray(a, np.int32)  # noqa: E731
         self.ops, self.in0, self.in1, self.in2, self.out = (arr(x) for x in (ops, in0, in1, in2,
                                                                             out))
@@ -367,9 +385,10 @@ class Circuit:
         self.num_wires = int(num_wires)
         self.words = P.TLWE1_WORDS if level == LVL1 else P.TLWE0_WORDS
         h = C.c_void_p()
-        check(load().cufhe_circuit_create(C.byref(h), level, self.num_wires, self.ops.size,
-                                          _p(self.ops), _p(self.in0), _p(self.in1),
-                                          _p(self.in2), _p(self.out), device), "circuit_create")
+        check(load().cufhe_circuit_create_split(C.byref(h), level, self.num_wires, self.ops.size,
+                                                _p(self.ops), _p(self.in0), _p(self.in1),
+                                                _p(self.in2), _p(self.out), device, parts),
+              "circuit_create")
         self.h = h
 
     def info(self) -> tuple[int, int, int]:

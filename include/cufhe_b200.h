@@ -270,6 +270,27 @@ int cufhe_circuit_wave_sizes(cufhe_circuit_t c, int32_t* gates, int32_t* lanes, 
 int cufhe_circuit_run(cufhe_circuit_t c, uint32_t* wires, cufhe_stream_t st, int use_graph);
 int cufhe_circuit_destroy(cufhe_circuit_t c);
 
+/* A circuit whose connected components (gates joined through the wires one
+ * writes and another reads) are packed into up to `parts` groups with
+ * balanced blind rotations, each group planned into waves and run on a
+ * stream of its own: cufhe_circuit_run forks from `st` into the groups'
+ * streams and joins back, so that one group's partly filled last round of
+ * rotations in a wave overlaps the other groups' waves.  Results are
+ * bit-identical to cufhe_circuit_create's.  With one component (or
+ * parts = 1) it is cufhe_circuit_create.  cufhe_circuit_info reports the
+ * most waves of any group; cufhe_circuit_wave_sizes the gates and rotations
+ * of the groups' wave w together.  cufhe_circuit_split_plan returns the
+ * group of every gate (host only, no GPU) and the number of groups.
+ * parts: 1 .. 64. */
+int cufhe_circuit_create_split(cufhe_circuit_t* c, int level, size_t num_wires,
+                               size_t num_gates, const int32_t* gate_ops, const int32_t* in0,
+                               const int32_t* in1, const int32_t* in2, const int32_t* out,
+                               int device, int parts);
+int cufhe_circuit_split_plan(int level, size_t num_wires, size_t num_gates,
+                             const int32_t* gate_ops, const int32_t* in0, const int32_t* in1,
+                             const int32_t* in2, const int32_t* out, int parts,
+                             int32_t* group_of_gate);
+
 /* ---- one batch or one circuit over several GPUs -------------------------
  * The reference spreads work over GPUs only through the device each Stream
  * is given in turn, with the keys replicated on every GPU

@@ -162,3 +162,58 @@ def test_plan_reports_the_same_errors_as_create():
         engine.circuit_plan(engine.LVL1, 4, [P.NAND, P.NAND], [0, 3], [1, 1], [-1, -1], [2, 3], 148)
     with pytest.raises(RuntimeError, match="written by gates"):
         engine.circuit_plan(engine.LVL1, 4, [P.NAND, P.AND], [0, 0], [1, 1], [-1, -1], [2, 2], 148)
+
+
+@pytest.mark.parametrize("parts", [1, 2, 3, 8])
+def test_split_plan_groups_whole_components(parts):
+    """cufhe_circuit_split_plan packs connected components into groups: every
+    component lies in one group (so no wire written in one group is read in
+    another), every group is used, and the groups' blind-rotation weights are
+    within one component's weight of each other."""
+    net = CI.uneven_workload(5, dags=20, adders=6, dag_gates=(50, 300), adder_width=(8, 24))
+    group, n = engine.circuit_split_plan(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1,
+                                         net.in2, net.out, parts)
+    assert n == parts and group.min() == 0 and group.max() == n - 1
+    writer = np.full(net.num_wires, -1)
+    writer[net.out] = group
+    for arr in (net.in0, net.in1, net.in2):
+        used = arr >= 0
+        w = writer[arr[used]]
+        assert np.all((w < 0) | (w == group[used]))
+    lanes = np.where((net.ops == P.MUX) | (net.ops == P.NMUX), 2,
+                     np.where((net.ops == P.NOT) | (net.ops == P.COPY), 0, 1))
+    weight = 16 * lanes + 1
+    load = np.bincount(group, weights=weight, minlength=n)
+    # connected components (union-find over producer -> consumer wires)
+    parent = np.arange(net.gates)
+
+    def find(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+    prod = np.full(net.num_wires, -1)
+    prod[net.out] = np.arange(net.gates)
+    for g in range(net.gates):
+        for arr in (net.in0, net.in1, net.in2):
+            if arr[g] >= 0 and prod[arr[g]] >= 0:
+                a, b = find(g), find(int(prod[arr[g]]))
+                if a != b:
+                    parent[a] = b
+    roots = np.array([find(g) for g in range(net.gates)])
+    _, comp = np.unique(roots, return_inverse=True)
+    comp_weight = np.bincount(comp, weights=weight)
+    assert all(np.unique(group[comp == k]).size == 1 for k in range(comp_weight.size))
+    assert load.max() - load.min() <= comp_weight.max()
+
+
+def test_split_plan_rejects_bad_part_counts():
+    net = CI.ripple_carry_adder(4)
+    for bad in (0, 65):
+        with pytest.raises(engine.CufheError):
+            engine.circuit_split_plan(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1,
+                                      net.in2, net.out, bad)
+    # one component: one group whatever was asked
+    group, n = engine.circuit_split_plan(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1,
+                                         net.in2, net.out, 4)
+    assert n == 1 and not group.any()

@@ -190,3 +190,41 @@ def test_autotune_table_and_gates(lvl1_ctx):
     engine.synchronize()
     exp = np.array([P.TRUTH[g](int(x), int(y), int(z)) for g, x, y, z in zip(gates, a, b, c)])
     assert np.array_equal(client.decrypt_bits(sk, out, 1), exp)
+
+
+@pytest.mark.parametrize("parts", [2, 3])
+def test_split_circuit_is_bit_identical(lvl1_ctx, parts):
+    """cufhe_circuit_create_split: the circuit's connected components packed
+    into groups that run concurrently on streams of their own give the same
+    wires, bit for bit, as the one-stream circuit (graph and direct runs, on
+    the default and on a created stream)."""
+    sk = lvl1_ctx
+    net = CI.uneven_workload(23, dags=12, adders=4, dag_gates=(50, 400), adder_width=(8, 24))
+    bits, host = prepare(sk, net, engine.LVL1, 61)
+    ref, _, _, _ = run_circuit(net, engine.LVL1, host)
+    group, n = engine.circuit_split_plan(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1,
+                                         net.in2, net.out, parts)
+    assert n == parts
+    sub_waves = []
+    for k in range(n):
+        m = np.flatnonzero(group == k)
+        sub_waves.append(engine.circuit_plan(engine.LVL1, net.num_wires, net.ops[m], net.in0[m],
+                                             net.in1[m], net.in2[m], net.out[m])[1])
+    d = engine.to_device(host)
+    c = engine.Circuit(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1, net.in2, net.out,
+                       parts=parts)
+    assert c.info()[0] == max(sub_waves)
+    gs, _ = c.wave_sizes()
+    assert gs.sum() == net.gates
+    st = engine.Stream(0)
+    for graph, stream in ((False, None), (True, None), (True, None), (True, st), (False, st)):
+        d.upload(host)
+        engine.synchronize()
+        c.run(d, stream=stream, graph=graph)
+        if stream is not None:
+            stream.synchronize()  # the download below runs on the default stream
+        got = engine.from_device(d, host.shape)
+        assert np.array_equal(got, ref), (graph, stream is not None)
+    st.destroy()
+    c.destroy()
+    check_decrypts(sk, net, engine.LVL1, bits, ref)
