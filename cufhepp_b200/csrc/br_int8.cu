@@ -865,7 +865,7 @@ __global__ void k_i8_extract(const uint32_t* __restrict__ acc, int lanes,
             lane_out[(size_t)l * kTlwe1 + i] = i == kN ? a[kN] : (i == 0 ? a[0] : 0u - a[kN - i]);
 }
 
-cudaError_t ensure_ws(Int8Workspace& w, int lanes)
+cudaError_t ensure_ws(Int8Workspace& w, int lanes, cudaStream_t st)
 {
     if ((size_t)lanes <= w.cap) return cudaSuccess;
     int8_workspace_free(w);
@@ -874,7 +874,11 @@ cudaError_t ensure_ws(Int8Workspace& w, int lanes)
     if ((e = cudaMalloc(&w.acc, (size_t)lanes * kTrlwe * 4)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&w.abar, (size_t)lanes * 640 * 2)) != cudaSuccess) return e;
     if ((e = cudaMalloc((void**)&w.digits, (size_t)groups * kChunks * kTileBytes)) != cudaSuccess) return e;
-    if ((e = cudaMemset(w.digits, 0, (size_t)groups * kChunks * kTileBytes)) != cudaSuccess) return e;
+    // zeroed on the stream of the launches that use it: the engine's streams
+    // are non-blocking, so a memset on the legacy stream would not be ordered
+    // before (and could land after) the first decompose's stores
+    e = cudaMemsetAsync(w.digits, 0, (size_t)groups * kChunks * kTileBytes, st);
+    if (e != cudaSuccess) return e;
     w.cap = (size_t)lanes;
     return cudaSuccess;
 }
@@ -978,9 +982,9 @@ void int8_workspace_free(Int8Workspace& w)
     w = Int8Workspace();
 }
 
-cudaError_t int8_reserve(Int8Workspace& w, int lanes)
+cudaError_t int8_reserve(Int8Workspace& w, int lanes, cudaStream_t st)
 {
-    const cudaError_t e = ensure_ws(w, lanes);
+    const cudaError_t e = ensure_ws(w, lanes, st);
     return e != cudaSuccess ? e : set_gemm_attr();
 }
 
@@ -990,7 +994,7 @@ cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* l
 {
     *launches = 0;
     if (lanes <= 0) return cudaSuccess;
-    cudaError_t e = int8_reserve(w, lanes);
+    cudaError_t e = int8_reserve(w, lanes, st);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);

@@ -38,11 +38,12 @@ void int8_workspace_free(Int8Workspace& w);
 // graph once the workspace is reserved): a kernel whose bounded wait gives
 // up sets *err, which the caller reads at synchronisation.
 // int8_reserve*: size the workspace for `lanes` and set the kernels'
-// attributes; call before a graph capture.
+// attributes; call before a graph capture.  A new workspace is zeroed on
+// `st`, so the launches that use it must be ordered after that stream's work.
 // launch_br_int8: `steps` counts CMUX steps of a plain key, pairs of a
 // KeyBundle key (all of them when steps < 0).
-cudaError_t int8_reserve(Int8Workspace& w, int lanes);
-cudaError_t int8_reserve2(Int8Workspace2& w, int lanes);
+cudaError_t int8_reserve(Int8Workspace& w, int lanes, cudaStream_t st);
+cudaError_t int8_reserve2(Int8Workspace2& w, int lanes, cudaStream_t st);
 cudaError_t launch_br_int8(const Int8Key& k, Int8Workspace& w, const uint32_t* lane_in, int lanes,
                            uint32_t mu, int steps, uint32_t* acc_out, uint32_t* lane_out,
                            int* err, cudaStream_t st, int* launches);

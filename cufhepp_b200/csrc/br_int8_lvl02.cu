@@ -557,7 +557,7 @@ __global__ void k_i82_extract(const uint64_t* __restrict__ acc, int lanes,
                 i == kN2 ? a[kN2] : (i == 0 ? a[0] : 0ull - a[kN2 - i]);
 }
 
-cudaError_t ensure_ws2(Int8Workspace2& w, int lanes)
+cudaError_t ensure_ws2(Int8Workspace2& w, int lanes, cudaStream_t st)
 {
     if ((size_t)lanes <= w.cap) return cudaSuccess;
     int8_workspace2_free(w);
@@ -567,7 +567,8 @@ cudaError_t ensure_ws2(Int8Workspace2& w, int lanes)
     if ((e = cudaMalloc(&w.acc, (size_t)lanes * kTrlwe2 * 8)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&w.abar, (size_t)lanes * kAbarStride * 2)) != cudaSuccess) return e;
     if ((e = cudaMalloc((void**)&w.digits, dbytes)) != cudaSuccess) return e;
-    if ((e = cudaMemset(w.digits, 0, dbytes)) != cudaSuccess) return e;
+    // zeroed in stream order (the engine's streams are non-blocking)
+    if ((e = cudaMemsetAsync(w.digits, 0, dbytes, st)) != cudaSuccess) return e;
     w.cap = (size_t)lanes;
     return cudaSuccess;
 }
@@ -606,9 +607,9 @@ void int8_workspace2_free(Int8Workspace2& w)
     w = Int8Workspace2();
 }
 
-cudaError_t int8_reserve2(Int8Workspace2& w, int lanes)
+cudaError_t int8_reserve2(Int8Workspace2& w, int lanes, cudaStream_t st)
 {
-    const cudaError_t e = ensure_ws2(w, lanes);
+    const cudaError_t e = ensure_ws2(w, lanes, st);
     return e != cudaSuccess ? e : set_gemm2_attr();
 }
 
@@ -618,7 +619,7 @@ cudaError_t launch_br2_int8(const Int8Key& k, Int8Workspace2& w, const uint32_t*
 {
     *launches = 0;
     if (lanes <= 0) return cudaSuccess;
-    cudaError_t e = int8_reserve2(w, lanes);
+    cudaError_t e = int8_reserve2(w, lanes, st);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);

@@ -735,14 +735,17 @@ void circuit_drop_graph(cufhe_circuit_s* c)
     c->graph_wires = nullptr;
 }
 
-// Captures every wave into a CUDA graph (on the circuit's private stream)
-int circuit_capture(cufhe_circuit_s* c, uint32_t* wires)
+// Captures every wave into a CUDA graph (on the circuit's private stream);
+// `st` is the stream the graph is launched on next
+int circuit_capture(cufhe_circuit_s* c, uint32_t* wires, cudaStream_t st)
 {
     circuit_drop_graph(c);
     if (g_precision == CUFHE_INT8_EXACT && c->max_lanes > 0) {
-        // the INT8 workspace must not be allocated inside the capture
-        const cudaError_t e = c->level == CUFHE_LVL02 ? int8_reserve2(c->exec.ws.i8_2, c->max_lanes)
-                                                      : int8_reserve(c->exec.ws.i8, c->max_lanes);
+        // the INT8 workspace must not be allocated inside the capture; a new
+        // one is zeroed on `st`, ahead of the graph launch
+        const cudaError_t e = c->level == CUFHE_LVL02
+                                  ? int8_reserve2(c->exec.ws.i8_2, c->max_lanes, st)
+                                  : int8_reserve(c->exec.ws.i8, c->max_lanes, st);
         if (e != cudaSuccess)
             return fail(CUFHE_ERR_NOMEM, "INT8 workspace: %s", cudaGetErrorString(e));
     }
@@ -1507,9 +1510,13 @@ static int build_circuit(cufhe_circuit_t* out_c, int level, size_t num_wires, si
     if (e == cudaSuccess) {
         const int units = level == CUFHE_LVL1 ? max_lanes : max_gates;
         if (units > 0) e = iks_tc_reserve(level == CUFHE_LVL02 ? ws.iks2 : ws.iks, units,
-                                          level == CUFHE_LVL02);
+                                          level == CUFHE_LVL02, 0);
     }
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking);
+    // the plan upload (a pageable copy may return before its DMA ends) and the
+    // zeroing above are on the legacy stream, which the engine's non-blocking
+    // streams do not wait for: finish them before the circuit can run
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
         circuit_free(c);
         return fail(CUFHE_ERR_NOMEM, "circuit buffers: %s", cudaGetErrorString(e));
@@ -1692,7 +1699,7 @@ static int circuit_run_on(cufhe_circuit_s* c, uint32_t* wires, cudaStream_t st, 
         return CUFHE_OK;
     }
     if (!c->gexec || c->graph_wires != wires || c->graph_precision != g_precision) {
-        const int rc = circuit_capture(c, wires);
+        const int rc = circuit_capture(c, wires, st);
         if (rc) return rc;
     }
     CK(cudaGraphLaunch(c->gexec, st));
@@ -2038,6 +2045,9 @@ int cufhe_sharded_create(cufhe_sharded_t* out_c, int level, size_t num_wires, si
         if (e == cudaSuccess && !rows.empty()) e = cudaMalloc(&c->rowbuf[k], rows.size() * 4);
         if (e == cudaSuccess && !rows.empty())
             e = cudaMemcpy(c->rowbuf[k], rows.data(), rows.size() * 4, cudaMemcpyHostToDevice);
+        // a pageable copy may return before its DMA ends, and the shard streams
+        // are non-blocking: finish it before they can read the rows
+        if (e == cudaSuccess && !rows.empty()) e = cudaStreamSynchronize(0);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st[k], cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev[k], cudaEventDisableTiming);
         if (e != cudaSuccess) {

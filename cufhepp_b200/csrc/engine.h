@@ -244,8 +244,8 @@ size_t iks_tc_key_bytes();
 cudaError_t iks_tc_key_build(const uint32_t* ksk_dev, uint8_t* key_tiles, cudaStream_t st);
 void iks_tc_workspace_free(IksWorkspace& w);
 // sizes the workspace for `units` key switches up front (lvl1 or lvl2 inputs),
-// so that later launches allocate nothing
-cudaError_t iks_tc_reserve(IksWorkspace& w, int units, bool lvl2);
+// so that later launches allocate nothing; a new workspace is zeroed on `st`
+cudaError_t iks_tc_reserve(IksWorkspace& w, int units, bool lvl2, cudaStream_t st);
 cudaError_t launch_iks_tc(int mode, const Plan& plan, const uint32_t* in0, const uint32_t* in1,
                           const uint32_t* in2, const uint32_t* lane_out, const uint8_t* key_tiles,
                           uint32_t* dst, IksWorkspace& w, int* err, cudaStream_t st,

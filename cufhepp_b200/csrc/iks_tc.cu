@@ -427,14 +427,16 @@ cudaError_t iks20_tc_key_build(const uint32_t* ksk_dev, uint8_t* key_tiles, cuda
     return cudaGetLastError();
 }
 
-static cudaError_t iks_tc_workspace(IksWorkspace& w, int units, int chunks)
+static cudaError_t iks_tc_workspace(IksWorkspace& w, int units, int chunks, cudaStream_t st)
 {
     if ((size_t)units <= w.cap && chunks == w.chunks) return cudaSuccess;
     iks_tc_workspace_free(w);
     const size_t tiles = (size_t)(units + kMGates - 1) / kMGates;
     cudaError_t e;
     if ((e = cudaMalloc(&w.atiles, tiles * chunks * kATile)) != cudaSuccess) return e;
-    if ((e = cudaMemset(w.atiles, 0, tiles * chunks * kATile)) != cudaSuccess) return e;
+    // zeroed in stream order: the engine's streams are non-blocking, so a
+    // memset on the legacy stream could land after the first prep's stores
+    if ((e = cudaMemsetAsync(w.atiles, 0, tiles * chunks * kATile, st)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&w.xb, (size_t)units * 4)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&w.valid, (size_t)units * 4)) != cudaSuccess) return e;
     w.cap = (size_t)units;
@@ -442,9 +444,9 @@ static cudaError_t iks_tc_workspace(IksWorkspace& w, int units, int chunks)
     return cudaSuccess;
 }
 
-cudaError_t iks_tc_reserve(IksWorkspace& w, int units, bool lvl2)
+cudaError_t iks_tc_reserve(IksWorkspace& w, int units, bool lvl2, cudaStream_t st)
 {
-    return iks_tc_workspace(w, units, lvl2 ? iks_chunks<CUFHE_LVL2_N>() : kChunks);
+    return iks_tc_workspace(w, units, lvl2 ? iks_chunks<CUFHE_LVL2_N>() : kChunks, st);
 }
 
 void iks_tc_workspace_free(IksWorkspace& w)
@@ -474,7 +476,7 @@ cudaError_t launch_iks_tc(int mode, const Plan& plan, const uint32_t* in0, const
     *launches = 0;
     const int units = mode == 0 ? plan.lanes : plan.count;
     if (units <= 0) return cudaSuccess;
-    cudaError_t e = iks_tc_workspace(w, units, kChunks);
+    cudaError_t e = iks_tc_workspace(w, units, kChunks, st);
     if (e == cudaSuccess) e = gemm_attr<kChunks, kNTiles, kTlwe0>();
     if (e != cudaSuccess) return e;
     k_iks_prep<<<units, 256, 0, st>>>(mode, plan, in0, in1, in2, lane_out, w.atiles, w.xb, w.valid);
@@ -494,7 +496,7 @@ cudaError_t launch_iks20_tc(const Plan& plan, const uint64_t* lane_out, const ui
     *launches = 0;
     const int units = plan.count;
     if (units <= 0) return cudaSuccess;
-    cudaError_t e = iks_tc_workspace(w, units, kCh);
+    cudaError_t e = iks_tc_workspace(w, units, kCh, st);
     if (e == cudaSuccess) e = gemm_attr<kCh, kNTiles, kTlwe0>();
     if (e != cudaSuccess) return e;
     k_iks20_prep<<<units, 256, 0, st>>>(plan, lane_out, w.atiles, w.xb, w.valid);
@@ -522,7 +524,7 @@ cudaError_t launch_privks_tc(const uint64_t* tlwe, int units, const uint8_t* key
 {
     *launches = 0;
     if (units <= 0) return cudaSuccess;
-    cudaError_t e = iks_tc_workspace(w, units, kPksChunks);
+    cudaError_t e = iks_tc_workspace(w, units, kPksChunks, st);
     constexpr int kMT = 2;  // two unit tiles per CTA share each 2.5 GB key's chunks
     if (e == cudaSuccess) e = gemm_attr<kPksChunks, kPksNTiles, kPksWordsOut, kMT>();
     if (e != cudaSuccess) return e;

@@ -8,7 +8,9 @@
 * gates with scheduling slack move into narrow later waves without adding
   waves;
 * the INT8 form runs circuits as a CUDA graph too (bit-identical to the
-  direct run) and decrypts correctly;
+  direct run) and decrypts correctly, also split into concurrent groups,
+  whose new INT8 workspaces are zeroed in stream order while the other
+  group's kernels run;
 * cufhe_autotune yields a table of lanes-per-CTA choices and gates stay
   correct under it.
 """
@@ -156,6 +158,17 @@ def test_circuit_int8_form(keys, kb):
         direct, g1, g2, (waves, _, _) = run_circuit(net, engine.LVL1, host)
         assert np.array_equal(direct, g1) and np.array_equal(g1, g2)
         check_decrypts(sk, net, engine.LVL1, bits, direct)
+        # the same circuit as concurrent groups of its components (each group
+        # with its own INT8 workspace): the same bits, graph and direct
+        c = engine.Circuit(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1, net.in2,
+                           net.out, parts=2)
+        d = engine.to_device(host)
+        for graph in (True, False):
+            d.upload(host)
+            engine.synchronize()
+            c.run(d, graph=graph)
+            assert np.array_equal(engine.from_device(d, host.shape), direct), graph
+        c.destroy()
     finally:
         engine.set_precision(P.FP64_FFNT)
         engine.initialize(keys[1])  # the KeyBundle key of the module's other tests
