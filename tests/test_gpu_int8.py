@@ -143,3 +143,31 @@ def test_int8_reproduces_golden_digests(ctx):
             want["cases"]["iks16"]["outputs"]
     finally:
         engine.initialize(ctx[1])
+
+
+def test_int8_fresh_streams_run_concurrently(ctx):
+    """Gate batches on newly created engine streams, launched back to back so
+    that their kernels overlap: each stream's first launch allocates and
+    zeroes its INT8 and key-switch workspaces, in stream order, while the
+    other stream's kernels run.  Every output equals the same batch run alone
+    on the default stream (the exact form does not depend on scheduling)."""
+    sk, ek = ctx
+    count = 600
+    rng = np.random.default_rng(91)
+    gates = rng.choice(np.array([P.NAND, P.AND, P.XOR, P.MUX], np.int32), count)
+    cts = [client.encrypt_bits(sk, rng.integers(0, 2, count).astype(np.uint8), 1, seed=92 + i)
+           for i in range(3)]
+    alone = engine.gate_batch_host(gates, engine.LVL1, *cts)
+    engine.synchronize()
+    d_in = [engine.to_device(c) for c in cts]
+    for _ in range(2):
+        streams = [engine.Stream(0) for _ in range(2)]
+        outs = [engine.DeviceBuffer(count * P.TLWE1_WORDS * 4) for _ in streams]
+        for s, o in zip(streams, outs):
+            engine.gate_batch(gates, count, engine.LVL1, o, *d_in, stream=s)
+        for s in streams:
+            s.synchronize()
+        for o in outs:
+            assert np.array_equal(engine.from_device(o, (count, P.TLWE1_WORDS)), alone)
+        for s in streams:
+            s.destroy()
