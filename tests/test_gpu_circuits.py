@@ -183,6 +183,16 @@ def test_circuit_lvl02():
         direct, g1, g2, _ = run_circuit(net, engine.LVL02, host)
         assert np.array_equal(direct, g1) and np.array_equal(g1, g2)
         check_decrypts(sk, net, engine.LVL02, bits, direct)
+        # split into two concurrent groups: the same bits, graph and direct
+        c = engine.Circuit(engine.LVL02, net.num_wires, net.ops, net.in0, net.in1, net.in2,
+                           net.out, parts=2)
+        d = engine.to_device(host)
+        for graph in (True, False):
+            d.upload(host)
+            engine.synchronize()
+            c.run(d, graph=graph)
+            assert np.array_equal(engine.from_device(d, host.shape), direct), graph
+        c.destroy()
     finally:
         engine.cleanup_lvl02()
 
@@ -205,26 +215,28 @@ def test_autotune_table_and_gates(lvl1_ctx):
     assert np.array_equal(client.decrypt_bits(sk, out, 1), exp)
 
 
-@pytest.mark.parametrize("parts", [2, 3])
-def test_split_circuit_is_bit_identical(lvl1_ctx, parts):
+@pytest.mark.parametrize("level,parts", [(engine.LVL1, 2), (engine.LVL1, 3), (engine.LVL0, 2)],
+                         ids=["lvl1-2", "lvl1-3", "lvl0-2"])
+def test_split_circuit_is_bit_identical(lvl1_ctx, level, parts):
     """cufhe_circuit_create_split: the circuit's connected components packed
     into groups that run concurrently on streams of their own give the same
     wires, bit for bit, as the one-stream circuit (graph and direct runs, on
-    the default and on a created stream)."""
+    the default and on a created stream), with Ctxt<lvl1> wires (IKS then
+    blind rotation) and Ctxt<lvl0> wires (blind rotation then IKS)."""
     sk = lvl1_ctx
     net = CI.uneven_workload(23, dags=12, adders=4, dag_gates=(50, 400), adder_width=(8, 24))
-    bits, host = prepare(sk, net, engine.LVL1, 61)
-    ref, _, _, _ = run_circuit(net, engine.LVL1, host)
-    group, n = engine.circuit_split_plan(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1,
+    bits, host = prepare(sk, net, level, 61)
+    ref, _, _, _ = run_circuit(net, level, host)
+    group, n = engine.circuit_split_plan(level, net.num_wires, net.ops, net.in0, net.in1,
                                          net.in2, net.out, parts)
     assert n == parts
     sub_waves = []
     for k in range(n):
         m = np.flatnonzero(group == k)
-        sub_waves.append(engine.circuit_plan(engine.LVL1, net.num_wires, net.ops[m], net.in0[m],
+        sub_waves.append(engine.circuit_plan(level, net.num_wires, net.ops[m], net.in0[m],
                                              net.in1[m], net.in2[m], net.out[m])[1])
     d = engine.to_device(host)
-    c = engine.Circuit(engine.LVL1, net.num_wires, net.ops, net.in0, net.in1, net.in2, net.out,
+    c = engine.Circuit(level, net.num_wires, net.ops, net.in0, net.in1, net.in2, net.out,
                        parts=parts)
     assert c.info()[0] == max(sub_waves)
     gs, _ = c.wave_sizes()
@@ -240,4 +252,4 @@ def test_split_circuit_is_bit_identical(lvl1_ctx, parts):
         assert np.array_equal(got, ref), (graph, stream is not None)
     st.destroy()
     c.destroy()
-    check_decrypts(sk, net, engine.LVL1, bits, ref)
+    check_decrypts(sk, net, level, bits, ref)
