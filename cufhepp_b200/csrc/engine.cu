@@ -1684,9 +1684,11 @@ static int circuit_run_on(cufhe_circuit_s* c, uint32_t* wires, cudaStream_t st, 
         for (size_t i = 0; i < c->parts.size(); i++) {
             CK(cudaStreamWaitEvent(c->part_st[i], c->part_fork, 0));
             const int rc = circuit_run_on(c->parts[i], wires, c->part_st[i], graph);
-            if (rc) return rc;
+            // joined even when the group failed part-way, so that the caller's
+            // stream still orders after whatever the group did launch
             CK(cudaEventRecord(c->part_done[i], c->part_st[i]));
             CK(cudaStreamWaitEvent(st, c->part_done[i], 0));
+            if (rc) return rc;
         }
         return CUFHE_OK;
     }
