@@ -281,6 +281,9 @@ int cufhe_circuit_destroy(cufhe_circuit_t c);
  * most waves of any group; cufhe_circuit_wave_sizes the gates and rotations
  * of the groups' wave w together.  cufhe_circuit_split_plan returns the
  * group of every gate (host only, no GPU) and the number of groups.
+ * Every group keeps a workspace of its own, sized for its widest wave (the
+ * INT8 form's part on the group's first INT8 run, zeroed on the group's
+ * stream), so device memory grows with the number of groups.
  * parts: 1 .. 64. */
 int cufhe_circuit_create_split(cufhe_circuit_t* c, int level, size_t num_wires,
                                size_t num_gates, const int32_t* gate_ops, const int32_t* in0,
