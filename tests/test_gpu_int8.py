@@ -98,7 +98,7 @@ def test_int8_full_rotation_bit_exact(ctx):
 @pytest.mark.parametrize("level", [1, 0])
 def test_int8_gates_bit_exact(ctx, level):
     sk, ek = ctx
-    gates = np.array([P.NAND, P.AND, P.OR, P.XOR, P.XNOR, P.MUX, P.NMUX, P.NOT], np.int32)
+    gates = np.arange(14, dtype=np.int32).repeat(2)  # every gate id, twice
     rng = np.random.default_rng(50 + level)
     a, b, c = (rng.integers(0, 2, gates.size).astype(np.uint8) for _ in range(3))
     cts = [client.encrypt_bits(sk, x, level, seed=60 + i) for i, x in enumerate((a, b, c))]
