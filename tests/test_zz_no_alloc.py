@@ -73,6 +73,18 @@ def test_noalloc_matches_batch_two_calls_in_a_row(ctx):
     assert np.array_equal(client.decrypt_bits(sk, new, 0), exp)
 
 
+@pytest.mark.parametrize("level", [1, 0])
+def test_noalloc_every_gate_matches_batch(ctx, level):
+    """Every gate id (Not and Copy bootstrap nothing, Mux and NMux two lanes a
+    gate) through the allocation-free entry point equals cufhe_gate_batch bit
+    for bit and decrypts to its truth table."""
+    sk = ctx
+    for gate in range(14):
+        ref, new, exp = run_both(sk, gate, 12, level, seed=1000 + 20 * gate + level)
+        assert np.array_equal(new, ref), P.GATE_NAMES[gate]
+        assert np.array_equal(client.decrypt_bits(sk, new, level), exp), P.GATE_NAMES[gate]
+
+
 def test_noalloc_calls_leave_device_memory_unchanged(ctx):
     """After one warm-up pass (the first launch of each kernel may make the
     driver load its code), further calls of every size and level do not
