@@ -7,7 +7,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from cufhepp_b200 import client, gates as G, params as P
+from cufhepp_b200 import client, engine, gates as G, params as P
 
 ROOT = Path(__file__).resolve().parents[1]
 LIB = ROOT / "cufhepp_b200" / "lib"
@@ -105,3 +105,73 @@ def test_python_mirror_lvl02_gates():
             s.Destroy()
     finally:
         G.CleanUp_lvl02()
+
+
+class _View:
+    """A Ctxt-shaped view of one row of a device table (the g* gates read only
+    the level and the device pointer)."""
+
+    def __init__(self, level, ptr):
+        self.level = level
+        self.tlwedevices = [engine.DeviceView(ptr)]
+
+
+@pytest.mark.gpu
+def test_intensive_chained_gates_polled_by_stream_query(keys):
+    """The reference's intensive test (test/test_intensive.cc:23-134): 1000
+    streams, each running a chain of 20 gates in which every gate's output is
+    the next gate's input (NAND and MUX alternating), scheduled by a host loop
+    that polls StreamQuery and issues a stream's next gate only when the
+    stream is idle.  Every chain's last ciphertext decrypts to the chain's
+    plaintext evaluation."""
+    sk, ek, _ = keys
+    streams_n, depth, level = 1000, 20, 1
+    words = P.TLWE1_WORDS
+    G.Initialize(ek)
+    try:
+        rng = np.random.default_rng(2024)
+        x0 = rng.integers(0, 2, streams_n).astype(np.uint8)
+        y = rng.integers(0, 2, (streams_n, depth)).astype(np.uint8)
+        z = rng.integers(0, 2, (streams_n, depth)).astype(np.uint8)
+        # operand table: rows [0, S) chain starts, then y and z of every step
+        ops = np.concatenate([client.encrypt_bits(sk, x0, level, seed=1),
+                              client.encrypt_bits(sk, y.ravel(), level, seed=2),
+                              client.encrypt_bits(sk, z.ravel(), level, seed=3)])
+        d_ops = engine.to_device(ops)
+        d_acc = engine.DeviceBuffer(2 * streams_n * words * 4)  # ping-pong per stream
+        row = lambda base, r: _View(level, base.ptr + r * words * 4)  # noqa: E731
+        yrow = lambda i, k: row(d_ops, streams_n + i * depth + k)  # noqa: E731
+        zrow = lambda i, k: row(d_ops, streams_n + streams_n * depth + i * depth + k)  # noqa: E731
+        st = [G.Stream() for _ in range(streams_n)]
+        for s in st:
+            s.Create()
+        step = [0] * streams_n
+        while True:
+            pending = [i for i in range(streams_n) if step[i] < depth]
+            if not pending:
+                break
+            for i in pending:
+                if not G.StreamQuery(st[i]):
+                    continue
+                k = step[i]
+                src = row(d_ops, i) if k == 0 else row(d_acc, 2 * i + (k - 1) % 2)
+                dst = row(d_acc, 2 * i + k % 2)
+                if k % 2 == 0:
+                    G.gNand(dst, src, yrow(i, k), st[i])
+                else:
+                    G.gMux(dst, yrow(i, k), src, zrow(i, k), st[i])
+                step[i] += 1
+        G.Synchronize()
+        assert all(G.StreamQuery(s) for s in st)
+        acc = engine.from_device(d_acc, (streams_n, 2, words))[:, (depth - 1) % 2]
+        want = x0.astype(np.int64).copy()
+        for k in range(depth):
+            if k % 2 == 0:
+                want = 1 - (want & y[:, k])
+            else:
+                want = np.where(y[:, k] == 1, want, z[:, k])
+        assert np.array_equal(client.decrypt_bits(sk, acc, level), want.astype(np.uint8))
+        for s in st:
+            s.Destroy()
+    finally:
+        G.CleanUp()
